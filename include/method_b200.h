@@ -1,0 +1,121 @@
+/* METHOD-B200 C ABI: the per-timestep hot path of METHOD on one B200.
+ *
+ * Plain C types only (no CUDA or torch types), so that the reference's C++
+ * classes, a ctypes loader or any FFI can bind it.  One handle owns one
+ * simulation's device-resident state in METHOD's own layout,
+ * ID(var,i,j,k) = var*Nx*Ny*Nz + i*Ny*Nz + j*Nz + k (Project/CPU/Include/simData.h:10),
+ * ghost cells included, so host arrays of the reference can be uploaded and
+ * downloaded with plain copies.
+ *
+ * Every entry point returns an mth_status.  Calls on one handle are ordered on
+ * the handle's CUDA stream; calls that return data to the host synchronise.
+ * Errors raised on the device (non-convergence) are sticky until read by
+ * mth_sync / mth_get_stats, which return them as status codes.
+ */
+#ifndef METHOD_B200_H
+#define METHOD_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  MTH_OK = 0,
+  MTH_ERR_C2P = 1,        /* primitive recovery did not converge (srrmhd.cc:576-579) */
+  MTH_ERR_IMPLICIT = 2,   /* SSP2 implicit stage did not converge (SSP2.cc:89-98, 134-143) */
+  MTH_ERR_INVALID = 3,    /* bad configuration or argument (simData.cc:100-106, weno.cc:13-20) */
+  MTH_ERR_CUDA = 4        /* CUDA runtime error (no device, launch failure, ...) */
+} mth_status;
+
+enum { MTH_SRMHD = 0, MTH_SRRMHD = 1 };                       /* Model subclasses */
+enum { MTH_OUTFLOW = 0, MTH_PERIODIC = 1, MTH_FLOW = 2 };     /* Bcs subclasses */
+enum { MTH_RK2 = 0, MTH_RKSPLIT = 1, MTH_SSP2 = 2 };          /* TimeIntegrator subclasses */
+enum { MTH_PLAIN_FP64 = 0, MTH_MIXED = 1 };                   /* precision of the flux path */
+enum { MTH_GUESS_PREVIOUS = 0, MTH_GUESS_MLP = 1 };           /* C2P initial guess */
+
+/* The Data constructor arguments (Project/CPU/Include/simData.h:205-218) plus
+ * the choice of Model, WENO order, Bcs and TimeIntegrator. */
+typedef struct {
+  int model;                 /* MTH_SRMHD / MTH_SRRMHD */
+  int nx, ny, nz;            /* interior cells; ny = 0 for 1D, nz = 0 for 2D */
+  double xmin, xmax, ymin, ymax, zmin, zmax;
+  double endTime, cfl;
+  int Ng;                    /* ghost cells, >= WENO shift + 1 */
+  double gamma, sigma, cp;
+  int weno_order;            /* 3 or 5 (Weno3 / Weno5) */
+  int bcs;                   /* MTH_OUTFLOW / MTH_PERIODIC / MTH_FLOW */
+  int integrator;            /* MTH_RK2 / MTH_RKSPLIT / MTH_SSP2 */
+  int precision;             /* MTH_PLAIN_FP64 / MTH_MIXED */
+  int guess;                 /* MTH_GUESS_PREVIOUS / MTH_GUESS_MLP */
+  int device;                /* CUDA device ordinal */
+} mth_config;
+
+typedef struct {
+  long long c2p_cells;        /* cells solved by primitive recovery */
+  long long c2p_evals;        /* residual evaluations spent by primitive recovery */
+  long long c2p_unconverged;  /* cells left unconverged (after the SRMHD retry) */
+  long long implicit_cells;   /* cells solved by SSP2 implicit stages */
+  long long implicit_evals;   /* residual evaluations of the implicit stages */
+  long long implicit_failed;  /* implicit solves that did not converge */
+  long long steps;            /* time steps taken */
+  double t, dt;               /* simulation time and last time step */
+  int iters;                  /* Data::iters */
+} mth_stats;
+
+typedef struct mth_handle mth_handle;
+
+/* Data + Model + Bcs + FluxMethod + TimeIntegrator construction, with the
+ * reference's validation (Data::initData, WenoBase::checkSufficientGhostZones).
+ * Allocates all device state. */
+mth_status mth_create(const mth_config* cfg, mth_handle** out);
+mth_status mth_destroy(mth_handle* h);
+const char* mth_last_error(const mth_handle* h);
+
+/* Extents: Nx, Ny, Nz, Ncons, Nprims, Naux, dims. */
+mth_status mth_get_dims(const mth_handle* h, int* dims7);
+
+/* InitialFunc + Simulation::set: takes the primitive state of every cell
+ * (Nprims*Nx*Ny*Nz doubles) and derives cons/aux on the device
+ * (Model::primsToAll, srmhd.cc:573-673 / srrmhd.cc:358-510) then applies the
+ * boundary conditions (simulation.cc:80-101). */
+mth_status mth_set_prims(mth_handle* h, const double* prims_host);
+
+/* Whole-state upload / download in the reference layout.  Any pointer may be
+ * NULL.  Download materialises ghost cells first (Bcs::apply). */
+mth_status mth_upload(mth_handle* h, const double* cons, const double* prims, const double* aux);
+mth_status mth_download(mth_handle* h, double* cons, double* prims, double* aux);
+
+/* Bcs::apply (boundaryConds.h:46) on the device state. */
+mth_status mth_apply_bcs(mth_handle* h);
+/* Model::primsToAll on the device state. */
+mth_status mth_prims_to_all(mth_handle* h);
+/* Model::getPrimitiveVars (model.h:80) on the device state, guess = current prims/aux. */
+mth_status mth_c2p(mth_handle* h);
+/* FluxMethod::F (flux.h:72): fnet of the current state into fnet_host
+ * (Ncons*Nx*Ny*Nz doubles, interior written, rest zero). */
+mth_status mth_flux_F(mth_handle* h, double* fnet_host);
+/* Model::sourceTerm of the current state (interior cells) into source_host. */
+mth_status mth_source(mth_handle* h, double* source_host);
+
+/* TimeIntegrator::step (timeInt.h:61) with an explicit dt; enqueued as one
+ * CUDA graph launch, asynchronous. */
+mth_status mth_step(mth_handle* h, double dt);
+/* Simulation::updateTime (simulation.cc:104-133) n times: dt from cfl with the
+ * slow start and end-time clamp, then step, t += dt, iters++. */
+mth_status mth_update_time(mth_handle* h, int n);
+/* Simulation::evolve without output: updateTime until t >= endTime. */
+mth_status mth_evolve(mth_handle* h);
+/* Waits for queued work and returns the first device-side error, if any. */
+mth_status mth_sync(mth_handle* h);
+mth_status mth_get_stats(mth_handle* h, mth_stats* s);
+mth_status mth_reset_stats(mth_handle* h);
+
+/* Zero-copy access for frameworks that manage device memory themselves:
+ * device pointers of cons, prims, aux (reference layout), valid until
+ * mth_destroy. */
+mth_status mth_device_state(mth_handle* h, double** cons, double** prims, double** aux);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* METHOD_B200_H */

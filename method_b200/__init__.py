@@ -1,0 +1,186 @@
+"""METHOD-B200: METHOD's per-timestep hot path on B200 behind METHOD's own API.
+
+Python mirror of the reference's Simulation interface
+(Project/CPU/Include/simulation.h:23-118) over the C ABI of
+``include/method_b200.h``.  The model, flux method, boundary conditions and
+time integrator are chosen by name exactly as a reference ``main.cc`` wires
+the corresponding classes together (Examples/KelvinHelmholtz/
+SingleFluidIdealSerial/main.cc:18-79).
+
+Errors follow the reference's exceptions: non-convergence raises
+RuntimeError (srrmhd.cc:578, SSP2.cc:92-137), bad configuration raises
+ValueError (std::invalid_argument in simData.cc:100-106, weno.cc:18).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+
+MODELS = {"srmhd": 0, "srrmhd": 1}
+BCS = {"outflow": 0, "periodic": 1, "flow": 2}
+INTEGRATORS = {"rk2": 0, "rksplit": 1, "ssp2": 2}
+PRECISIONS = {"fp64": 0, "mixed": 1}
+GUESSES = {"previous": 0, "mlp": 1}
+
+__all__ = ["Simulation", "MODELS", "BCS", "INTEGRATORS"]
+
+
+def _dptr(a):
+    if a is None:
+        return None
+    if a.dtype != np.float64 or not a.flags["C_CONTIGUOUS"]:
+        raise ValueError("arrays must be C-contiguous float64")
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class Simulation:
+    """One device-resident simulation (Data + Model + FVS + Bcs + integrator).
+
+    Keyword arguments are the reference Data constructor's (nx, ny, nz, xmin ..
+    zmax, endTime, cfl, Ng, gamma, sigma, cp) plus ``model``, ``weno``,
+    ``bcs``, ``integrator``, ``precision`` and ``guess``.
+    """
+
+    def __init__(self, nx, ny, nz=0, xmin=0.0, xmax=1.0, ymin=0.0, ymax=1.0, zmin=0.0,
+                 zmax=1.0, endTime=1.0, cfl=0.5, Ng=4, gamma=5.0 / 3.0, sigma=1e3, cp=0.1,
+                 model="srmhd", weno=3, bcs="periodic", integrator="rk2", precision="fp64",
+                 guess="previous", device=0):
+        self.L = _lib.load()
+        c = _lib.Config()
+        c.model = MODELS[model]
+        c.nx, c.ny, c.nz = nx, ny, nz
+        c.xmin, c.xmax, c.ymin, c.ymax, c.zmin, c.zmax = xmin, xmax, ymin, ymax, zmin, zmax
+        c.endTime, c.cfl, c.Ng = endTime, cfl, Ng
+        c.gamma, c.sigma, c.cp = gamma, sigma, cp
+        c.weno_order = weno
+        c.bcs = BCS[bcs]
+        c.integrator = INTEGRATORS[integrator]
+        c.precision = PRECISIONS[precision]
+        c.guess = GUESSES[guess]
+        c.device = device
+        self.cfg = c
+        h = C.c_void_p()
+        rc = self.L.mth_create(C.byref(c), C.byref(h))
+        if rc == 3:
+            raise ValueError("invalid simulation configuration")
+        if rc != 0:
+            raise RuntimeError(f"mth_create failed: {_lib.STATUS.get(rc, rc)}")
+        self.h = h
+        d = (C.c_int * 7)()
+        self.L.mth_get_dims(self.h, d)
+        self.Nx, self.Ny, self.Nz, self.Ncons, self.Nprims, self.Naux, self.dims = list(d)
+
+    # -- lifetime ---------------------------------------------------------------
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.mth_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -- helpers ----------------------------------------------------------------
+    def _check(self, rc, what):
+        if rc == 0:
+            return
+        msg = self.L.mth_last_error(self.h).decode()
+        if rc in (1, 2):
+            raise RuntimeError(f"{what}: {msg}")
+        if rc == 3:
+            raise ValueError(f"{what}: {msg}")
+        raise RuntimeError(f"{what}: CUDA error: {msg}")
+
+    def shape(self, nv):
+        return (nv, self.Nx, self.Ny, self.Nz)
+
+    def zeros(self, nv):
+        return np.zeros(self.shape(nv), dtype=np.float64)
+
+    # -- reference API ----------------------------------------------------------
+    def set_prims(self, prims):
+        """InitialFunc + Simulation::set: primitive state of every cell."""
+        prims = np.ascontiguousarray(prims, dtype=np.float64)
+        if prims.shape != self.shape(self.Nprims):
+            raise ValueError(f"prims must have shape {self.shape(self.Nprims)}")
+        self._check(self.L.mth_set_prims(self.h, _dptr(prims)), "set")
+
+    def upload(self, cons=None, prims=None, aux=None):
+        f = lambda a: None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+        cons, prims, aux = f(cons), f(prims), f(aux)
+        self._check(self.L.mth_upload(self.h, _dptr(cons), _dptr(prims), _dptr(aux)), "upload")
+
+    def state(self):
+        """(cons, prims, aux) in the reference layout, ghosts included."""
+        c, p, a = self.zeros(self.Ncons), self.zeros(self.Nprims), self.zeros(self.Naux)
+        self._check(self.L.mth_download(self.h, _dptr(c), _dptr(p), _dptr(a)), "download")
+        return c, p, a
+
+    def apply_bcs(self):
+        self._check(self.L.mth_apply_bcs(self.h), "Bcs::apply")
+
+    def prims_to_all(self):
+        self._check(self.L.mth_prims_to_all(self.h), "primsToAll")
+
+    def c2p(self):
+        self._check(self.L.mth_c2p(self.h), "getPrimitiveVars")
+
+    def flux_F(self):
+        f = self.zeros(self.Ncons)
+        self._check(self.L.mth_flux_F(self.h, _dptr(f)), "FVS::F")
+        return f
+
+    def source(self):
+        s = self.zeros(self.Ncons)
+        self._check(self.L.mth_source(self.h, _dptr(s)), "sourceTerm")
+        return s
+
+    def step(self, dt, sync=True):
+        """TimeIntegrator::step with an explicit dt."""
+        self._check(self.L.mth_step(self.h, float(dt)), "step")
+        if sync:
+            self.sync()
+
+    def update_time(self, n=1, sync=True):
+        """Simulation::updateTime, n times."""
+        self._check(self.L.mth_update_time(self.h, int(n)), "updateTime")
+        if sync:
+            self.sync()
+
+    def evolve(self):
+        self._check(self.L.mth_evolve(self.h), "evolve")
+
+    def sync(self):
+        self._check(self.L.mth_sync(self.h), "step")
+
+    def stats(self):
+        s = _lib.Stats()
+        rc = self.L.mth_get_stats(self.h, C.byref(s))
+        d = {k: getattr(s, k) for k, _ in _lib.Stats._fields_}
+        d["status"] = rc
+        return d
+
+    def reset_stats(self):
+        self._check(self.L.mth_reset_stats(self.h), "reset_stats")
+
+    def device_state(self):
+        """Raw device pointers (cons, prims, aux) for zero-copy interop."""
+        c, p, a = C.POINTER(C.c_double)(), C.POINTER(C.c_double)(), C.POINTER(C.c_double)()
+        self._check(self.L.mth_device_state(self.h, C.byref(c), C.byref(p), C.byref(a)), "state")
+        return (C.cast(c, C.c_void_p).value, C.cast(p, C.c_void_p).value,
+                C.cast(a, C.c_void_p).value)
+
+    @property
+    def t(self):
+        return self.stats()["t"]

@@ -1,0 +1,83 @@
+"""ctypes binding of the METHOD-B200 C ABI (include/method_b200.h).
+
+The library is built in-tree (``python -m method_b200.build``) and loaded from
+this package directory.  There is no fallback: if the library or a CUDA device
+is missing, the calls fail with an exception.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmethod_b200.so")
+
+STATUS = {0: "MTH_OK", 1: "MTH_ERR_C2P", 2: "MTH_ERR_IMPLICIT", 3: "MTH_ERR_INVALID",
+          4: "MTH_ERR_CUDA"}
+
+# Exported symbols of include/method_b200.h, in declaration order.
+SYMBOLS = [
+    "mth_create", "mth_destroy", "mth_last_error", "mth_get_dims", "mth_set_prims",
+    "mth_upload", "mth_download", "mth_apply_bcs", "mth_prims_to_all", "mth_c2p",
+    "mth_flux_F", "mth_source", "mth_step", "mth_update_time", "mth_evolve", "mth_sync",
+    "mth_get_stats", "mth_reset_stats", "mth_device_state",
+]
+
+
+class Config(C.Structure):
+    _fields_ = [
+        ("model", C.c_int), ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+        ("xmin", C.c_double), ("xmax", C.c_double), ("ymin", C.c_double),
+        ("ymax", C.c_double), ("zmin", C.c_double), ("zmax", C.c_double),
+        ("endTime", C.c_double), ("cfl", C.c_double), ("Ng", C.c_int),
+        ("gamma", C.c_double), ("sigma", C.c_double), ("cp", C.c_double),
+        ("weno_order", C.c_int), ("bcs", C.c_int), ("integrator", C.c_int),
+        ("precision", C.c_int), ("guess", C.c_int), ("device", C.c_int),
+    ]
+
+
+class Stats(C.Structure):
+    _fields_ = [
+        ("c2p_cells", C.c_longlong), ("c2p_evals", C.c_longlong),
+        ("c2p_unconverged", C.c_longlong), ("implicit_cells", C.c_longlong),
+        ("implicit_evals", C.c_longlong), ("implicit_failed", C.c_longlong),
+        ("steps", C.c_longlong), ("t", C.c_double), ("dt", C.c_double), ("iters", C.c_int),
+    ]
+
+
+_LIB = None
+
+
+def load():
+    """Loads libmethod_b200.so and declares the prototypes."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(
+            f"{LIB_PATH} is missing; build it with `python -m method_b200.build`")
+    L = C.CDLL(LIB_PATH)
+    H = C.c_void_p
+    D = C.POINTER(C.c_double)
+    L.mth_create.argtypes = [C.POINTER(Config), C.POINTER(H)]
+    L.mth_destroy.argtypes = [H]
+    L.mth_last_error.argtypes = [H]
+    L.mth_last_error.restype = C.c_char_p
+    L.mth_get_dims.argtypes = [H, C.POINTER(C.c_int)]
+    L.mth_set_prims.argtypes = [H, D]
+    L.mth_upload.argtypes = [H, D, D, D]
+    L.mth_download.argtypes = [H, D, D, D]
+    for n in ("mth_apply_bcs", "mth_prims_to_all", "mth_c2p", "mth_evolve", "mth_sync",
+              "mth_reset_stats"):
+        getattr(L, n).argtypes = [H]
+    L.mth_flux_F.argtypes = [H, D]
+    L.mth_source.argtypes = [H, D]
+    L.mth_step.argtypes = [H, C.c_double]
+    L.mth_update_time.argtypes = [H, C.c_int]
+    L.mth_get_stats.argtypes = [H, C.POINTER(Stats)]
+    L.mth_device_state.argtypes = [H, C.POINTER(D), C.POINTER(D), C.POINTER(D)]
+    for n in SYMBOLS:
+        if n != "mth_last_error":
+            getattr(L, n).restype = C.c_int
+    _LIB = L
+    return L

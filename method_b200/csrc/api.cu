@@ -1,0 +1,507 @@
+// C-ABI of METHOD-B200 (include/method_b200.h).
+//
+// One handle = one simulation: the state arrays of Data (cons, prims, aux),
+// the work arrays of the chosen TimeIntegrator, and a CUDA stream.  A time
+// step is captured once per distinct dt into a CUDA graph and replayed, so the
+// host enters the device once per step.
+#include <cmath>
+#include <cstdio>
+#include <cstdint>
+#include <cstring>
+#include <map>
+#include <string>
+
+#include <cuda_runtime.h>
+
+#include "launch.h"
+#include "mixed.h"
+#include "../../include/method_b200.h"
+
+using namespace mth;
+
+struct mth_handle {
+  mth_config cfg{};
+  Grid g{};
+  int NC = 0, NP = 0, NA = 0;
+  int device = 0;
+  cudaStream_t st = nullptr;
+  double *cons = nullptr, *prims = nullptr, *aux = nullptr;
+  double *p1cons = nullptr, *p1prims = nullptr, *p1aux = nullptr;
+  double* solution = nullptr;
+  double *u1 = nullptr, *u2 = nullptr, *flux1 = nullptr, *flux2 = nullptr;
+  double *src1 = nullptr, *src2 = nullptr;
+  double *fnet = nullptr, *fplus = nullptr, *fminus = nullptr, *frecon = nullptr;
+  int* fail_list = nullptr;
+  int* fail_count = nullptr;
+  long long* counters = nullptr;  // [0..3] C2P, [4..7] implicit, [8..9] Newton fallbacks
+  MixedWork mixed{};
+  double t = 0, dt = 0;
+  int iters = 0;
+  long long steps = 0;
+  bool ghosts_dirty = false;
+  bool fused = false;
+  std::map<uint64_t, cudaGraphExec_t> graphs;
+  std::string err;
+};
+
+namespace {
+
+mth_status fail(mth_handle* h, mth_status s, const std::string& msg) {
+  if (h) h->err = msg;
+  return s;
+}
+
+#define CU(h, expr)                                                                 \
+  do {                                                                              \
+    cudaError_t _e = (expr);                                                        \
+    if (_e != cudaSuccess)                                                          \
+      return fail(h, MTH_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(_e)); \
+  } while (0)
+
+C2PWork c2p_work(mth_handle* h) { return C2PWork{h->fail_list, h->fail_count, h->counters}; }
+C2PWork imex_work(mth_handle* h) { return C2PWork{h->fail_list, h->fail_count, h->counters + 4}; }
+
+size_t bytes(const mth_handle* h, int nv) { return sizeof(double) * (size_t)nv * h->g.Ntot; }
+
+cudaError_t alloc0(double** p, size_t n, cudaStream_t st) {
+  cudaError_t e = cudaMalloc(p, n);
+  if (e != cudaSuccess) return e;
+  return cudaMemsetAsync(*p, 0, n, st);
+}
+
+// Model::getPrimitiveVars of `cons` into prims/aux, seeded by the guess arrays.
+cudaError_t c2p(mth_handle* h, const double* cons, const double* pg, const double* ag,
+                double* prims, double* aux) {
+  if (h->cfg.precision == MTH_MIXED || h->cfg.guess == MTH_GUESS_MLP)
+    return launch_c2p_mixed(h->g, h->cfg.model, h->cfg.guess, cons, pg, ag, prims, aux,
+                            h->solution, c2p_work(h), h->mixed, h->st);
+  if (h->cfg.model == MTH_SRMHD)
+    return launch_c2p_srmhd(h->g, cons, pg, ag, prims, aux, h->solution, c2p_work(h), h->st);
+  return launch_c2p_srrmhd(h->g, cons, ag, prims, aux, c2p_work(h), h->st);
+}
+
+// FVS::F of (c, p, a) combined with a stage update into `out`.
+cudaError_t flux_stage(mth_handle* h, double* c, double* p, double* a, const double* u0,
+                       double* out, double dt, int mode) {
+  const Grid& g = h->g;
+  if (h->fused) {
+    if (h->cfg.precision == MTH_MIXED)
+      return launch_fvs2d_fp32(g, h->cfg.model, h->cfg.weno_order, c, p, a, u0, out, dt, mode,
+                               h->st);
+    return launch_fvs2d_fp64(g, h->cfg.model, h->cfg.weno_order, c, p, a, u0, out, dt, mode,
+                             h->st);
+  }
+  cudaError_t e = launch_fvs_generic(g, h->cfg.model, h->cfg.weno_order, c, p, a, h->fplus,
+                                     h->fminus, h->frecon, h->fnet, h->st);
+  if (e != cudaSuccess) return e;
+  if (mode == STAGE_FNET)
+    return cudaMemcpyAsync(out, h->fnet, bytes(h, h->NC), cudaMemcpyDeviceToDevice, h->st);
+  return launch_stage_update(g, h->NC, mode, u0, c, h->fnet, dt, out, h->st);
+}
+
+// One TimeIntegrator::step, enqueued on the handle's stream.
+cudaError_t enqueue_step(mth_handle* h, double dt) {
+  cudaError_t e;
+  const int integ = h->cfg.integrator;
+  if (integ == MTH_RK2 || integ == MTH_RKSPLIT) {
+    // RK2::step (RK2.cc:93-100): predictor, finalise(p1), corrector, finalise.
+    if ((e = flux_stage(h, h->cons, h->prims, h->aux, nullptr, h->p1cons, dt, STAGE_EULER)))
+      return e;
+    if ((e = c2p(h, h->p1cons, h->prims, h->aux, h->p1prims, h->p1aux))) return e;
+    if ((e = flux_stage(h, h->p1cons, h->p1prims, h->p1aux, h->cons, h->cons, dt,
+                        STAGE_RK2_CORR)))
+      return e;
+    if ((e = c2p(h, h->cons, h->prims, h->aux, h->prims, h->aux))) return e;
+    if (integ == MTH_RKSPLIT) {
+      // RKSplit::step (rkSplit.cc:31-53): U += dt S(U), finalise.
+      if ((e = launch_source_add(h->g, h->cfg.model, h->cons, h->prims, h->aux, h->cons, dt,
+                                 h->st)))
+        return e;
+      if ((e = c2p(h, h->cons, h->prims, h->aux, h->prims, h->aux))) return e;
+    }
+    return cudaSuccess;
+  }
+  // SSP2::step (SSP2.cc:53-173).
+  if ((e = launch_imex_stage(h->g, 1, h->cons, h->aux, nullptr, nullptr, nullptr, h->u1, dt,
+                             imex_work(h), h->st)))
+    return e;
+  if ((e = c2p(h, h->u1, h->prims, h->aux, h->prims, h->aux))) return e;
+  if ((e = launch_source(h->g, h->cfg.model, h->u1, h->aux, h->src1, h->st))) return e;
+  if ((e = flux_stage(h, h->u1, h->prims, h->aux, nullptr, h->flux1, dt, STAGE_FNET))) return e;
+  if ((e = launch_imex_stage(h->g, 2, h->cons, h->aux, h->u1, h->flux1, h->src1, h->u2, dt,
+                             imex_work(h), h->st)))
+    return e;
+  if ((e = c2p(h, h->u2, h->prims, h->aux, h->prims, h->aux))) return e;
+  if ((e = launch_source(h->g, h->cfg.model, h->u2, h->aux, h->src2, h->st))) return e;
+  if ((e = flux_stage(h, h->u2, h->prims, h->aux, nullptr, h->flux2, dt, STAGE_FNET))) return e;
+  if ((e = launch_ssp2_combine(h->g, h->NC, h->cons, h->flux1, h->flux2, h->src1, h->src2, dt,
+                               h->st)))
+    return e;
+  return c2p(h, h->cons, h->prims, h->aux, h->prims, h->aux);
+}
+
+uint64_t dt_key(double dt) {
+  uint64_t k;
+  std::memcpy(&k, &dt, sizeof k);
+  return k;
+}
+
+mth_status launch_step(mth_handle* h, double dt) {
+  auto it = h->graphs.find(dt_key(dt));
+  cudaGraphExec_t exec = nullptr;
+  if (it == h->graphs.end()) {
+    if (h->graphs.size() >= 8) {
+      for (auto& kv : h->graphs) cudaGraphExecDestroy(kv.second);
+      h->graphs.clear();
+    }
+    cudaGraph_t graph;
+    CU(h, cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e = enqueue_step(h, dt);
+    cudaError_t e2 = cudaStreamEndCapture(h->st, &graph);
+    if (e != cudaSuccess) return fail(h, MTH_ERR_CUDA, std::string("step: ") + cudaGetErrorString(e));
+    if (e2 != cudaSuccess) return fail(h, MTH_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(e2));
+    CU(h, cudaGraphInstantiate(&exec, graph, 0));
+    cudaGraphDestroy(graph);
+    h->graphs[dt_key(dt)] = exec;
+  } else {
+    exec = it->second;
+  }
+  CU(h, cudaGraphLaunch(exec, h->st));
+  h->ghosts_dirty = true;
+  h->steps++;
+  return MTH_OK;
+}
+
+// Simulation::updateTime's dt (simulation.cc:113-124).
+double next_dt(const mth_handle* h) {
+  const mth_config& c = h->cfg;
+  const Grid& g = h->g;
+  double dtX(c.cfl * g.dx / (1.0 * std::sqrt((double)g.dims)));
+  double dtY(c.cfl * g.dy / (1.0 * std::sqrt((double)g.dims)));
+  double dtZ(c.cfl * g.dz / (1.0 * std::sqrt((double)g.dims)));
+  double dt = (dtX <= dtY && dtX <= dtZ) ? dtX : ((dtY < dtZ) ? dtY : dtZ);
+  if (h->iters < 15) dt *= 0.1;
+  if (h->iters >= 15 && h->iters < 30) dt *= 0.25;
+  if (h->t + dt > c.endTime) dt = c.endTime - h->t;
+  return dt;
+}
+
+mth_status read_status(mth_handle* h) {
+  CU(h, cudaStreamSynchronize(h->st));
+  long long cnt[16];
+  CU(h, cudaMemcpy(cnt, h->counters, sizeof cnt, cudaMemcpyDeviceToHost));
+  long long flags = cnt[3] | cnt[7];
+  if (flags & ERR_IMPLICIT)
+    return fail(h, MTH_ERR_IMPLICIT,
+                "IMEX time integrator could not converge to a solution (implicit stage)");
+  if (flags & ERR_C2P) return fail(h, MTH_ERR_C2P, "C2P could not converge.");
+  return MTH_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+mth_status mth_create(const mth_config* cfg, mth_handle** out) {
+  if (!cfg || !out) return MTH_ERR_INVALID;
+  *out = nullptr;
+  mth_handle* h = new mth_handle();
+  h->cfg = *cfg;
+  const mth_config& c = *cfg;
+  // Validation of Data::initData (simData.cc:98-107) and the WENO ghost rule
+  // (weno.cc:13-20).
+  if (c.model != MTH_SRMHD && c.model != MTH_SRRMHD) {
+    delete h;
+    return MTH_ERR_INVALID;
+  }
+  if (c.sigma < 0.0 || (c.weno_order != 3 && c.weno_order != 5) ||
+      c.Ng < (c.weno_order + 1) / 2 + 1 || c.nx <= 0 || c.ny < 0 || c.nz < 0 ||
+      (c.ny == 0 && c.nz != 0) || c.bcs < 0 || c.bcs > 2 || c.integrator < 0 ||
+      c.integrator > 2 || (c.integrator == MTH_SSP2 && c.model != MTH_SRRMHD) ||
+      c.precision < 0 || c.precision > 1 || c.guess < 0 || c.guess > 1) {
+    delete h;
+    return MTH_ERR_INVALID;
+  }
+  Grid& g = h->g;
+  g.nx = c.nx;
+  g.ny = c.ny;
+  g.nz = c.nz;
+  g.Ng = c.Ng;
+  g.Nx = c.nx + 2 * c.Ng;
+  g.Ny = c.ny + 2 * c.Ng;
+  g.Nz = c.nz + 2 * c.Ng;
+  g.dims = 3;
+  double zmin = c.zmin, zmax = c.zmax, ymin = c.ymin, ymax = c.ymax;
+  if (c.nz == 0) {
+    g.Nz = 1;
+    zmin = -1e20;
+    zmax = 1e20;
+    g.dims = 2;
+  }
+  if (c.ny == 0) {
+    g.Nz = g.Ny = 1;
+    zmin = ymin = -1e20;
+    zmax = ymax = 1e20;
+    g.dims = 1;
+  }
+  g.is = c.Ng; g.ie = g.Nx - c.Ng;
+  g.js = c.Ng; g.je = g.Ny - c.Ng;
+  g.ks = c.Ng; g.ke = g.Nz - c.Ng;
+  if (g.dims < 3) { g.ks = 0; g.ke = 1; }
+  if (g.dims < 2) { g.js = 0; g.je = 1; }
+  // Periodic ghost copies must come from interior cells.
+  if ((c.bcs == MTH_PERIODIC || c.bcs == MTH_FLOW) && c.nx < c.Ng) { delete h; return MTH_ERR_INVALID; }
+  if (c.bcs == MTH_PERIODIC && ((g.dims > 1 && c.ny < c.Ng) || (g.dims > 2 && c.nz < c.Ng))) {
+    delete h;
+    return MTH_ERR_INVALID;
+  }
+  g.bcx = c.bcs == MTH_OUTFLOW ? DIM_OUTFLOW : DIM_PERIODIC;
+  g.bcy = g.dims > 1 ? (c.bcs == MTH_PERIODIC ? DIM_PERIODIC : DIM_OUTFLOW) : DIM_NONE;
+  g.bcz = g.dims > 2 ? (c.bcs == MTH_PERIODIC ? DIM_PERIODIC : DIM_OUTFLOW) : DIM_NONE;
+  g.dx = (c.xmax - c.xmin) / (c.nx);
+  g.dy = (ymax - ymin) / (c.ny);
+  g.dz = (zmax - zmin) / (c.nz);
+  g.gamma = c.gamma;
+  g.sigma = c.sigma;
+  g.cp = c.cp;
+  g.Ntot = (long long)g.Nx * g.Ny * g.Nz;
+  h->NC = c.model == MTH_SRMHD ? 9 : 14;
+  h->NP = c.model == MTH_SRMHD ? 8 : 11;
+  h->NA = c.model == MTH_SRMHD ? 13 : 17;
+  h->fused = (g.dims == 2);
+  h->device = c.device;
+
+  auto bail = [&](const char* what, cudaError_t e) {
+    std::fprintf(stderr, "mth_create: %s: %s\n", what, cudaGetErrorString(e));
+    mth_destroy(h);
+    return MTH_ERR_CUDA;
+  };
+  cudaError_t e;
+  if ((e = cudaSetDevice(c.device)) != cudaSuccess) { delete h; return MTH_ERR_CUDA; }
+  if ((e = cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking))) return bail("stream", e);
+  if ((e = alloc0(&h->cons, bytes(h, h->NC), h->st))) return bail("cons", e);
+  if ((e = alloc0(&h->prims, bytes(h, h->NP), h->st))) return bail("prims", e);
+  if ((e = alloc0(&h->aux, bytes(h, h->NA), h->st))) return bail("aux", e);
+  if (c.integrator != MTH_SSP2) {
+    if ((e = alloc0(&h->p1cons, bytes(h, h->NC), h->st))) return bail("p1cons", e);
+    if ((e = alloc0(&h->p1prims, bytes(h, h->NP), h->st))) return bail("p1prims", e);
+    if ((e = alloc0(&h->p1aux, bytes(h, h->NA), h->st))) return bail("p1aux", e);
+  } else {
+    for (double** p : {&h->u1, &h->u2, &h->flux1, &h->flux2, &h->src1, &h->src2})
+      if ((e = alloc0(p, bytes(h, h->NC), h->st))) return bail("ssp2", e);
+  }
+  if (c.model == MTH_SRMHD && (e = alloc0(&h->solution, bytes(h, 2), h->st)))
+    return bail("solution", e);
+  if ((e = alloc0(&h->fnet, bytes(h, h->NC), h->st))) return bail("fnet", e);
+  if (!h->fused) {
+    for (double** p : {&h->fplus, &h->fminus, &h->frecon})
+      if ((e = alloc0(p, bytes(h, h->NC), h->st))) return bail("generic", e);
+  }
+  if ((e = cudaMalloc(&h->fail_list, sizeof(int) * (size_t)g.Ntot))) return bail("fails", e);
+  if ((e = cudaMalloc(&h->fail_count, sizeof(int)))) return bail("fails", e);
+  if ((e = cudaMemsetAsync(h->fail_count, 0, sizeof(int), h->st))) return bail("fails", e);
+  if ((e = cudaMalloc(&h->counters, sizeof(long long) * 16))) return bail("counters", e);
+  if ((e = cudaMemsetAsync(h->counters, 0, sizeof(long long) * 16, h->st))) return bail("counters", e);
+  if (c.precision == MTH_MIXED || c.guess == MTH_GUESS_MLP) {
+    if ((e = mixed_init(&h->mixed, g, c.model, h->st))) return bail("mixed", e);
+  }
+  if ((e = cudaStreamSynchronize(h->st))) return bail("sync", e);
+  *out = h;
+  return MTH_OK;
+}
+
+mth_status mth_destroy(mth_handle* h) {
+  if (!h) return MTH_OK;
+  cudaSetDevice(h->device);
+  if (h->st) cudaStreamSynchronize(h->st);
+  for (auto& kv : h->graphs) cudaGraphExecDestroy(kv.second);
+  for (double* p : {h->cons, h->prims, h->aux, h->p1cons, h->p1prims, h->p1aux, h->solution,
+                    h->u1, h->u2, h->flux1, h->flux2, h->src1, h->src2, h->fnet, h->fplus,
+                    h->fminus, h->frecon})
+    if (p) cudaFree(p);
+  if (h->fail_list) cudaFree(h->fail_list);
+  if (h->fail_count) cudaFree(h->fail_count);
+  if (h->counters) cudaFree(h->counters);
+  mixed_free(&h->mixed);
+  if (h->st) cudaStreamDestroy(h->st);
+  delete h;
+  return MTH_OK;
+}
+
+const char* mth_last_error(const mth_handle* h) { return h ? h->err.c_str() : "null handle"; }
+
+mth_status mth_get_dims(const mth_handle* h, int* d) {
+  if (!h || !d) return MTH_ERR_INVALID;
+  d[0] = h->g.Nx; d[1] = h->g.Ny; d[2] = h->g.Nz;
+  d[3] = h->NC; d[4] = h->NP; d[5] = h->NA; d[6] = h->g.dims;
+  return MTH_OK;
+}
+
+mth_status mth_set_prims(mth_handle* h, const double* prims_host) {
+  if (!h || !prims_host) return MTH_ERR_INVALID;
+  CU(h, cudaSetDevice(h->device));
+  CU(h, cudaMemcpyAsync(h->prims, prims_host, bytes(h, h->NP), cudaMemcpyHostToDevice, h->st));
+  CU(h, launch_prims_to_all(h->g, h->cfg.model, h->prims, h->cons, h->aux, h->st));
+  CU(h, launch_apply_bcs(h->g, h->cons, h->NC, h->st));
+  CU(h, launch_apply_bcs(h->g, h->prims, h->NP, h->st));
+  CU(h, launch_apply_bcs(h->g, h->aux, h->NA, h->st));
+  h->t = 0;
+  h->iters = 0;
+  h->ghosts_dirty = false;
+  CU(h, cudaStreamSynchronize(h->st));
+  return MTH_OK;
+}
+
+mth_status mth_upload(mth_handle* h, const double* cons, const double* prims, const double* aux) {
+  if (!h) return MTH_ERR_INVALID;
+  CU(h, cudaSetDevice(h->device));
+  if (cons) CU(h, cudaMemcpyAsync(h->cons, cons, bytes(h, h->NC), cudaMemcpyHostToDevice, h->st));
+  if (prims) CU(h, cudaMemcpyAsync(h->prims, prims, bytes(h, h->NP), cudaMemcpyHostToDevice, h->st));
+  if (aux) CU(h, cudaMemcpyAsync(h->aux, aux, bytes(h, h->NA), cudaMemcpyHostToDevice, h->st));
+  h->ghosts_dirty = false;
+  CU(h, cudaStreamSynchronize(h->st));
+  return MTH_OK;
+}
+
+mth_status mth_apply_bcs(mth_handle* h) {
+  if (!h) return MTH_ERR_INVALID;
+  CU(h, cudaSetDevice(h->device));
+  CU(h, launch_apply_bcs(h->g, h->cons, h->NC, h->st));
+  CU(h, launch_apply_bcs(h->g, h->prims, h->NP, h->st));
+  CU(h, launch_apply_bcs(h->g, h->aux, h->NA, h->st));
+  h->ghosts_dirty = false;
+  return MTH_OK;
+}
+
+mth_status mth_download(mth_handle* h, double* cons, double* prims, double* aux) {
+  if (!h) return MTH_ERR_INVALID;
+  CU(h, cudaSetDevice(h->device));
+  if (h->ghosts_dirty) {
+    mth_status s = mth_apply_bcs(h);
+    if (s != MTH_OK) return s;
+  }
+  if (cons) CU(h, cudaMemcpyAsync(cons, h->cons, bytes(h, h->NC), cudaMemcpyDeviceToHost, h->st));
+  if (prims) CU(h, cudaMemcpyAsync(prims, h->prims, bytes(h, h->NP), cudaMemcpyDeviceToHost, h->st));
+  if (aux) CU(h, cudaMemcpyAsync(aux, h->aux, bytes(h, h->NA), cudaMemcpyDeviceToHost, h->st));
+  CU(h, cudaStreamSynchronize(h->st));
+  return MTH_OK;
+}
+
+mth_status mth_prims_to_all(mth_handle* h) {
+  if (!h) return MTH_ERR_INVALID;
+  CU(h, cudaSetDevice(h->device));
+  CU(h, launch_prims_to_all(h->g, h->cfg.model, h->prims, h->cons, h->aux, h->st));
+  CU(h, cudaStreamSynchronize(h->st));
+  return MTH_OK;
+}
+
+mth_status mth_c2p(mth_handle* h) {
+  if (!h) return MTH_ERR_INVALID;
+  CU(h, cudaSetDevice(h->device));
+  CU(h, c2p(h, h->cons, h->prims, h->aux, h->prims, h->aux));
+  h->ghosts_dirty = true;
+  return read_status(h);
+}
+
+mth_status mth_flux_F(mth_handle* h, double* fnet_host) {
+  if (!h || !fnet_host) return MTH_ERR_INVALID;
+  CU(h, cudaSetDevice(h->device));
+  if (!h->fplus) {
+    for (double** p : {&h->fplus, &h->fminus, &h->frecon})
+      CU(h, alloc0(p, bytes(h, h->NC), h->st));
+  }
+  // FVS::F on the arrays exactly as they are (ghosts included), like the
+  // reference's F, which reads whatever the ghost cells hold.
+  Grid g = h->g;
+  g.bcx = g.bcy = g.bcz = DIM_NONE;  // no remapping: raw ghost values
+  CU(h, cudaMemsetAsync(h->fnet, 0, bytes(h, h->NC), h->st));
+  CU(h, launch_fvs_generic_raw(g, h->cfg.model, h->cfg.weno_order, h->cons, h->prims, h->aux,
+                               h->fplus, h->fminus, h->frecon, h->fnet, h->st));
+  CU(h, cudaMemcpyAsync(fnet_host, h->fnet, bytes(h, h->NC), cudaMemcpyDeviceToHost, h->st));
+  CU(h, cudaStreamSynchronize(h->st));
+  return MTH_OK;
+}
+
+mth_status mth_source(mth_handle* h, double* source_host) {
+  if (!h || !source_host) return MTH_ERR_INVALID;
+  CU(h, cudaSetDevice(h->device));
+  CU(h, cudaMemsetAsync(h->fnet, 0, bytes(h, h->NC), h->st));
+  CU(h, launch_source(h->g, h->cfg.model, h->cons, h->aux, h->fnet, h->st));
+  CU(h, cudaMemcpyAsync(source_host, h->fnet, bytes(h, h->NC), cudaMemcpyDeviceToHost, h->st));
+  CU(h, cudaStreamSynchronize(h->st));
+  return MTH_OK;
+}
+
+mth_status mth_step(mth_handle* h, double dt) {
+  if (!h || !(dt > 0)) return fail(h, MTH_ERR_INVALID, "dt must be positive");
+  CU(h, cudaSetDevice(h->device));
+  h->dt = dt;
+  return launch_step(h, dt);
+}
+
+mth_status mth_update_time(mth_handle* h, int n) {
+  if (!h) return MTH_ERR_INVALID;
+  CU(h, cudaSetDevice(h->device));
+  for (int s = 0; s < n; ++s) {
+    double dt = next_dt(h);
+    h->dt = dt;
+    mth_status st = launch_step(h, dt);
+    if (st != MTH_OK) return st;
+    h->t += dt;
+    h->iters++;
+  }
+  return MTH_OK;
+}
+
+mth_status mth_evolve(mth_handle* h) {
+  if (!h) return MTH_ERR_INVALID;
+  while (h->t < h->cfg.endTime) {
+    mth_status s = mth_update_time(h, 1);
+    if (s != MTH_OK) return s;
+  }
+  return mth_sync(h);
+}
+
+mth_status mth_sync(mth_handle* h) {
+  if (!h) return MTH_ERR_INVALID;
+  CU(h, cudaSetDevice(h->device));
+  return read_status(h);
+}
+
+mth_status mth_get_stats(mth_handle* h, mth_stats* s) {
+  if (!h || !s) return MTH_ERR_INVALID;
+  CU(h, cudaSetDevice(h->device));
+  mth_status st = read_status(h);
+  long long cnt[16];
+  CU(h, cudaMemcpy(cnt, h->counters, sizeof cnt, cudaMemcpyDeviceToHost));
+  s->c2p_cells = cnt[0];
+  s->c2p_evals = cnt[1];
+  s->c2p_unconverged = cnt[2];
+  s->implicit_cells = cnt[4];
+  s->implicit_evals = cnt[5];
+  s->implicit_failed = cnt[6];
+  s->steps = h->steps;
+  s->t = h->t;
+  s->dt = h->dt;
+  s->iters = h->iters;
+  return st;
+}
+
+mth_status mth_reset_stats(mth_handle* h) {
+  if (!h) return MTH_ERR_INVALID;
+  CU(h, cudaSetDevice(h->device));
+  CU(h, cudaMemsetAsync(h->counters, 0, sizeof(long long) * 16, h->st));
+  CU(h, cudaStreamSynchronize(h->st));
+  h->steps = 0;
+  return MTH_OK;
+}
+
+mth_status mth_device_state(mth_handle* h, double** cons, double** prims, double** aux) {
+  if (!h) return MTH_ERR_INVALID;
+  if (cons) *cons = h->cons;
+  if (prims) *prims = h->prims;
+  if (aux) *aux = h->aux;
+  return MTH_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,64 @@
+// Grid description, reference-layout indexing and in-kernel ghost mapping.
+//
+// State lives in HBM in METHOD's own layout, ID(var,i,j,k) =
+// var*Nx*Ny*Nz + i*Ny*Nz + j*Nz + k (Project/CPU/Include/simData.h:10), with
+// Ng ghost cells on each side of every active direction
+// (Project/CPU/Src/simData.cc:65-97).  Kernels never read a ghost cell
+// directly: a ghost index is mapped onto the interior cell that the
+// reference's Bcs::apply would have copied into it (Outflow: nearest
+// interior cell; Periodic: the opposite edge; Flow: periodic in x, outflow in
+// y and z; Project/CPU/Src/boundaryConds.cc:5-145, 449-733).  Because every
+// ghost value of the reference is an exact copy of an interior value, this
+// mapping is bit-identical to materialising the ghosts.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace mth {
+
+enum BcKind : int { BC_OUTFLOW = 0, BC_PERIODIC = 1, BC_FLOW = 2 };
+enum DimBc : int { DIM_NONE = 0, DIM_OUTFLOW = 1, DIM_PERIODIC = 2 };
+
+enum StageMode : int {
+  STAGE_FNET = 0,      // out = fnet (FVS::F)
+  STAGE_EULER = 1,     // out = in - dt * fnet (RK2 predictor, RK2.cc:58-66)
+  STAGE_RK2_CORR = 2,  // out = 0.5 * (u0 + in - dt * fnet) (RK2.cc:81-89)
+};
+
+struct Grid {
+  int nx, ny, nz;        // interior cells (reference Data::nx..nz; 0 for inactive)
+  int Nx, Ny, Nz;        // ghost-inclusive extents
+  int Ng, dims;
+  int is, ie, js, je, ks, ke;
+  int bcx, bcy, bcz;     // DimBc per direction
+  double dx, dy, dz;
+  double gamma, sigma, cp;
+  long long Ntot;        // Nx*Ny*Nz
+};
+
+__host__ __device__ inline long long cell_id(const Grid& g, int i, int j, int k) {
+  return ((long long)i * g.Ny + j) * g.Nz + k;
+}
+
+// Maps an index of one direction onto the interior cell whose value the
+// reference's boundary pass would have copied there.
+__host__ __device__ inline int map_dim(int i, int n, int Ng, int kind) {
+  if (kind == DIM_PERIODIC) {
+    if (i < Ng) return i + n;
+    if (i >= n + Ng) return i - n;
+    return i;
+  }
+  if (kind == DIM_OUTFLOW) {
+    if (i < Ng) return Ng;
+    if (i > n + Ng - 1) return n + Ng - 1;
+    return i;
+  }
+  return i;
+}
+
+__host__ __device__ inline long long mapped_cell(const Grid& g, int i, int j, int k) {
+  return cell_id(g, map_dim(i, g.nx, g.Ng, g.bcx), map_dim(j, g.ny, g.Ng, g.bcy),
+                 map_dim(k, g.nz, g.Ng, g.bcz));
+}
+
+}  // namespace mth

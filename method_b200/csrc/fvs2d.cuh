@@ -1,0 +1,174 @@
+// Fused 2D flux-vector-splitting stage kernel.
+//
+// One CTA owns a TI x 32 tile of interior cells (32 consecutive j per warp, the
+// contiguous direction of METHOD's layout).  For each direction it
+//   1. loads the tile plus a halo of H cells along that direction, mapping
+//      ghost indices onto the interior (in-kernel boundary conditions),
+//   2. evaluates Model::fluxVector and the Lax-Friedrichs split
+//      f+- = 0.5 (f +- U) (Project/CPU/Src/fluxVectorSplitting.cc:22-33) into
+//      shared memory,
+//   3. reconstructs every face with WENO upwind(f+) + downwind(f-)
+//      (fluxVectorSplitting.cc:36-49, weno.cc:123-228),
+//   4. forms fnet = (fx[i+1]/dx - fx[i]/dx) + (fy[j+1]/dy - fy[j]/dy)
+//      (fluxVectorSplitting.cc:105-111) in registers,
+// and finally applies the Runge-Kutta stage update to its own cells, so a
+// stage reads each state array once and writes the new conserved state once.
+//
+// `R` is the arithmetic type of flux, split and reconstruction: double in the
+// plain form (compiled without FMA, bit-identical to the reference), float in
+// the mixed form.  The conserved-state update is always FP64.
+#pragma once
+#include "common.cuh"
+#include "weno.cuh"
+
+namespace mth {
+
+template <int ORDER, typename R>
+__device__ __forceinline__ R weno_face(const R* p, const R* m, int stride, int base) {
+  // p, m point at the first stencil cell of the region column; `base` is the
+  // region index of cell i-H for face i (face between cells i-1 and i).
+  if constexpr (ORDER == 3) {
+    // upwind cells i-2, i-1, i ; downwind cells i+1, i, i-1 (weno.cc:123-164)
+    if constexpr (sizeof(R) == 8) {
+      return weno3_exact(p[(base + 0) * stride], p[(base + 1) * stride], p[(base + 2) * stride]) +
+             weno3_exact(m[(base + 3) * stride], m[(base + 2) * stride], m[(base + 1) * stride]);
+    } else {
+      return weno3_fast(p[(base + 0) * stride], p[(base + 1) * stride], p[(base + 2) * stride]) +
+             weno3_fast(m[(base + 3) * stride], m[(base + 2) * stride], m[(base + 1) * stride]);
+    }
+  } else {
+    // upwind cells i-3 .. i+1 ; downwind cells i+2 .. i-2 (weno.cc:175-228)
+    if constexpr (sizeof(R) == 8) {
+      return weno5_exact(p[(base + 0) * stride], p[(base + 1) * stride], p[(base + 2) * stride],
+                         p[(base + 3) * stride], p[(base + 4) * stride]) +
+             weno5_exact(m[(base + 5) * stride], m[(base + 4) * stride], m[(base + 3) * stride],
+                         m[(base + 2) * stride], m[(base + 1) * stride]);
+    } else {
+      return weno5_fast(p[(base + 0) * stride], p[(base + 1) * stride], p[(base + 2) * stride],
+                        p[(base + 3) * stride], p[(base + 4) * stride]) +
+             weno5_fast(m[(base + 5) * stride], m[(base + 4) * stride], m[(base + 3) * stride],
+                        m[(base + 2) * stride], m[(base + 1) * stride]);
+    }
+  }
+}
+
+template <int ORDER>
+struct Halo {
+  static constexpr int H = (ORDER == 3) ? 2 : 3;
+};
+
+template <class M, typename R, int ORDER, int TI>
+struct Fvs2dSmem {
+  static constexpr int TJ = 32;
+  static constexpr int H = Halo<ORDER>::H;
+  static constexpr int RX = (TI + 2 * H) * TJ;
+  static constexpr int RY = TI * (TJ + 2 * H);
+  static constexpr int RMAX = RX > RY ? RX : RY;
+  static constexpr int FX = (TI + 1) * TJ;
+  static constexpr int FY = TI * (TJ + 1);
+  static constexpr int FMAX = FX > FY ? FX : FY;
+  static constexpr size_t bytes = sizeof(R) * (size_t)M::NC * (2 * RMAX + FMAX);
+};
+
+// Loads one cell's flux inputs (in R) and writes f+ and f- of direction `dir`.
+template <class M, typename R>
+__device__ __forceinline__ void split_cell(const Grid& g, const double* __restrict__ cons,
+                                           const double* __restrict__ prims,
+                                           const double* __restrict__ aux, long long cell, int dir,
+                                           R* sp, R* sm, int stride) {
+  R c[M::NC], p[M::NP], a[M::NA];
+  M::template load_flux_inputs<R>(cons, prims, aux, g.Ntot, cell, c, p, a);
+  R f[M::NC];
+  M::template flux<R>(c, p, a, dir, f);
+#pragma unroll
+  for (int v = 0; v < M::NC; ++v) {
+    sp[v * stride] = R(0.5) * (f[v] + c[v]);
+    sm[v * stride] = R(0.5) * (f[v] - c[v]);
+  }
+}
+
+template <class M, typename R, int ORDER, int TI>
+__global__ void __launch_bounds__(32 * TI)
+    k_fvs2d(Grid g, const double* __restrict__ cons, const double* __restrict__ prims,
+            const double* __restrict__ aux, const double* u0, double* out, double dt,
+            int mode) {
+  using S = Fvs2dSmem<M, R, ORDER, TI>;
+  constexpr int NC = M::NC, TJ = S::TJ, H = S::H, NT = 32 * TI;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  R* sp = reinterpret_cast<R*>(smem_raw);
+  R* sm = sp + NC * S::RMAX;
+  R* sr = sm + NC * S::RMAX;
+
+  const int lane = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + lane;
+  const int i0 = g.is + blockIdx.y * TI, j0 = g.js + blockIdx.x * TJ;
+  const int ci = i0 + ty, cj = j0 + lane;
+  R acc[NC];
+
+  // ---------------- x direction ----------------
+  for (int e = tid; e < S::RX; e += NT) {
+    int r = e / TJ, c = e - r * TJ;
+    int gi = min(i0 - H + r, g.ie - 1 + H);
+    int gj = min(j0 + c, g.je - 1);
+    split_cell<M, R>(g, cons, prims, aux, mapped_cell(g, gi, gj, 0), 0, sp + e, sm + e, S::RX);
+  }
+  __syncthreads();
+  for (int e = tid; e < NC * S::FX; e += NT) {
+    int v = e / S::FX, rem = e - v * S::FX;
+    int fi = rem / TJ, c = rem - fi * TJ;
+    const R* P = sp + v * S::RX + c;
+    const R* Mm = sm + v * S::RX + c;
+    // face i0+fi: cell i-H sits at region row fi
+    sr[v * S::FX + rem] = weno_face<ORDER, R>(P, Mm, TJ, fi + H - (ORDER == 3 ? 2 : 3));
+  }
+  __syncthreads();
+  {
+    const R dx = R(g.dx);
+#pragma unroll
+    for (int v = 0; v < NC; ++v)
+      acc[v] = sr[v * S::FX + (ty + 1) * TJ + lane] / dx - sr[v * S::FX + ty * TJ + lane] / dx;
+  }
+  __syncthreads();
+
+  // ---------------- y direction ----------------
+  constexpr int WY = TJ + 2 * H;
+  for (int e = tid; e < S::RY; e += NT) {
+    int r = e / WY, c = e - r * WY;
+    int gi = min(i0 + r, g.ie - 1);
+    int gj = min(j0 - H + c, g.je - 1 + H);
+    split_cell<M, R>(g, cons, prims, aux, mapped_cell(g, gi, gj, 0), 1, sp + e, sm + e, S::RY);
+  }
+  __syncthreads();
+  for (int e = tid; e < NC * S::FY; e += NT) {
+    int v = e / S::FY, rem = e - v * S::FY;
+    int r = rem / (TJ + 1), fj = rem - r * (TJ + 1);
+    const R* P = sp + v * S::RY + r * WY;
+    const R* Mm = sm + v * S::RY + r * WY;
+    sr[v * S::FY + rem] = weno_face<ORDER, R>(P, Mm, 1, fj + H - (ORDER == 3 ? 2 : 3));
+  }
+  __syncthreads();
+  if (ci >= g.ie || cj >= g.je) return;
+  {
+    const R dy = R(g.dy);
+#pragma unroll
+    for (int v = 0; v < NC; ++v)
+      acc[v] = acc[v] + (sr[v * S::FY + ty * (TJ + 1) + lane + 1] / dy -
+                         sr[v * S::FY + ty * (TJ + 1) + lane] / dy);
+  }
+
+  // ---------------- stage update ----------------
+  const long long cell = cell_id(g, ci, cj, 0);
+#pragma unroll
+  for (int v = 0; v < NC; ++v) {
+    const long long o = (long long)v * g.Ntot + cell;
+    const double fn = (double)acc[v];
+    if (mode == STAGE_FNET) {
+      out[o] = fn;
+    } else if (mode == STAGE_EULER) {
+      out[o] = cons[o] - dt * fn;
+    } else {
+      out[o] = 0.5 * (u0[o] + cons[o] - dt * fn);
+    }
+  }
+}
+
+}  // namespace mth

@@ -1,0 +1,666 @@
+// Plain FP64 kernels.  This translation unit is compiled with -fmad=false
+// (and IEEE division / square root, the nvcc defaults) so that every
+// expression rounds exactly like the reference's x86-64 build, which has no
+// FMA contraction at the default -march.
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+#include "fvs2d.cuh"
+#include "launch.h"
+#include "minpack.cuh"
+#include "srmhd.cuh"
+#include "srrmhd.cuh"
+
+namespace mth {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+inline int blocks_for(long long n, int t = kThreads) { return (int)((n + t - 1) / t); }
+
+__device__ __forceinline__ void interior_ijk(const Grid& g, long long t, int& i, int& j, int& k) {
+  const int nk = g.ke - g.ks, nj = g.je - g.js;
+  k = g.ks + (int)(t % nk);
+  t /= nk;
+  j = g.js + (int)(t % nj);
+  i = g.is + (int)(t / nj);
+}
+
+__device__ __forceinline__ long long n_interior(const Grid& g) {
+  return (long long)(g.ie - g.is) * (g.je - g.js) * (g.ke - g.ks);
+}
+
+// ---------------------------------------------------------------------------
+// primsToAll over every cell (srmhd.cc:573-673, srrmhd.cc:358-510).
+__global__ void k_prims_to_all_srmhd(Grid g, const double* __restrict__ prims,
+                                     double* __restrict__ cons, double* __restrict__ aux) {
+  long long cell = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (cell >= g.Ntot) return;
+  const long long N = g.Ntot;
+  double p[8], c[9], a[13];
+#pragma unroll
+  for (int v = 0; v < 8; ++v) p[v] = prims[v * N + cell];
+  srmhd::prims_to_all(p, g.gamma, c, a);
+#pragma unroll
+  for (int v = 0; v < 9; ++v) cons[v * N + cell] = c[v];
+#pragma unroll
+  for (int v = 0; v < 13; ++v) aux[v * N + cell] = a[v];
+}
+
+// ---------------------------------------------------------------------------
+// Boundary conditions: every ghost cell receives the interior value it maps
+// to.  Sources are always interior cells, so one pass is race free.
+__global__ void k_apply_bcs(Grid g, double* __restrict__ arr, int nvars) {
+  long long cell = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (cell >= g.Ntot) return;
+  int k = (int)(cell % g.Nz);
+  long long t = cell / g.Nz;
+  int j = (int)(t % g.Ny);
+  int i = (int)(t / g.Ny);
+  bool ghost = (i < g.is || i >= g.ie) || (g.dims > 1 && (j < g.js || j >= g.je)) ||
+               (g.dims > 2 && (k < g.ks || k >= g.ke));
+  if (!ghost) return;
+  long long src = mapped_cell(g, i, j, k);
+  for (int v = 0; v < nvars; ++v) arr[v * g.Ntot + cell] = arr[v * g.Ntot + src];
+}
+
+// ---------------------------------------------------------------------------
+// Generic flux path, one direction at a time, on materialised ghosts.  Mirrors
+// FVS::fluxReconstruction and FVS::F (fluxVectorSplitting.cc:4-131).
+// Flux vector and Lax-Friedrichs split of one direction over every cell.
+template <class M>
+__global__ void k_split_dir_full(Grid g, const double* __restrict__ cons,
+                                 const double* __restrict__ prims,
+                                 const double* __restrict__ aux, int dir,
+                                 double* __restrict__ fplus, double* __restrict__ fminus) {
+  long long cell = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (cell >= g.Ntot) return;
+  double c[M::NC], p[M::NP], a[M::NA], f[M::NC];
+  M::template load_flux_inputs<double>(cons, prims, aux, g.Ntot, cell, c, p, a);
+  M::template flux<double>(c, p, a, dir, f);
+#pragma unroll
+  for (int v = 0; v < M::NC; ++v) {
+    fplus[v * g.Ntot + cell] = 0.5 * (f[v] + 1.0 * c[v]);
+    fminus[v * g.Ntot + cell] = 0.5 * (f[v] - 1.0 * c[v]);
+  }
+}
+
+__global__ void k_weno_dir(Grid g, int nc, int order, int dir, const double* __restrict__ fplus,
+                           const double* __restrict__ fminus, double* __restrict__ frecon) {
+  long long cell = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (cell >= g.Ntot) return;
+  int k = (int)(cell % g.Nz);
+  long long t = cell / g.Nz;
+  int j = (int)(t % g.Ny);
+  int i = (int)(t / g.Ny);
+  const int shift = (order + 1) / 2;
+  int idx = dir == 0 ? i : (dir == 1 ? j : k);
+  int n = dir == 0 ? g.Nx : (dir == 1 ? g.Ny : g.Nz);
+  long long stride = dir == 0 ? (long long)g.Ny * g.Nz : (dir == 1 ? g.Nz : 1);
+  for (int v = 0; v < nc; ++v) {
+    double r = 0.0;  // the reference zero-initialises its reconstruction arrays
+    if (idx >= shift && idx < n - shift) {
+      const double* P = fplus + v * g.Ntot + cell;
+      const double* Mm = fminus + v * g.Ntot + cell;
+      double up, dn;
+      if (order == 3) {
+        up = weno3_exact(P[-2 * stride], P[-1 * stride], P[0]);
+        dn = weno3_exact(Mm[1 * stride], Mm[0], Mm[-1 * stride]);
+      } else {
+        up = weno5_exact(P[-3 * stride], P[-2 * stride], P[-1 * stride], P[0], P[1 * stride]);
+        dn = weno5_exact(Mm[2 * stride], Mm[1 * stride], Mm[0], Mm[-1 * stride],
+                         Mm[-2 * stride]);
+      }
+      r = up + dn;
+    } else {
+      r = 0.0 + 0.0;
+    }
+    frecon[v * g.Ntot + cell] = r;
+  }
+}
+
+__global__ void k_fnet_dir(Grid g, int nc, int dir, int first, const double* __restrict__ frecon,
+                           double* __restrict__ fnet) {
+  long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= n_interior(g)) return;
+  int i, j, k;
+  interior_ijk(g, t, i, j, k);
+  const long long cell = cell_id(g, i, j, k);
+  const long long nb = dir == 0 ? cell_id(g, i + 1, j, k)
+                                : (dir == 1 ? cell_id(g, i, j + 1, k) : cell_id(g, i, j, k + 1));
+  const double d = dir == 0 ? g.dx : (dir == 1 ? g.dy : g.dz);
+  for (int v = 0; v < nc; ++v) {
+    const double* F = frecon + v * g.Ntot;
+    double val = F[nb] / d - F[cell] / d;
+    fnet[v * g.Ntot + cell] = first ? val : fnet[v * g.Ntot + cell] + val;
+  }
+}
+
+__global__ void k_stage_update(Grid g, int nc, int mode, const double* u0,
+                               const double* in, const double* __restrict__ fnet, double dt,
+                               double* out) {
+  long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= n_interior(g)) return;
+  int i, j, k;
+  interior_ijk(g, t, i, j, k);
+  const long long cell = cell_id(g, i, j, k);
+  for (int v = 0; v < nc; ++v) {
+    const long long o = v * g.Ntot + cell;
+    if (mode == STAGE_EULER) out[o] = in[o] - dt * fnet[o];
+    else if (mode == STAGE_RK2_CORR) out[o] = 0.5 * (u0[o] + in[o] - dt * fnet[o]);
+    else out[o] = fnet[o];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// SRMHD primitive recovery (srmhd.cc:390-562): one Powell-hybrid solve per
+// interior cell from the previous state's guess; cells that fail are queued
+// for the neighbour-average retry.
+constexpr double kSrmhdTol = 1.49011612e-7;
+
+__global__ void __launch_bounds__(128)
+    k_c2p_srmhd(Grid g, const double* __restrict__ cons, const double* prims_guess,
+                const double* aux_guess, double* prims, double* aux,
+                double* __restrict__ solution, C2PWork w) {
+  long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  long long nfev = 0;
+  if (t < n_interior(g)) {
+    int i, j, k;
+    interior_ijk(g, t, i, j, k);
+    const long long N = g.Ntot, cell = cell_id(g, i, j, k);
+    double c[9];
+#pragma unroll
+    for (int v = 0; v < 9; ++v) c[v] = cons[v * N + cell];
+    double pg[4];
+#pragma unroll
+    for (int v = 0; v < 4; ++v) pg[v] = prims_guess[v * N + cell];
+    double hg = aux_guess[cell];
+    srmhd::Residual R = srmhd::residual_args(c, g.gamma);
+    double x[2], fv[2];
+    srmhd::guess_from_prims(pg, hg, x);
+    HybrdResult res = Hybrd<2>::solve(R, x, fv, kSrmhdTol);
+    nfev = res.nfev;
+    if (res.info == 1) {
+      solution[cell] = x[0];
+      solution[N + cell] = x[1];
+      double p[8], a[13];
+      srmhd::from_solution(c, x, g.gamma, R.BS, R.Bsq, R.Ssq, p, a);
+#pragma unroll
+      for (int v = 0; v < 8; ++v) prims[v * N + cell] = p[v];
+#pragma unroll
+      for (int v = 0; v < 13; ++v) aux[v * N + cell] = a[v];
+    } else {
+      prims[5 * N + cell] = c[5];
+      prims[6 * N + cell] = c[6];
+      prims[7 * N + cell] = c[7];
+      aux[10 * N + cell] = R.BS;
+      aux[11 * N + cell] = R.Bsq;
+      aux[12 * N + cell] = R.Ssq;
+      int slot = atomicAdd(w.fail_count, 1);
+      w.fail_list[slot] = (int)cell;
+    }
+  }
+  // one atomic per warp for the statistics
+  unsigned mask = __ballot_sync(0xffffffffu, t < n_interior(g));
+  for (int o = 16; o > 0; o >>= 1) nfev += __shfl_down_sync(0xffffffffu, nfev, o);
+  if ((threadIdx.x & 31) == 0 && mask) {
+    atomicAdd((unsigned long long*)&w.counters[0], (unsigned long long)__popc(mask));
+    atomicAdd((unsigned long long*)&w.counters[1], (unsigned long long)nfev);
+  }
+}
+
+// Neighbour-average retry of failed cells (srmhd.cc:458-507), processed one
+// at a time in (i, j, k) order as the reference does.  The reference solves
+// the retry with the residual arguments left over from the last interior cell
+// of the first pass; that behaviour is kept so that results stay identical.
+__global__ void k_c2p_retry_srmhd(Grid g, const double* __restrict__ cons, double* prims,
+                                  double* aux, double* solution, C2PWork w) {
+  if (threadIdx.x != 0) return;
+  const int n = *w.fail_count;
+  if (n == 0) return;
+  int* L = w.fail_list;
+  // heap sort of the failed cell ids (ascending = the reference's loop order)
+  for (int s = n / 2 - 1; s >= 0; --s) {
+    for (int r = s;;) {
+      int ch = 2 * r + 1;
+      if (ch >= n) break;
+      if (ch + 1 < n && L[ch + 1] > L[ch]) ++ch;
+      if (L[r] >= L[ch]) break;
+      int tmp = L[r]; L[r] = L[ch]; L[ch] = tmp;
+      r = ch;
+    }
+  }
+  for (int end = n - 1; end > 0; --end) {
+    int tmp = L[0]; L[0] = L[end]; L[end] = tmp;
+    for (int r = 0;;) {
+      int ch = 2 * r + 1;
+      if (ch >= end) break;
+      if (ch + 1 < end && L[ch + 1] > L[ch]) ++ch;
+      if (L[r] >= L[ch]) break;
+      int t2 = L[r]; L[r] = L[ch]; L[ch] = t2;
+      r = ch;
+    }
+  }
+  const long long N = g.Ntot;
+  double cl[9];
+  const long long last = cell_id(g, g.ie - 1, g.je - 1, g.ke - 1);
+  for (int v = 0; v < 9; ++v) cl[v] = cons[v * N + last];
+  srmhd::Residual R = srmhd::residual_args(cl, g.gamma);
+  long long still = 0, nfev = 0;
+  for (int f = 0; f < n; ++f) {
+    const long long cell = L[f];
+    const int z = (int)(cell % g.Nz);
+    const int y = (int)((cell / g.Nz) % g.Ny);
+    const int x = (int)(cell / ((long long)g.Nz * g.Ny));
+    long long nb[6];
+    int cnt = 0;
+    if (x > 0) nb[cnt++] = cell_id(g, x - 1, y, z);
+    if (y > 0) nb[cnt++] = cell_id(g, x, y - 1, z);
+    if (z > 0) nb[cnt++] = cell_id(g, x, y, z - 1);
+    if (x < g.Nx - 1) nb[cnt++] = cell_id(g, x + 1, y, z);
+    if (y < g.Ny - 1) nb[cnt++] = cell_id(g, x, y + 1, z);
+    if (z < g.Nz - 1) nb[cnt++] = cell_id(g, x, y, z + 1);
+    double s[2] = {0, 0};
+    for (int q = 0; q < cnt; ++q) {
+      s[0] += solution[nb[q]];
+      s[1] += solution[N + nb[q]];
+    }
+    s[0] /= (double)cnt;
+    s[1] /= (double)cnt;
+    double fv[2];
+    HybrdResult res = Hybrd<2>::solve(R, s, fv, kSrmhdTol);
+    nfev += res.nfev;
+    if (res.info != 1) ++still;
+    solution[cell] = s[0];
+    solution[N + cell] = s[1];
+    double c[9];
+    for (int v = 0; v < 9; ++v) c[v] = cons[v * N + cell];
+    double p[8], a[13];
+    srmhd::from_solution(c, s, g.gamma, aux[10 * N + cell], aux[11 * N + cell],
+                         aux[12 * N + cell], p, a);
+    for (int v = 0; v < 8; ++v) prims[v * N + cell] = p[v];
+    for (int v = 0; v < 13; ++v) aux[v * N + cell] = a[v];
+  }
+  w.counters[1] += nfev;
+  w.counters[2] += still;
+  *w.fail_count = 0;
+}
+
+// RKSplit source step: target += dt * S(cons) on the interior (rkSplit.cc:31-53).
+template <int MODEL>
+__global__ void k_source_add(Grid g, const double* __restrict__ cons,
+                             const double* __restrict__ prims, const double* __restrict__ aux,
+                             double* target, double dt) {
+  long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= n_interior(g)) return;
+  int i, j, k;
+  interior_ijk(g, t, i, j, k);
+  const long long N = g.Ntot, cell = cell_id(g, i, j, k);
+  if (MODEL == MODEL_SRMHD) {
+    double c[9], s[9];
+#pragma unroll
+    for (int v = 0; v < 9; ++v) c[v] = cons[v * N + cell];
+    srmhd::source(c, g.cp, s);
+#pragma unroll
+    for (int v = 0; v < 9; ++v) target[v * N + cell] = target[v * N + cell] + dt * s[v];
+  } else {
+    double c[14], a[17], s[14];
+#pragma unroll
+    for (int v = 0; v < 14; ++v) c[v] = cons[v * N + cell];
+#pragma unroll
+    for (int v = 0; v < 17; ++v) a[v] = aux[v * N + cell];
+    srrmhd::source(c, a, g.cp, s);
+#pragma unroll
+    for (int v = 0; v < 14; ++v) target[v * N + cell] = target[v * N + cell] + dt * s[v];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// SRRMHD primsToAll with the 4th-order central-difference charge density
+// (srrmhd.cc:358-510); the stencil reads the input primitives of neighbours.
+__global__ void k_prims_to_all_srrmhd(Grid g, const double* __restrict__ prims,
+                                      double* __restrict__ cons, double* __restrict__ aux) {
+  long long cell = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (cell >= g.Ntot) return;
+  const long long N = g.Ntot;
+  const int k = (int)(cell % g.Nz);
+  const int j = (int)((cell / g.Nz) % g.Ny);
+  const int i = (int)(cell / ((long long)g.Nz * g.Ny));
+  double p[11], c[14], a[17];
+#pragma unroll
+  for (int v = 0; v < 11; ++v) p[v] = prims[v * N + cell];
+  auto P = [&](int v, int ii, int jj, int kk) { return prims[v * N + cell_id(g, ii, jj, kk)]; };
+  bool qfd = true;
+  double divE = 0.0;
+  if (i > 1 && j > 1 && k > 1 && i < g.Nx - 2 && j < g.Ny - 2 && k < g.Nz - 2) {
+    divE = (-P(8, i + 2, j, k) + 8 * P(8, i + 1, j, k) - 8 * P(8, i - 1, j, k) + P(8, i - 2, j, k)) /
+               (12 * g.dx) +
+           (-P(9, i, j + 2, k) + 8 * P(9, i, j + 1, k) - 8 * P(9, i, j - 1, k) + P(9, i, j - 2, k)) /
+               (12 * g.dy) +
+           (-P(10, i, j, k + 2) + 8 * P(10, i, j, k + 1) - 8 * P(10, i, j, k - 1) +
+            P(10, i, j, k - 2)) /
+               (12 * g.dz);
+  } else if (i > 1 && j > 1 && i < g.Nx - 2 && j < g.Ny - 2 && g.nz == 0) {
+    divE = (-P(8, i + 2, j, k) + 8 * P(8, i + 1, j, k) - 8 * P(8, i - 1, j, k) + P(8, i - 2, j, k)) /
+               (12 * g.dx) +
+           (-P(9, i, j + 2, k) + 8 * P(9, i, j + 1, k) - 8 * P(9, i, j - 1, k) + P(9, i, j - 2, k)) /
+               (12 * g.dy);
+  } else if (i > 1 && i < g.Nx - 2 && g.ny == 0) {
+    divE = (-P(8, i + 2, j, k) + 8 * P(8, i + 1, j, k) - 8 * P(8, i - 1, j, k) + P(8, i - 2, j, k)) /
+           (12 * g.dx);
+  } else {
+    qfd = false;
+  }
+  srrmhd::prims_to_all(p, g.gamma, g.sigma, qfd, divE, c, a);
+#pragma unroll
+  for (int v = 0; v < 14; ++v) cons[v * N + cell] = c[v];
+#pragma unroll
+  for (int v = 0; v < 17; ++v) aux[v * N + cell] = a[v];
+}
+
+// SRRMHD grid primitive recovery (srrmhd.cc:314-356): secant on Z per
+// interior cell, seeded from the guess array's aux[10].
+__global__ void __launch_bounds__(128)
+    k_c2p_srrmhd(Grid g, const double* __restrict__ cons, const double* aux_guess, double* prims,
+                 double* aux, C2PWork w) {
+  long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  long long evals = 0;
+  if (t < n_interior(g)) {
+    int i, j, k;
+    interior_ijk(g, t, i, j, k);
+    const long long N = g.Ntot, cell = cell_id(g, i, j, k);
+    double c[14], p[11], a[17];
+#pragma unroll
+    for (int v = 0; v < 14; ++v) c[v] = cons[v * N + cell];
+    a[10] = aux_guess[10 * N + cell];
+    int ev = 0;
+    bool ok = srrmhd::c2p_cell(c, g.gamma, g.sigma, p, a, ev);
+    evals = ev;
+    if (ok) {
+#pragma unroll
+      for (int v = 0; v < 11; ++v) prims[v * N + cell] = p[v];
+#pragma unroll
+      for (int v = 0; v < 17; ++v) aux[v * N + cell] = a[v];
+    } else {
+      atomicAdd((unsigned long long*)&w.counters[2], 1ull);
+      atomicOr((unsigned long long*)&w.counters[3], (unsigned long long)ERR_C2P);
+    }
+  }
+  unsigned mask = __ballot_sync(0xffffffffu, t < n_interior(g));
+  for (int o = 16; o > 0; o >>= 1) evals += __shfl_down_sync(0xffffffffu, evals, o);
+  if ((threadIdx.x & 31) == 0 && mask) {
+    atomicAdd((unsigned long long*)&w.counters[0], (unsigned long long)__popc(mask));
+    atomicAdd((unsigned long long*)&w.counters[1], (unsigned long long)evals);
+  }
+}
+
+// Model::sourceTerm into an interior array.
+template <int MODEL>
+__global__ void k_source(Grid g, const double* __restrict__ cons, const double* __restrict__ aux,
+                         double* __restrict__ out) {
+  long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= n_interior(g)) return;
+  int i, j, k;
+  interior_ijk(g, t, i, j, k);
+  const long long N = g.Ntot, cell = cell_id(g, i, j, k);
+  if (MODEL == MODEL_SRMHD) {
+    double c[9], s[9];
+#pragma unroll
+    for (int v = 0; v < 9; ++v) c[v] = cons[v * N + cell];
+    srmhd::source(c, g.cp, s);
+#pragma unroll
+    for (int v = 0; v < 9; ++v) out[v * N + cell] = s[v];
+  } else {
+    double c[14], a[17], s[14];
+#pragma unroll
+    for (int v = 0; v < 14; ++v) c[v] = cons[v * N + cell];
+#pragma unroll
+    for (int v = 0; v < 17; ++v) a[v] = aux[v * N + cell];
+    srrmhd::source(c, a, g.cp, s);
+#pragma unroll
+    for (int v = 0; v < 14; ++v) out[v * N + cell] = s[v];
+  }
+}
+
+// One implicit SSP2(222) stage per interior cell: a 14-unknown Powell-hybrid
+// solve whose residual runs the secant C2P and the source (SSP2.cc:72-148).
+constexpr double kImexTol = 0.000000149011612;
+// The reference's SSP2 assigns IMEX2Arguments(data) to its member, but
+// IMEX2Arguments::operator= (IMEX2Args.cc:34-63) does not copy gam / om2gam,
+// so the constants in effect are those of the default constructor
+// (IMEX2Args.h:35-37): om2gam = 0.4142135623730950, one ulp above the
+// parameterised constructor's 0.4142135623730949.
+constexpr double kImexGam = 0.2928932188134525;
+constexpr double kImexOm2Gam = 0.4142135623730950;
+
+template <int STAGE>
+__global__ void __launch_bounds__(64)
+    k_imex_stage(Grid g, const double* __restrict__ cons, const double* __restrict__ aux_guess,
+                 const double* __restrict__ u1, const double* __restrict__ flux1,
+                 const double* __restrict__ source1, double* __restrict__ out, double dt,
+                 C2PWork w) {
+  long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  long long evals = 0;
+  if (t < n_interior(g)) {
+    int i, j, k;
+    interior_ijk(g, t, i, j, k);
+    const long long N = g.Ntot, cell = cell_id(g, i, j, k);
+    double u[14], f1[14], s1[14], x[14], fv[14];
+#pragma unroll
+    for (int v = 0; v < 14; ++v) u[v] = cons[v * N + cell];
+    if (STAGE == 1) {
+#pragma unroll
+      for (int v = 0; v < 14; ++v) x[v] = u[v];
+    } else {
+#pragma unroll
+      for (int v = 0; v < 14; ++v) {
+        f1[v] = flux1[v * N + cell];
+        s1[v] = source1[v * N + cell];
+        x[v] = 0.5 * (u[v] + u1[v * N + cell] - dt * f1[v]);
+      }
+    }
+    srrmhd::ImexResidual R;
+    R.u = u;
+    R.flux1 = f1;
+    R.source1 = s1;
+    R.dt = dt;
+    R.gam = kImexGam;
+    R.om2gam = kImexOm2Gam;
+    R.g = g.gamma;
+    R.sigma = g.sigma;
+    R.cp = g.cp;
+    R.Z = aux_guess[10 * N + cell];
+    R.stage = STAGE;
+    R.evals = 0;
+    HybrdResult res = Hybrd<14>::solve(R, x, fv, kImexTol);
+    evals = res.nfev;
+#pragma unroll
+    for (int v = 0; v < 14; ++v) out[v * N + cell] = x[v];
+    if (res.info != 1) {
+      atomicAdd((unsigned long long*)&w.counters[2], 1ull);
+      atomicOr((unsigned long long*)&w.counters[3], (unsigned long long)ERR_IMPLICIT);
+    }
+  }
+  unsigned mask = __ballot_sync(0xffffffffu, t < n_interior(g));
+  for (int o = 16; o > 0; o >>= 1) evals += __shfl_down_sync(0xffffffffu, evals, o);
+  if ((threadIdx.x & 31) == 0 && mask) {
+    atomicAdd((unsigned long long*)&w.counters[0], (unsigned long long)__popc(mask));
+    atomicAdd((unsigned long long*)&w.counters[1], (unsigned long long)evals);
+  }
+}
+
+// SSP2 combination U += -0.5 dt (flux1 + flux2 - source1 - source2)
+// (SSP2.cc:155-166).
+__global__ void k_ssp2_combine(Grid g, int nc, double* cons, const double* __restrict__ flux1,
+                               const double* __restrict__ flux2,
+                               const double* __restrict__ source1,
+                               const double* __restrict__ source2, double dt) {
+  long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= n_interior(g)) return;
+  int i, j, k;
+  interior_ijk(g, t, i, j, k);
+  const long long cell = cell_id(g, i, j, k);
+  for (int v = 0; v < nc; ++v) {
+    const long long o = v * g.Ntot + cell;
+    cons[o] += -0.5 * dt * (flux1[o] + flux2[o] - source1[o] - source2[o]);
+  }
+}
+
+template <class M, int ORDER, int TI>
+cudaError_t fvs2d_instance(const Grid& g, const double* cons, const double* prims,
+                           const double* aux, const double* u0, double* out, double dt, int mode,
+                           cudaStream_t st) {
+  using S = Fvs2dSmem<M, double, ORDER, TI>;
+  auto kern = k_fvs2d<M, double, ORDER, TI>;
+  static bool configured = false;
+  if (!configured) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)S::bytes);
+    if (e != cudaSuccess) return e;
+    configured = true;
+  }
+  dim3 grid((g.je - g.js + 31) / 32, (g.ie - g.is + TI - 1) / TI);
+  dim3 block(32, TI);
+  kern<<<grid, block, S::bytes, st>>>(g, cons, prims, aux, u0, out, dt, mode);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+cudaError_t launch_prims_to_all(const Grid& g, int model, const double* prims, double* cons,
+                                double* aux, cudaStream_t st) {
+  if (model == MODEL_SRMHD) {
+    k_prims_to_all_srmhd<<<blocks_for(g.Ntot), kThreads, 0, st>>>(g, prims, cons, aux);
+    return cudaGetLastError();
+  }
+  return launch_prims_to_all_srrmhd(g, prims, cons, aux, st);
+}
+
+cudaError_t launch_apply_bcs(const Grid& g, double* arr, int nvars, cudaStream_t st) {
+  k_apply_bcs<<<blocks_for(g.Ntot), kThreads, 0, st>>>(g, arr, nvars);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fvs2d_fp64(const Grid& g, int model, int order, const double* cons,
+                              const double* prims, const double* aux, const double* u0,
+                              double* out, double dt, int mode, cudaStream_t st) {
+  if (model == MODEL_SRMHD) {
+    if (order == 3) return fvs2d_instance<SRMHD, 3, 8>(g, cons, prims, aux, u0, out, dt, mode, st);
+    return fvs2d_instance<SRMHD, 5, 8>(g, cons, prims, aux, u0, out, dt, mode, st);
+  }
+  if (order == 3) return fvs2d_instance<SRRMHD, 3, 8>(g, cons, prims, aux, u0, out, dt, mode, st);
+  return fvs2d_instance<SRRMHD, 5, 8>(g, cons, prims, aux, u0, out, dt, mode, st);
+}
+
+cudaError_t launch_fvs_generic(const Grid& g, int model, int order, double* cons, double* prims,
+                               double* aux, double* fplus, double* fminus, double* frecon,
+                               double* fnet, cudaStream_t st) {
+  const int nc = model == MODEL_SRMHD ? 9 : 14;
+  const int np = model == MODEL_SRMHD ? 8 : 11;
+  const int na = model == MODEL_SRMHD ? 13 : 17;
+  cudaError_t e;
+  if ((e = launch_apply_bcs(g, cons, nc, st)) != cudaSuccess) return e;
+  if ((e = launch_apply_bcs(g, prims, np, st)) != cudaSuccess) return e;
+  if ((e = launch_apply_bcs(g, aux, na, st)) != cudaSuccess) return e;
+  return launch_fvs_generic_raw(g, model, order, cons, prims, aux, fplus, fminus, frecon, fnet,
+                                st);
+}
+
+cudaError_t launch_fvs_generic_raw(const Grid& g, int model, int order, const double* cons,
+                                   const double* prims, const double* aux, double* fplus,
+                                   double* fminus, double* frecon, double* fnet,
+                                   cudaStream_t st) {
+  const int nc = model == MODEL_SRMHD ? 9 : 14;
+  const long long nI = (long long)(g.ie - g.is) * (g.je - g.js) * (g.ke - g.ks);
+  for (int dir = 0; dir < g.dims; ++dir) {
+    if (model == MODEL_SRMHD)
+      k_split_dir_full<SRMHD><<<blocks_for(g.Ntot), kThreads, 0, st>>>(g, cons, prims, aux, dir,
+                                                                        fplus, fminus);
+    else
+      k_split_dir_full<SRRMHD><<<blocks_for(g.Ntot), kThreads, 0, st>>>(g, cons, prims, aux,
+                                                                         dir, fplus, fminus);
+    k_weno_dir<<<blocks_for(g.Ntot), kThreads, 0, st>>>(g, nc, order, dir, fplus, fminus,
+                                                        frecon);
+    k_fnet_dir<<<blocks_for(nI), kThreads, 0, st>>>(g, nc, dir, dir == 0, frecon, fnet);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_stage_update(const Grid& g, int nc, int mode, const double* u0,
+                                const double* in, const double* fnet, double dt, double* out,
+                                cudaStream_t st) {
+  const long long nI = (long long)(g.ie - g.is) * (g.je - g.js) * (g.ke - g.ks);
+  k_stage_update<<<blocks_for(nI), kThreads, 0, st>>>(g, nc, mode, u0, in, fnet, dt, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_c2p_srmhd(const Grid& g, const double* cons, const double* prims_guess,
+                             const double* aux_guess, double* prims, double* aux,
+                             double* solution, C2PWork w, cudaStream_t st) {
+  const long long nI = (long long)(g.ie - g.is) * (g.je - g.js) * (g.ke - g.ks);
+  k_c2p_srmhd<<<blocks_for(nI, 128), 128, 0, st>>>(g, cons, prims_guess, aux_guess, prims, aux,
+                                                    solution, w);
+  k_c2p_retry_srmhd<<<1, 32, 0, st>>>(g, cons, prims, aux, solution, w);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_prims_to_all_srrmhd(const Grid& g, const double* prims, double* cons,
+                                       double* aux, cudaStream_t st) {
+  k_prims_to_all_srrmhd<<<blocks_for(g.Ntot), kThreads, 0, st>>>(g, prims, cons, aux);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_c2p_srrmhd(const Grid& g, const double* cons, const double* aux_guess,
+                              double* prims, double* aux, C2PWork w, cudaStream_t st) {
+  const long long nI = (long long)(g.ie - g.is) * (g.je - g.js) * (g.ke - g.ks);
+  k_c2p_srrmhd<<<blocks_for(nI, 128), 128, 0, st>>>(g, cons, aux_guess, prims, aux, w);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_source(const Grid& g, int model, const double* cons, const double* aux,
+                          double* out, cudaStream_t st) {
+  const long long nI = (long long)(g.ie - g.is) * (g.je - g.js) * (g.ke - g.ks);
+  if (model == MODEL_SRMHD)
+    k_source<MODEL_SRMHD><<<blocks_for(nI), kThreads, 0, st>>>(g, cons, aux, out);
+  else
+    k_source<MODEL_SRRMHD><<<blocks_for(nI), kThreads, 0, st>>>(g, cons, aux, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_imex_stage(const Grid& g, int stage, const double* cons,
+                              const double* aux_guess, const double* u1, const double* flux1,
+                              const double* source1, double* out, double dt, C2PWork w,
+                              cudaStream_t st) {
+  const long long nI = (long long)(g.ie - g.is) * (g.je - g.js) * (g.ke - g.ks);
+  if (stage == 1)
+    k_imex_stage<1><<<blocks_for(nI, 64), 64, 0, st>>>(g, cons, aux_guess, u1, flux1, source1,
+                                                        out, dt, w);
+  else
+    k_imex_stage<2><<<blocks_for(nI, 64), 64, 0, st>>>(g, cons, aux_guess, u1, flux1, source1,
+                                                        out, dt, w);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ssp2_combine(const Grid& g, int nc, double* cons, const double* flux1,
+                                const double* flux2, const double* source1,
+                                const double* source2, double dt, cudaStream_t st) {
+  const long long nI = (long long)(g.ie - g.is) * (g.je - g.js) * (g.ke - g.ks);
+  k_ssp2_combine<<<blocks_for(nI), kThreads, 0, st>>>(g, nc, cons, flux1, flux2, source1, source2,
+                                                      dt);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_source_add(const Grid& g, int model, const double* cons, const double* prims,
+                              const double* aux, double* target, double dt, cudaStream_t st) {
+  const long long nI = (long long)(g.ie - g.is) * (g.je - g.js) * (g.ke - g.ks);
+  if (model == MODEL_SRMHD)
+    k_source_add<MODEL_SRMHD><<<blocks_for(nI), kThreads, 0, st>>>(g, cons, prims, aux, target, dt);
+  else
+    k_source_add<MODEL_SRRMHD><<<blocks_for(nI), kThreads, 0, st>>>(g, cons, prims, aux, target,
+                                                                     dt);
+  return cudaGetLastError();
+}
+
+}  // namespace mth

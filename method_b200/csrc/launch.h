@@ -1,0 +1,58 @@
+// Host-side launchers shared between the kernel translation units and the
+// C-ABI.  Every launcher enqueues on `st` and returns the launch status.
+#pragma once
+#include <cuda_runtime.h>
+#include "common.cuh"
+
+namespace mth {
+
+enum ModelId : int { MODEL_SRMHD = 0, MODEL_SRRMHD = 1 };
+
+// Per-call C2P bookkeeping on the device.
+struct C2PWork {
+  int* fail_list;         // capacity Ntot cell ids
+  int* fail_count;        // [0] = failures of the current call
+  long long* counters;    // [0] cells, [1] nfev sum, [2] cells failed, [3] sticky error flags
+};
+
+enum ErrFlag : long long {
+  ERR_C2P = 1,       // primitive recovery did not converge
+  ERR_IMPLICIT = 2,  // implicit source solve did not converge
+};
+
+// ---- plain FP64 (bit-compatible with the reference) --------------------------
+cudaError_t launch_prims_to_all(const Grid& g, int model, const double* prims, double* cons,
+                                double* aux, cudaStream_t st);
+cudaError_t launch_apply_bcs(const Grid& g, double* arr, int nvars, cudaStream_t st);
+cudaError_t launch_fvs2d_fp64(const Grid& g, int model, int order, const double* cons,
+                              const double* prims, const double* aux, const double* u0,
+                              double* out, double dt, int mode, cudaStream_t st);
+// Generic (1D/2D/3D) flux path: materialised ghosts, one pass per direction.
+cudaError_t launch_fvs_generic(const Grid& g, int model, int order, double* cons, double* prims,
+                               double* aux, double* fplus, double* fminus, double* frecon,
+                               double* fnet, cudaStream_t st);
+// FVS::F on the arrays as they are (ghost cells are read, not remapped).
+cudaError_t launch_fvs_generic_raw(const Grid& g, int model, int order, const double* cons,
+                                   const double* prims, const double* aux, double* fplus,
+                                   double* fminus, double* frecon, double* fnet, cudaStream_t st);
+cudaError_t launch_stage_update(const Grid& g, int nc, int mode, const double* u0,
+                                const double* in, const double* fnet, double dt, double* out,
+                                cudaStream_t st);
+cudaError_t launch_c2p_srmhd(const Grid& g, const double* cons, const double* prims_guess,
+                             const double* aux_guess, double* prims, double* aux,
+                             double* solution, C2PWork w, cudaStream_t st);
+cudaError_t launch_c2p_srrmhd(const Grid& g, const double* cons, const double* aux_guess,
+                              double* prims, double* aux, C2PWork w, cudaStream_t st);
+cudaError_t launch_source(const Grid& g, int model, const double* cons, const double* aux,
+                          double* out, cudaStream_t st);
+cudaError_t launch_imex_stage(const Grid& g, int stage, const double* cons,
+                              const double* aux_guess, const double* u1, const double* flux1,
+                              const double* source1, double* out, double dt, C2PWork w,
+                              cudaStream_t st);
+cudaError_t launch_ssp2_combine(const Grid& g, int nc, double* cons, const double* flux1,
+                                const double* flux2, const double* source1,
+                                const double* source2, double dt, cudaStream_t st);
+cudaError_t launch_source_add(const Grid& g, int model, const double* cons, const double* prims,
+                              const double* aux, double* target, double dt, cudaStream_t st);
+
+}  // namespace mth
