@@ -1,0 +1,377 @@
+#!/usr/bin/env python
+"""Benchmark: zone-updates/s of METHOD's RK2 time step on B200.
+
+Workload: SRMHD relativistic Orszag-Tang 2D, periodic [0,1]^2 at 1024x1024,
+rho = 1, p = 1, v = (-0.5 sin 2pi y, 0.5 sin 2pi x), B = (-sin 2pi y,
+sin 4pi x), gamma = 4/3, FVS + WENO5, RK2, CFL 0.4 (synthetic data built on
+the host, method_b200.initial.orszag_tang).  A step is one full RK2 step
+(two fused flux stages and two primitive recoveries) over the 1024^2 grid.
+
+Two forms run on the same initial data with the same dt sequence:
+  plain : all-FP64, bit-identical to the reference CPU build
+  mixed : FP32 flux/WENO, FP64 primitive recovery (Newton) and state
+The headline `value` is the mixed form; `plain` and the mixed form's L1
+error against the plain FP64 result are on the same line.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Multi-GPU: one process per GPU under torchrun, each advancing an independent
+replica (the single-domain path has no exchange step), so scaling is weak;
+timing is the max over ranks of device time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_DEFAULT = 1024
+WORKLOAD = ("SRMHD relativistic Orszag-Tang 2D 1024x1024 periodic, FVS+WENO5, RK2, CFL 0.4, "
+            "gamma 4/3")
+CFG = dict(model="srmhd", xmin=0.0, xmax=1.0, ymin=0.0, ymax=1.0, endTime=1e9, cfl=0.4, Ng=4,
+           gamma=4.0 / 3.0, weno=5, bcs="periodic", integrator="rk2")
+
+
+def steady_dt(n):
+    # Simulation::updateTime's dt after the slow start (simulation.cc:113-117)
+    dx = 1.0 / n
+    return 0.4 * dx / (1.0 * np.sqrt(2.0))
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+
+    def summary(self):
+        self.f.flush()
+        self.f.seek(0)
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.f.read().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = max(mx, float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.f.name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def interior(a, Ng=4):
+    return a[:, Ng:-Ng, Ng:-Ng, :]
+
+
+def run_form(mb, torch, prims0, n, form, steps, warmup, dt, device):
+    sim = mb.Simulation(nx=n, ny=n, precision=form, device=device, **CFG)
+    sim.set_prims(prims0)
+    stream = torch.cuda.Stream(device=device)
+    sim.set_stream(stream.cuda_stream)
+    for _ in range(warmup):
+        sim.step(dt, sync=False)
+    sim.sync()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    return sim, stream, start, end
+
+
+def roofline_of(sim, dt, peak, reps=3):
+    ks = sim.profile_step(dt, reps=reps)
+    top = max(ks, key=lambda k: k["total_ms"])
+    avg_ms = top["total_ms"] / top["launches"]
+    achieved = top["bytes_per_launch"] / (avg_ms * 1e-3) / 1e9
+    return ks, top, {"kernel": top["name"], "bound": "hbm", "achieved": round(achieved, 1),
+                     "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                     "avg_launch_ms": round(avg_ms, 4),
+                     "bytes_per_launch": top["bytes_per_launch"]}
+
+
+def ncu_traffic(kernel):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary, or None."""
+    p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        d = json.load(f)
+    v = d.get(kernel)
+    return None if v is None else v.get("dram_bytes_per_launch_full_size")
+
+
+def cpu_baseline(n, steps=2):
+    """The reference CPU build (serial) on the same workload, bounded sample."""
+    from method_b200 import initial
+    prims = initial.orszag_tang(n, Ng=4)
+    try:
+        from oracle import ref
+        if not ref.available():
+            raise FileNotFoundError
+        sim = ref.RefSim(prims=prims, nx=n, ny=n, **CFG)
+        kind = "reference"
+    except (FileNotFoundError, OSError):
+        from oracle import port
+        sim = port.PortSim(prims, nx=n, ny=n, **CFG)
+        kind = "port"
+    dt = steady_dt(n)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        sim.step_dt(dt)
+    el = time.perf_counter() - t0
+    return {"value": n * n * steps / el, "unit": "zone-updates/s", "cores": 1, "kind": kind,
+            "sample": f"{steps} RK2 steps of the {n}x{n} grid, serial build (-O3), "
+                      f"{el:.1f} s on the host"}
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    n = args.n
+    out = {"metric": "zone-updates/s", "impl": "reference", "unit": "zone-updates/s",
+           "n_gpus": args.gpus, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": WORKLOAD, "n": n}}
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    from method_b200 import initial
+    from oracle import ref
+    prims = initial.orszag_tang(n, Ng=4)
+    dt = steady_dt(n)
+    if ref.available(omp=True):
+        sim = ref.RefSim(prims=prims, omp=True, nx=n, ny=n, **CFG)
+        kind = "reference"
+    else:
+        from oracle import port
+        sim = port.PortSim(prims, nx=n, ny=n, **CFG)
+        kind, threads = "port", 1
+    warm = min(args.warmup, 1)
+    timed = max(1, min(args.steps, 3))
+    for _ in range(warm):
+        sim.step_dt(dt)
+    t0 = time.perf_counter()
+    for _ in range(timed):
+        sim.step_dt(dt)
+    el = time.perf_counter() - t0
+    v = n * n * timed / el
+    out.update({"value": v, "steps": timed, "warmup": warm, "ms_per_step": el / timed * 1e3,
+                "cpu_baseline": {"value": v, "unit": "zone-updates/s", "cores": threads,
+                                 "kind": kind,
+                                 "sample": f"{timed} RK2 steps of the {n}x{n} grid after {warm} "
+                                           f"warm-up, OpenMP build, {threads} threads"},
+                "e2e": {"value": v, "unit": "zone-updates/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}})
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=N_DEFAULT)
+    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--forms", default="plain,mixed",
+                    help="forms to run (profiling runs one at a time)")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return reference_arm(args)
+
+    import torch
+    import method_b200 as mb
+    from method_b200 import initial
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if not dist:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    n = args.n
+    dt = steady_dt(n)
+    prims0 = initial.orszag_tang(n, Ng=4)
+    peak, peak_kind = measured_peaks()
+    K, W = args.steps, args.warmup
+    results = {}
+    clocks = Clocks(local)
+    forms = [f for f in ("plain", "mixed") if f in args.forms.split(",")]
+    with clocks:
+        for form in forms:
+            prec = "fp64" if form == "plain" else "mixed"
+            sim, stream, ev0, ev1 = run_form(mb, torch, prims0, n, prec, K, W, dt, local)
+            sim.reset_stats()
+            barrier()
+            ev0.record(stream)
+            for _ in range(K):
+                sim.step(dt, sync=False)
+            ev1.record(stream)
+            barrier()
+            sim.sync()
+            ms = ev0.elapsed_time(ev1)
+            ms = max_over_ranks(ms)
+            st = sim.stats()
+            c, p, a = sim.state()
+            results[form] = dict(sim=sim, ms=ms, stats=st, cons=interior(c), prims=interior(p))
+    clk = clocks.summary()
+
+    cells = n * n
+    for form in forms:
+        r = results[form]
+        ks, top, roof = roofline_of(r["sim"], dt, peak)
+        roof["peak_kind"] = peak_kind + " (burst copy bandwidth, kernel timed alone)"
+        roof["traffic"] = ncu_traffic(top["name"])
+        launches_per_step = sum(k["launches"] for k in ks) / 3.0
+        r.update(roof=roof, kernels=ks, launches_per_step=launches_per_step)
+        st = r["stats"]
+        r["summary"] = {
+            "value": world * cells * K / (r["ms"] * 1e-3),
+            "ms_per_step": r["ms"] / K,
+            "c2p_evals_per_cell": st["c2p_evals"] / max(st["c2p_cells"], 1),
+            "c2p_unconverged": st["c2p_unconverged"],
+            "roofline": roof,
+            "step_roofline": {"bytes_per_zone_update": 616, "achieved_gbs": round(
+                616 * cells / (r["ms"] / K * 1e-3) / 1e9, 1), "peak": peak},
+            "kernels": [{"name": k["name"], "launches_per_step": k["launches"] / 3.0,
+                         "ms_per_launch": round(k["total_ms"] / k["launches"], 4)} for k in ks],
+        }
+    if forms != ["plain", "mixed"]:
+        if rank == 0:
+            print(json.dumps({f: results[f]["summary"] for f in forms}), flush=True)
+        for r in results.values():
+            r["sim"].close()
+        return
+    # L1 of the mixed form against the FP64 result (bit-identical to the reference)
+    l1 = {}
+    for name in ("cons", "prims"):
+        ref_, mix = results["plain"][name], results["mixed"][name]
+        d = np.abs(mix - ref_)
+        l1[name] = {"l1_abs": float(d.mean()), "l1_rel": float(d.sum() / np.abs(ref_).sum()),
+                    "max_abs": float(d.max())}
+
+    # end to end through the reference-facing call on host arrays (mixed form)
+    e2e = None
+    if args.e2e_steps > 0:
+        sim = mb.Simulation(nx=n, ny=n, precision="mixed", device=local, **CFG)
+        sim.set_prims(prims0)
+        hc, hp, ha = sim.state()
+        for arr in (hc, hp, ha):
+            mb.pin_host(arr)
+        sim.step_host(hc, hp, ha, dt)
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            sim.step_host(hc, hp, ha, dt)
+        el = max_over_ranks(time.perf_counter() - t0)
+        for arr in (hc, hp, ha):
+            mb.unpin_host(arr)
+        nb = hc.nbytes + hp.nbytes + ha.nbytes
+        e2e = {"value": world * cells * args.e2e_steps / el, "unit": "zone-updates/s",
+               "h2d_bytes_per_step": nb, "d2h_bytes_per_step": nb,
+               "call": "mth_step_host (TimeIntegrator::step on host arrays), mixed form",
+               "steps": args.e2e_steps}
+        sim.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(n)
+
+    if rank == 0:
+        m = results["mixed"]["summary"]
+        line = {
+            "metric": "zone-updates/s", "value": m["value"], "unit": "zone-updates/s",
+            "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": m["ms_per_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 flux / f64 c2p+state", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "form": "mixed (FP32 flux, FP64 Newton C2P, "
+                                                      "previous-step guess)",
+                       "n": n, "cells_per_gpu": cells, "dt": "fixed steady-state CFL dt",
+                       "l2": "inputs larger than L2 (device state 0.5 GB per form)",
+                       "parallelism": f"replicas x{world}"},
+            "roofline": results["mixed"]["roof"],
+            "plain": {**results["plain"]["summary"], "dtype": "f64"},
+            "mixed": results["mixed"]["summary"],
+            "l1_mixed_vs_fp64": l1,
+            "speedup_mixed_vs_plain": results["plain"]["ms"] / results["mixed"]["ms"],
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "clocks": clk,
+            "gpu_launches": int(round(results["mixed"]["launches_per_step"] * K)),
+        }
+        print(json.dumps(line), flush=True)
+    for r in results.values():
+        r["sim"].close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

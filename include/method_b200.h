@@ -94,8 +94,21 @@ mth_status mth_c2p(mth_handle* h);
 /* FluxMethod::F (flux.h:72): fnet of the current state into fnet_host
  * (Ncons*Nx*Ny*Nz doubles, interior written, rest zero). */
 mth_status mth_flux_F(mth_handle* h, double* fnet_host);
-/* Model::sourceTerm of the current state (interior cells) into source_host. */
+/* Model::sourceTerm of the current state (every cell) into source_host. */
 mth_status mth_source(mth_handle* h, double* source_host);
+/* Model::fluxVector (model.h:121) of the current state for direction dir
+ * (0, 1, 2), every cell, into f_host (Ncons*Nx*Ny*Nz doubles). */
+mth_status mth_flux_vector(mth_handle* h, int dir, double* f_host);
+
+/* Model::getPrimitiveVarsSingleCell (model.h:85) applied to n independent
+ * cells, with no simulation handle.  Arrays are variable-major with stride n
+ * (cons[v*n + q]), host memory; prims/aux carry the initial guess in
+ * (SRMHD: rho, v, aux h; SRRMHD: aux[10] = rho h W^2) and the solution out.
+ * SRMHD solves with MINPACK hybrd1 at `tol` (the reference uses 1.4e-8,
+ * srmhd.cc:308); SRRMHD uses the reference's secant iteration (tol unused).
+ * Returns MTH_ERR_C2P when any cell did not converge. */
+mth_status mth_c2p_cells(int model, double gamma, double sigma, long long n, const double* cons,
+                         double* prims, double* aux, double tol, int device);
 
 /* TimeIntegrator::step (timeInt.h:61) with an explicit dt; enqueued as one
  * CUDA graph launch, asynchronous. */
@@ -109,6 +122,33 @@ mth_status mth_evolve(mth_handle* h);
 mth_status mth_sync(mth_handle* h);
 mth_status mth_get_stats(mth_handle* h, mth_stats* s);
 mth_status mth_reset_stats(mth_handle* h);
+
+/* Drop-in form of TimeIntegrator::step(cons, prims, aux, dt) (timeInt.h:61)
+ * on HOST arrays, the reference's own calling convention: uploads the three
+ * arrays, runs one step, downloads them, and returns the step's status.
+ * Pinned host memory (mth_pin_host) makes the copies asynchronous DMA. */
+mth_status mth_step_host(mth_handle* h, double* cons, double* prims, double* aux, double dt);
+/* Page-locks / releases a host range for fast copies (cudaHostRegister). */
+mth_status mth_pin_host(void* ptr, unsigned long long bytes);
+mth_status mth_unpin_host(void* ptr);
+
+/* Runs queued work on the caller's CUDA stream (a cudaStream_t passed as an
+ * opaque pointer; NULL restores the handle's own stream).  Graph launches,
+ * copies and eager kernels of this handle are then ordered on that stream. */
+mth_status mth_set_stream(mth_handle* h, void* stream);
+
+/* Per-kernel timing of one step, run eagerly `reps` times with CUDA events
+ * around every launch.  Fills up to max_out records; *n_out receives the
+ * number of distinct kernels.  `bytes_per_launch` is the kernel's algorithmic
+ * HBM traffic (each input array element read once, each output written once). */
+typedef struct {
+  char name[40];
+  int launches;
+  double total_ms;
+  double bytes_per_launch;
+} mth_kernel_time;
+mth_status mth_profile_step(mth_handle* h, double dt, int reps, mth_kernel_time* out,
+                            int max_out, int* n_out);
 
 /* Zero-copy access for frameworks that manage device memory themselves:
  * device pointers of cons, prims, aux (reference layout), valid until

@@ -25,7 +25,18 @@ INTEGRATORS = {"rk2": 0, "rksplit": 1, "ssp2": 2}
 PRECISIONS = {"fp64": 0, "mixed": 1}
 GUESSES = {"previous": 0, "mlp": 1}
 
-__all__ = ["Simulation", "MODELS", "BCS", "INTEGRATORS"]
+__all__ = ["Simulation", "MODELS", "BCS", "INTEGRATORS", "pin_host", "unpin_host"]
+
+
+def pin_host(arr):
+    """Page-locks a numpy array's memory for DMA copies."""
+    L = _lib.load()
+    if L.mth_pin_host(arr.ctypes.data, arr.nbytes) != 0:
+        raise RuntimeError("cudaHostRegister failed")
+
+
+def unpin_host(arr):
+    _lib.load().mth_unpin_host(arr.ctypes.data)
 
 
 def _dptr(a):
@@ -173,6 +184,28 @@ class Simulation:
 
     def reset_stats(self):
         self._check(self.L.mth_reset_stats(self.h), "reset_stats")
+
+    def step_host(self, cons, prims, aux, dt):
+        """TimeIntegrator::step(cons, prims, aux, dt) on host arrays (in place)."""
+        for a in (cons, prims, aux):
+            if a.dtype != np.float64 or not a.flags["C_CONTIGUOUS"]:
+                raise ValueError("arrays must be C-contiguous float64")
+        self._check(self.L.mth_step_host(self.h, _dptr(cons), _dptr(prims), _dptr(aux),
+                                         float(dt)), "step")
+
+    def set_stream(self, stream_ptr):
+        """Orders this simulation's work on an external cudaStream_t (int / None)."""
+        self._check(self.L.mth_set_stream(self.h, stream_ptr), "set_stream")
+
+    def profile_step(self, dt, reps=3):
+        """Per-kernel event timing of `reps` eager steps: list of dicts."""
+        out = (_lib.KernelTime * 32)()
+        n = C.c_int()
+        self._check(self.L.mth_profile_step(self.h, float(dt), int(reps), out, 32, C.byref(n)),
+                    "profile")
+        return [dict(name=out[i].name.decode(), launches=out[i].launches,
+                     total_ms=out[i].total_ms, bytes_per_launch=out[i].bytes_per_launch)
+                for i in range(min(n.value, 32))]
 
     def device_state(self):
         """Raw device pointers (cons, prims, aux) for zero-copy interop."""

@@ -19,8 +19,9 @@ STATUS = {0: "MTH_OK", 1: "MTH_ERR_C2P", 2: "MTH_ERR_IMPLICIT", 3: "MTH_ERR_INVA
 SYMBOLS = [
     "mth_create", "mth_destroy", "mth_last_error", "mth_get_dims", "mth_set_prims",
     "mth_upload", "mth_download", "mth_apply_bcs", "mth_prims_to_all", "mth_c2p",
-    "mth_flux_F", "mth_source", "mth_step", "mth_update_time", "mth_evolve", "mth_sync",
-    "mth_get_stats", "mth_reset_stats", "mth_device_state",
+    "mth_flux_F", "mth_source", "mth_flux_vector", "mth_c2p_cells", "mth_step", "mth_update_time", "mth_evolve", "mth_sync",
+    "mth_get_stats", "mth_reset_stats", "mth_step_host", "mth_pin_host", "mth_unpin_host",
+    "mth_set_stream", "mth_profile_step", "mth_device_state",
 ]
 
 
@@ -43,6 +44,11 @@ class Stats(C.Structure):
         ("implicit_evals", C.c_longlong), ("implicit_failed", C.c_longlong),
         ("steps", C.c_longlong), ("t", C.c_double), ("dt", C.c_double), ("iters", C.c_int),
     ]
+
+
+class KernelTime(C.Structure):
+    _fields_ = [("name", C.c_char * 40), ("launches", C.c_int), ("total_ms", C.c_double),
+                ("bytes_per_launch", C.c_double)]
 
 
 _LIB = None
@@ -72,10 +78,19 @@ def load():
         getattr(L, n).argtypes = [H]
     L.mth_flux_F.argtypes = [H, D]
     L.mth_source.argtypes = [H, D]
+    L.mth_flux_vector.argtypes = [H, C.c_int, D]
+    L.mth_c2p_cells.argtypes = [C.c_int, C.c_double, C.c_double, C.c_longlong, D, D, D,
+                                C.c_double, C.c_int]
     L.mth_step.argtypes = [H, C.c_double]
     L.mth_update_time.argtypes = [H, C.c_int]
     L.mth_get_stats.argtypes = [H, C.POINTER(Stats)]
     L.mth_device_state.argtypes = [H, C.POINTER(D), C.POINTER(D), C.POINTER(D)]
+    L.mth_step_host.argtypes = [H, D, D, D, C.c_double]
+    L.mth_pin_host.argtypes = [C.c_void_p, C.c_ulonglong]
+    L.mth_unpin_host.argtypes = [C.c_void_p]
+    L.mth_set_stream.argtypes = [H, C.c_void_p]
+    L.mth_profile_step.argtypes = [H, C.c_double, C.c_int, C.POINTER(KernelTime), C.c_int,
+                                   C.POINTER(C.c_int)]
     for n in SYMBOLS:
         if n != "mth_last_error":
             getattr(L, n).restype = C.c_int

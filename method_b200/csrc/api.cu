@@ -8,8 +8,10 @@
 #include <cstdio>
 #include <cstdint>
 #include <cstring>
+#include <functional>
 #include <map>
 #include <string>
+#include <vector>
 
 #include <cuda_runtime.h>
 
@@ -24,7 +26,8 @@ struct mth_handle {
   Grid g{};
   int NC = 0, NP = 0, NA = 0;
   int device = 0;
-  cudaStream_t st = nullptr;
+  cudaStream_t st = nullptr;      // stream that carries this handle's work
+  cudaStream_t own_st = nullptr;  // the handle's own stream (graph capture runs here)
   double *cons = nullptr, *prims = nullptr, *aux = nullptr;
   double *p1cons = nullptr, *p1prims = nullptr, *p1aux = nullptr;
   double* solution = nullptr;
@@ -42,6 +45,16 @@ struct mth_handle {
   bool fused = false;
   std::map<uint64_t, cudaGraphExec_t> graphs;
   std::string err;
+  // eager per-kernel timing (mth_profile_step)
+  struct ProfRec {
+    std::string name;
+    int launches;
+    double ms;
+    double bytes;
+  };
+  bool profiling = false;
+  std::vector<ProfRec> prof;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
 
 namespace {
@@ -58,6 +71,34 @@ mth_status fail(mth_handle* h, mth_status s, const std::string& msg) {
       return fail(h, MTH_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(_e)); \
   } while (0)
 
+long long n_interior(const mth_handle* h) {
+  const Grid& g = h->g;
+  return (long long)(g.ie - g.is) * (g.je - g.js) * (g.ke - g.ks);
+}
+
+// Runs one launch helper; when profiling, brackets it with CUDA events and
+// books its duration and algorithmic bytes (doubles per interior cell * 8).
+cudaError_t timed(mth_handle* h, const char* name, double doubles_per_cell,
+                  const std::function<cudaError_t()>& f) {
+  if (!h->profiling) return f();
+  cudaEventRecord(h->ev0, h->st);
+  cudaError_t e = f();
+  cudaEventRecord(h->ev1, h->st);
+  cudaEventSynchronize(h->ev1);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+  const double bytes = 8.0 * doubles_per_cell * (double)n_interior(h);
+  for (auto& r : h->prof)
+    if (r.name == name) {
+      r.launches++;
+      r.ms += ms;
+      r.bytes += bytes;
+      return e;
+    }
+  h->prof.push_back({name, 1, (double)ms, bytes});
+  return e;
+}
+
 C2PWork c2p_work(mth_handle* h) { return C2PWork{h->fail_list, h->fail_count, h->counters}; }
 C2PWork imex_work(mth_handle* h) { return C2PWork{h->fail_list, h->fail_count, h->counters + 4}; }
 
@@ -70,7 +111,7 @@ cudaError_t alloc0(double** p, size_t n, cudaStream_t st) {
 }
 
 // Model::getPrimitiveVars of `cons` into prims/aux, seeded by the guess arrays.
-cudaError_t c2p(mth_handle* h, const double* cons, const double* pg, const double* ag,
+cudaError_t c2p_raw(mth_handle* h, const double* cons, const double* pg, const double* ag,
                 double* prims, double* aux) {
   if (h->cfg.precision == MTH_MIXED || h->cfg.guess == MTH_GUESS_MLP)
     return launch_c2p_mixed(h->g, h->cfg.model, h->cfg.guess, cons, pg, ag, prims, aux,
@@ -81,7 +122,7 @@ cudaError_t c2p(mth_handle* h, const double* cons, const double* pg, const doubl
 }
 
 // FVS::F of (c, p, a) combined with a stage update into `out`.
-cudaError_t flux_stage(mth_handle* h, double* c, double* p, double* a, const double* u0,
+cudaError_t flux_stage_raw(mth_handle* h, double* c, double* p, double* a, const double* u0,
                        double* out, double dt, int mode) {
   const Grid& g = h->g;
   if (h->fused) {
@@ -99,6 +140,26 @@ cudaError_t flux_stage(mth_handle* h, double* c, double* p, double* a, const dou
   return launch_stage_update(g, h->NC, mode, u0, c, h->fnet, dt, out, h->st);
 }
 
+cudaError_t c2p(mth_handle* h, const double* cons, const double* pg, const double* ag,
+                double* prims, double* aux) {
+  const bool srmhd = h->cfg.model == MTH_SRMHD;
+  const bool mixed = h->cfg.precision == MTH_MIXED || h->cfg.guess == MTH_GUESS_MLP;
+  const char* name = srmhd ? (mixed ? "c2p_newton_srmhd" : "c2p_hybrd_srmhd")
+                           : (mixed ? "c2p_newton_srrmhd" : "c2p_secant_srrmhd");
+  return timed(h, name, srmhd ? 37 : 43,
+               [&] { return c2p_raw(h, cons, pg, ag, prims, aux); });
+}
+
+cudaError_t flux_stage(mth_handle* h, double* c, double* p, double* a, const double* u0,
+                       double* out, double dt, int mode) {
+  const bool srmhd = h->cfg.model == MTH_SRMHD;
+  const double in = srmhd ? 22 : 24, nc = h->NC;
+  const double dpc = in + nc + (mode == STAGE_RK2_CORR ? nc : 0);
+  const char* name = h->fused ? (h->cfg.precision == MTH_MIXED ? "fvs2d_fp32" : "fvs2d_fp64")
+                              : "fvs_generic";
+  return timed(h, name, dpc, [&] { return flux_stage_raw(h, c, p, a, u0, out, dt, mode); });
+}
+
 // One TimeIntegrator::step, enqueued on the handle's stream.
 cudaError_t enqueue_step(mth_handle* h, double dt) {
   cudaError_t e;
@@ -114,28 +175,42 @@ cudaError_t enqueue_step(mth_handle* h, double dt) {
     if ((e = c2p(h, h->cons, h->prims, h->aux, h->prims, h->aux))) return e;
     if (integ == MTH_RKSPLIT) {
       // RKSplit::step (rkSplit.cc:31-53): U += dt S(U), finalise.
-      if ((e = launch_source_add(h->g, h->cfg.model, h->cons, h->prims, h->aux, h->cons, dt,
-                                 h->st)))
+      if ((e = timed(h, "source_add", 2.0 * h->NC, [&] {
+             return launch_source_add(h->g, h->cfg.model, h->cons, h->prims, h->aux, h->cons, dt,
+                                      h->st);
+           })))
         return e;
       if ((e = c2p(h, h->cons, h->prims, h->aux, h->prims, h->aux))) return e;
     }
     return cudaSuccess;
   }
   // SSP2::step (SSP2.cc:53-173).
-  if ((e = launch_imex_stage(h->g, 1, h->cons, h->aux, nullptr, nullptr, nullptr, h->u1, dt,
-                             imex_work(h), h->st)))
+  if ((e = timed(h, "imex_stage1", 29, [&] {
+         return launch_imex_stage(h->g, 1, h->cons, h->aux, nullptr, nullptr, nullptr, h->u1, dt,
+                                  imex_work(h), h->st);
+       })))
     return e;
   if ((e = c2p(h, h->u1, h->prims, h->aux, h->prims, h->aux))) return e;
-  if ((e = launch_source(h->g, h->cfg.model, h->u1, h->aux, h->src1, h->st))) return e;
+  if ((e = timed(h, "source", 31, [&] {
+         return launch_source(h->g, h->cfg.model, h->u1, h->aux, h->src1, h->st);
+       })))
+    return e;
   if ((e = flux_stage(h, h->u1, h->prims, h->aux, nullptr, h->flux1, dt, STAGE_FNET))) return e;
-  if ((e = launch_imex_stage(h->g, 2, h->cons, h->aux, h->u1, h->flux1, h->src1, h->u2, dt,
-                             imex_work(h), h->st)))
+  if ((e = timed(h, "imex_stage2", 71, [&] {
+         return launch_imex_stage(h->g, 2, h->cons, h->aux, h->u1, h->flux1, h->src1, h->u2, dt,
+                                  imex_work(h), h->st);
+       })))
     return e;
   if ((e = c2p(h, h->u2, h->prims, h->aux, h->prims, h->aux))) return e;
-  if ((e = launch_source(h->g, h->cfg.model, h->u2, h->aux, h->src2, h->st))) return e;
+  if ((e = timed(h, "source", 31, [&] {
+         return launch_source(h->g, h->cfg.model, h->u2, h->aux, h->src2, h->st);
+       })))
+    return e;
   if ((e = flux_stage(h, h->u2, h->prims, h->aux, nullptr, h->flux2, dt, STAGE_FNET))) return e;
-  if ((e = launch_ssp2_combine(h->g, h->NC, h->cons, h->flux1, h->flux2, h->src1, h->src2, dt,
-                               h->st)))
+  if ((e = timed(h, "ssp2_combine", 6.0 * h->NC, [&] {
+         return launch_ssp2_combine(h->g, h->NC, h->cons, h->flux1, h->flux2, h->src1, h->src2,
+                                    dt, h->st);
+       })))
     return e;
   return c2p(h, h->cons, h->prims, h->aux, h->prims, h->aux);
 }
@@ -155,9 +230,16 @@ mth_status launch_step(mth_handle* h, double dt) {
       h->graphs.clear();
     }
     cudaGraph_t graph;
-    CU(h, cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
+    cudaStream_t work = h->st;
+    h->st = h->own_st;  // capture always runs on the handle's own stream
+    cudaError_t e0 = cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal);
+    if (e0 != cudaSuccess) {
+      h->st = work;
+      return fail(h, MTH_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(e0));
+    }
     cudaError_t e = enqueue_step(h, dt);
     cudaError_t e2 = cudaStreamEndCapture(h->st, &graph);
+    h->st = work;
     if (e != cudaSuccess) return fail(h, MTH_ERR_CUDA, std::string("step: ") + cudaGetErrorString(e));
     if (e2 != cudaSuccess) return fail(h, MTH_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(e2));
     CU(h, cudaGraphInstantiate(&exec, graph, 0));
@@ -278,7 +360,9 @@ mth_status mth_create(const mth_config* cfg, mth_handle** out) {
   };
   cudaError_t e;
   if ((e = cudaSetDevice(c.device)) != cudaSuccess) { delete h; return MTH_ERR_CUDA; }
-  if ((e = cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking))) return bail("stream", e);
+  if ((e = cudaStreamCreateWithFlags(&h->own_st, cudaStreamNonBlocking))) return bail("stream", e);
+  h->st = h->own_st;
+  if ((e = cudaEventCreate(&h->ev0)) || (e = cudaEventCreate(&h->ev1))) return bail("events", e);
   if ((e = alloc0(&h->cons, bytes(h, h->NC), h->st))) return bail("cons", e);
   if ((e = alloc0(&h->prims, bytes(h, h->NP), h->st))) return bail("prims", e);
   if ((e = alloc0(&h->aux, bytes(h, h->NA), h->st))) return bail("aux", e);
@@ -323,7 +407,9 @@ mth_status mth_destroy(mth_handle* h) {
   if (h->fail_count) cudaFree(h->fail_count);
   if (h->counters) cudaFree(h->counters);
   mixed_free(&h->mixed);
-  if (h->st) cudaStreamDestroy(h->st);
+  if (h->ev0) cudaEventDestroy(h->ev0);
+  if (h->ev1) cudaEventDestroy(h->ev1);
+  if (h->own_st) cudaStreamDestroy(h->own_st);
   delete h;
   return MTH_OK;
 }
@@ -398,8 +484,8 @@ mth_status mth_prims_to_all(mth_handle* h) {
 mth_status mth_c2p(mth_handle* h) {
   if (!h) return MTH_ERR_INVALID;
   CU(h, cudaSetDevice(h->device));
+  // the reference recovers the interior only and leaves ghost cells as they are
   CU(h, c2p(h, h->cons, h->prims, h->aux, h->prims, h->aux));
-  h->ghosts_dirty = true;
   return read_status(h);
 }
 
@@ -426,10 +512,51 @@ mth_status mth_source(mth_handle* h, double* source_host) {
   if (!h || !source_host) return MTH_ERR_INVALID;
   CU(h, cudaSetDevice(h->device));
   CU(h, cudaMemsetAsync(h->fnet, 0, bytes(h, h->NC), h->st));
-  CU(h, launch_source(h->g, h->cfg.model, h->cons, h->aux, h->fnet, h->st));
+  CU(h, launch_source(h->g, h->cfg.model, h->cons, h->aux, h->fnet, h->st, true));
   CU(h, cudaMemcpyAsync(source_host, h->fnet, bytes(h, h->NC), cudaMemcpyDeviceToHost, h->st));
   CU(h, cudaStreamSynchronize(h->st));
   return MTH_OK;
+}
+
+mth_status mth_flux_vector(mth_handle* h, int dir, double* f_host) {
+  if (!h || !f_host || dir < 0 || dir >= 3) return MTH_ERR_INVALID;
+  CU(h, cudaSetDevice(h->device));
+  CU(h, launch_flux_vector(h->g, h->cfg.model, h->cons, h->prims, h->aux, dir, h->fnet, h->st));
+  CU(h, cudaMemcpyAsync(f_host, h->fnet, bytes(h, h->NC), cudaMemcpyDeviceToHost, h->st));
+  CU(h, cudaStreamSynchronize(h->st));
+  return MTH_OK;
+}
+
+mth_status mth_c2p_cells(int model, double gamma, double sigma, long long n, const double* cons,
+                         double* prims, double* aux, double tol, int device) {
+  if ((model != MTH_SRMHD && model != MTH_SRRMHD) || n <= 0 || !cons || !prims || !aux)
+    return MTH_ERR_INVALID;
+  const int nc = model == MTH_SRMHD ? 9 : 14, np = model == MTH_SRMHD ? 8 : 11,
+            na = model == MTH_SRMHD ? 13 : 17;
+  if (cudaSetDevice(device) != cudaSuccess) return MTH_ERR_CUDA;
+  double *dc = nullptr, *dp = nullptr, *da = nullptr;
+  int* flag = nullptr;
+  mth_status st = MTH_OK;
+  int hflag = 0;
+  const size_t b = sizeof(double) * (size_t)n;
+  if (cudaMalloc(&dc, b * nc) || cudaMalloc(&dp, b * np) || cudaMalloc(&da, b * na) ||
+      cudaMalloc(&flag, sizeof(int)) || cudaMemset(flag, 0, sizeof(int)) ||
+      cudaMemcpy(dc, cons, b * nc, cudaMemcpyHostToDevice) ||
+      cudaMemcpy(dp, prims, b * np, cudaMemcpyHostToDevice) ||
+      cudaMemcpy(da, aux, b * na, cudaMemcpyHostToDevice) ||
+      launch_c2p_cells(model, gamma, sigma, n, dc, dp, da, tol, flag, 0) ||
+      cudaMemcpy(prims, dp, b * np, cudaMemcpyDeviceToHost) ||
+      cudaMemcpy(aux, da, b * na, cudaMemcpyDeviceToHost) ||
+      cudaMemcpy(&hflag, flag, sizeof(int), cudaMemcpyDeviceToHost)) {
+    st = MTH_ERR_CUDA;
+  } else if (hflag) {
+    st = MTH_ERR_C2P;
+  }
+  cudaFree(dc);
+  cudaFree(dp);
+  cudaFree(da);
+  cudaFree(flag);
+  return st;
 }
 
 mth_status mth_step(mth_handle* h, double dt) {
@@ -494,6 +621,72 @@ mth_status mth_reset_stats(mth_handle* h) {
   CU(h, cudaStreamSynchronize(h->st));
   h->steps = 0;
   return MTH_OK;
+}
+
+mth_status mth_set_stream(mth_handle* h, void* stream) {
+  if (!h) return MTH_ERR_INVALID;
+  CU(h, cudaSetDevice(h->device));
+  CU(h, cudaStreamSynchronize(h->st));
+  h->st = stream ? static_cast<cudaStream_t>(stream) : h->own_st;
+  return MTH_OK;
+}
+
+mth_status mth_pin_host(void* ptr, unsigned long long bytes) {
+  if (!ptr) return MTH_ERR_INVALID;
+  return cudaHostRegister(ptr, (size_t)bytes, cudaHostRegisterDefault) == cudaSuccess
+             ? MTH_OK
+             : MTH_ERR_CUDA;
+}
+
+mth_status mth_unpin_host(void* ptr) {
+  if (!ptr) return MTH_ERR_INVALID;
+  return cudaHostUnregister(ptr) == cudaSuccess ? MTH_OK : MTH_ERR_CUDA;
+}
+
+mth_status mth_step_host(mth_handle* h, double* cons, double* prims, double* aux, double dt) {
+  if (!h || !cons || !prims || !aux || !(dt > 0)) return MTH_ERR_INVALID;
+  CU(h, cudaSetDevice(h->device));
+  CU(h, cudaMemcpyAsync(h->cons, cons, bytes(h, h->NC), cudaMemcpyHostToDevice, h->st));
+  CU(h, cudaMemcpyAsync(h->prims, prims, bytes(h, h->NP), cudaMemcpyHostToDevice, h->st));
+  CU(h, cudaMemcpyAsync(h->aux, aux, bytes(h, h->NA), cudaMemcpyHostToDevice, h->st));
+  h->dt = dt;
+  mth_status s = launch_step(h, dt);
+  if (s != MTH_OK) return s;
+  // the reference leaves its arrays with boundary conditions applied (finalise)
+  CU(h, launch_apply_bcs(h->g, h->cons, h->NC, h->st));
+  CU(h, launch_apply_bcs(h->g, h->prims, h->NP, h->st));
+  CU(h, launch_apply_bcs(h->g, h->aux, h->NA, h->st));
+  h->ghosts_dirty = false;
+  CU(h, cudaMemcpyAsync(cons, h->cons, bytes(h, h->NC), cudaMemcpyDeviceToHost, h->st));
+  CU(h, cudaMemcpyAsync(prims, h->prims, bytes(h, h->NP), cudaMemcpyDeviceToHost, h->st));
+  CU(h, cudaMemcpyAsync(aux, h->aux, bytes(h, h->NA), cudaMemcpyDeviceToHost, h->st));
+  return read_status(h);
+}
+
+mth_status mth_profile_step(mth_handle* h, double dt, int reps, mth_kernel_time* out,
+                            int max_out, int* n_out) {
+  if (!h || !out || !n_out || reps <= 0 || !(dt > 0)) return MTH_ERR_INVALID;
+  CU(h, cudaSetDevice(h->device));
+  CU(h, cudaStreamSynchronize(h->st));
+  h->prof.clear();
+  h->profiling = true;
+  cudaError_t e = cudaSuccess;
+  for (int r = 0; r < reps && e == cudaSuccess; ++r) e = enqueue_step(h, dt);
+  h->profiling = false;
+  if (e != cudaSuccess) return fail(h, MTH_ERR_CUDA, cudaGetErrorString(e));
+  h->ghosts_dirty = true;
+  int n = 0;
+  for (auto& r : h->prof) {
+    if (n < max_out) {
+      std::snprintf(out[n].name, sizeof out[n].name, "%s", r.name.c_str());
+      out[n].launches = r.launches;
+      out[n].total_ms = r.ms;
+      out[n].bytes_per_launch = r.bytes / r.launches;
+    }
+    ++n;
+  }
+  *n_out = n;
+  return read_status(h);
 }
 
 mth_status mth_device_state(mth_handle* h, double** cons, double** prims, double** aux) {

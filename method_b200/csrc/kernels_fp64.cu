@@ -395,15 +395,23 @@ __global__ void __launch_bounds__(128)
   }
 }
 
-// Model::sourceTerm into an interior array.
-template <int MODEL>
+// Model::sourceTerm into an array, over the interior (ALL = false) or every
+// cell (ALL = true, the reference's sourceTerm loops, srmhd.cc:226-250).
+template <int MODEL, bool ALL>
 __global__ void k_source(Grid g, const double* __restrict__ cons, const double* __restrict__ aux,
                          double* __restrict__ out) {
   long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (t >= n_interior(g)) return;
-  int i, j, k;
-  interior_ijk(g, t, i, j, k);
-  const long long N = g.Ntot, cell = cell_id(g, i, j, k);
+  long long cell;
+  if (ALL) {
+    if (t >= g.Ntot) return;
+    cell = t;
+  } else {
+    if (t >= n_interior(g)) return;
+    int i, j, k;
+    interior_ijk(g, t, i, j, k);
+    cell = cell_id(g, i, j, k);
+  }
+  const long long N = g.Ntot;
   if (MODEL == MODEL_SRMHD) {
     double c[9], s[9];
 #pragma unroll
@@ -505,6 +513,70 @@ __global__ void k_ssp2_combine(Grid g, int nc, double* cons, const double* __res
     const long long o = v * g.Ntot + cell;
     cons[o] += -0.5 * dt * (flux1[o] + flux2[o] - source1[o] - source2[o]);
   }
+}
+
+// Model::fluxVector over every cell (srmhd.cc:72-206, srrmhd.cc:65-192).
+template <class M>
+__global__ void k_flux_vector(Grid g, const double* __restrict__ cons,
+                              const double* __restrict__ prims, const double* __restrict__ aux,
+                              int dir, double* __restrict__ f) {
+  long long cell = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (cell >= g.Ntot) return;
+  double c[M::NC], p[M::NP], a[M::NA], fv[M::NC];
+  M::template load_flux_inputs<double>(cons, prims, aux, g.Ntot, cell, c, p, a);
+  M::template flux<double>(c, p, a, dir, fv);
+#pragma unroll
+  for (int v = 0; v < M::NC; ++v) f[v * g.Ntot + cell] = fv[v];
+}
+
+// SRMHD::getPrimitiveVarsSingleCell (srmhd.cc:297-377) on n independent
+// cells, variable-major with stride n.
+__global__ void __launch_bounds__(128)
+    k_c2p_cells_srmhd(long long n, double gamma, double tol, const double* __restrict__ cons,
+                      double* prims, double* aux, int* flag) {
+  long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  double c[9], pg[4];
+#pragma unroll
+  for (int v = 0; v < 9; ++v) c[v] = cons[v * n + q];
+#pragma unroll
+  for (int v = 0; v < 4; ++v) pg[v] = prims[v * n + q];
+  srmhd::Residual R = srmhd::residual_args(c, gamma);
+  double x[2], fv[2];
+  srmhd::guess_from_prims(pg, aux[q], x);
+  HybrdResult res = Hybrd<2>::solve(R, x, fv, tol);
+  if (res.info != 1) {
+    atomicOr(flag, 1);
+    return;
+  }
+  double p[8], a[13];
+  srmhd::from_solution(c, x, gamma, R.BS, R.Bsq, R.Ssq, p, a);
+#pragma unroll
+  for (int v = 0; v < 8; ++v) prims[v * n + q] = p[v];
+#pragma unroll
+  for (int v = 0; v < 13; ++v) aux[v * n + q] = a[v];
+}
+
+// SRRMHD::getPrimitiveVarsSingleCell (srrmhd.cc:256-312) on n cells.
+__global__ void __launch_bounds__(128)
+    k_c2p_cells_srrmhd(long long n, double gamma, double sigma, const double* __restrict__ cons,
+                       double* prims, double* aux, int* flag) {
+  long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  double c[14], p[11], a[17];
+#pragma unroll
+  for (int v = 0; v < 14; ++v) c[v] = cons[v * n + q];
+  a[10] = aux[10 * n + q];
+  int ev = 0;
+  if (!srrmhd::c2p_cell(c, gamma, sigma, p, a, ev)) {
+    aux[10 * n + q] = a[10];
+    atomicOr(flag, 1);
+    return;
+  }
+#pragma unroll
+  for (int v = 0; v < 11; ++v) prims[v * n + q] = p[v];
+#pragma unroll
+  for (int v = 0; v < 17; ++v) aux[v * n + q] = a[v];
 }
 
 template <class M, int ORDER, int TI>
@@ -620,12 +692,38 @@ cudaError_t launch_c2p_srrmhd(const Grid& g, const double* cons, const double* a
 }
 
 cudaError_t launch_source(const Grid& g, int model, const double* cons, const double* aux,
-                          double* out, cudaStream_t st) {
+                          double* out, cudaStream_t st, bool all_cells) {
   const long long nI = (long long)(g.ie - g.is) * (g.je - g.js) * (g.ke - g.ks);
+  if (all_cells) {
+    if (model == MODEL_SRMHD)
+      k_source<MODEL_SRMHD, true><<<blocks_for(g.Ntot), kThreads, 0, st>>>(g, cons, aux, out);
+    else
+      k_source<MODEL_SRRMHD, true><<<blocks_for(g.Ntot), kThreads, 0, st>>>(g, cons, aux, out);
+  } else if (model == MODEL_SRMHD) {
+    k_source<MODEL_SRMHD, false><<<blocks_for(nI), kThreads, 0, st>>>(g, cons, aux, out);
+  } else {
+    k_source<MODEL_SRRMHD, false><<<blocks_for(nI), kThreads, 0, st>>>(g, cons, aux, out);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_flux_vector(const Grid& g, int model, const double* cons, const double* prims,
+                               const double* aux, int dir, double* f, cudaStream_t st) {
   if (model == MODEL_SRMHD)
-    k_source<MODEL_SRMHD><<<blocks_for(nI), kThreads, 0, st>>>(g, cons, aux, out);
+    k_flux_vector<SRMHD><<<blocks_for(g.Ntot), kThreads, 0, st>>>(g, cons, prims, aux, dir, f);
   else
-    k_source<MODEL_SRRMHD><<<blocks_for(nI), kThreads, 0, st>>>(g, cons, aux, out);
+    k_flux_vector<SRRMHD><<<blocks_for(g.Ntot), kThreads, 0, st>>>(g, cons, prims, aux, dir, f);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_c2p_cells(int model, double gamma, double sigma, long long n,
+                             const double* cons, double* prims, double* aux, double tol,
+                             int* flag, cudaStream_t st) {
+  if (model == MODEL_SRMHD)
+    k_c2p_cells_srmhd<<<blocks_for(n, 128), 128, 0, st>>>(n, gamma, tol, cons, prims, aux, flag);
+  else
+    k_c2p_cells_srrmhd<<<blocks_for(n, 128), 128, 0, st>>>(n, gamma, sigma, cons, prims, aux,
+                                                            flag);
   return cudaGetLastError();
 }
 

@@ -44,7 +44,12 @@ cudaError_t launch_c2p_srmhd(const Grid& g, const double* cons, const double* pr
 cudaError_t launch_c2p_srrmhd(const Grid& g, const double* cons, const double* aux_guess,
                               double* prims, double* aux, C2PWork w, cudaStream_t st);
 cudaError_t launch_source(const Grid& g, int model, const double* cons, const double* aux,
-                          double* out, cudaStream_t st);
+                          double* out, cudaStream_t st, bool all_cells = false);
+cudaError_t launch_flux_vector(const Grid& g, int model, const double* cons, const double* prims,
+                               const double* aux, int dir, double* f, cudaStream_t st);
+cudaError_t launch_c2p_cells(int model, double gamma, double sigma, long long n,
+                             const double* cons, double* prims, double* aux, double tol,
+                             int* flag, cudaStream_t st);
 cudaError_t launch_imex_stage(const Grid& g, int stage, const double* cons,
                               const double* aux_guess, const double* u1, const double* flux1,
                               const double* source1, double* out, double dt, C2PWork w,

@@ -1,0 +1,46 @@
+"""CPU checks of the boundary: the C-ABI library loads and exports every
+symbol include/method_b200.h declares, configuration errors are rejected on
+the host, and a reference-style C++ driver builds against the drop-in headers."""
+import os
+import re
+import shutil
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "method_b200.h")
+
+
+def declared_symbols():
+    text = open(HEADER).read()
+    return sorted(set(re.findall(r"\b(mth_[A-Za-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    from method_b200 import _lib
+    L = _lib.load()
+    missing = [s for s in declared_symbols() if not hasattr(L, s)]
+    assert not missing, f"symbols declared but not exported: {missing}"
+    assert set(declared_symbols()) == set(_lib.SYMBOLS)
+
+
+def test_invalid_configuration_rejected_on_host():
+    import method_b200 as mb
+    with pytest.raises(ValueError):  # WENO5 needs Ng >= 4 (weno.cc:13-20)
+        mb.Simulation(nx=16, ny=16, Ng=3, weno=5)
+    with pytest.raises(ValueError):  # sigma >= 0 (simData.cc:100-102)
+        mb.Simulation(nx=16, ny=16, sigma=-1.0)
+    with pytest.raises(ValueError):  # SSP2 is provided for SRRMHD
+        mb.Simulation(nx=16, ny=16, model="srmhd", integrator="ssp2")
+
+
+@pytest.mark.skipif(shutil.which("g++") is None, reason="no host compiler")
+def test_reference_style_driver_builds(tmp_path):
+    exe = tmp_path / "kh_main"
+    cmd = ["g++", "-std=c++11", "-O2", "-I", os.path.join(ROOT, "include", "method_b200"),
+           os.path.join(ROOT, "tests", "cpp", "kh_main.cc"), "-o", str(exe),
+           "-L", os.path.join(ROOT, "method_b200"), "-lmethod_b200",
+           "-Wl,-rpath," + os.path.join(ROOT, "method_b200")]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
