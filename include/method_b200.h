@@ -150,6 +150,32 @@ typedef struct {
 mth_status mth_profile_step(mth_handle* h, double dt, int reps, mth_kernel_time* out,
                             int max_out, int* n_out);
 
+/* Largest number of interior cells mth_c2p_srmhd_noalloc accepts per call. */
+#define MTH_NOALLOC_MAX_CELLS (1 << 20)
+
+/* SRMHD primitive recovery (the grid C2P of mth_c2p, with its neighbour-
+ * average retry) for callers that may not allocate device memory: a host
+ * application that owns all device memory through its own fixed pool, or a
+ * latency-critical loop that cannot afford cudaMalloc and the synchronisation
+ * it may bring.  No counterpart in the reference (its C2P is a host method).
+ * All pointers are device arrays in the reference layout for a grid of
+ * nx x ny x nz interior cells with Ng ghosts (ny = 0: 1D, nz = 0: 2D):
+ * cons (9 vars), prims_guess / aux_guess (the previous state, 8 / 13 vars),
+ * prims / aux (8 / 13 vars, out; may alias the guesses), solution (2 vars,
+ * in/out, the per-cell (v^2, rho h W^2) the retry averages; keep it across
+ * calls as the reference's SRMHD::solution).  Work is enqueued on `stream`
+ * (a cudaStream_t, NULL = default stream) of the calling thread's current
+ * device; the call allocates nothing.  The failure queue and counters live in
+ * one fixed device array (about 4 MiB per GPU, held until exit) shared by all
+ * calls: calls that overlap on the GPU race on it, so order them on one
+ * stream.  The first call on each device looks up that array's address;
+ * make it before any stream capture.  Returns MTH_ERR_INVALID, with a message
+ * on stderr, when the grid has more than MTH_NOALLOC_MAX_CELLS interior cells. */
+mth_status mth_c2p_srmhd_noalloc(int nx, int ny, int nz, int Ng, double gamma,
+                                 const double* cons, const double* prims_guess,
+                                 const double* aux_guess, double* prims, double* aux,
+                                 double* solution, void* stream);
+
 /* Zero-copy access for frameworks that manage device memory themselves:
  * device pointers of cons, prims, aux (reference layout), valid until
  * mth_destroy. */

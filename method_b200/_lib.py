@@ -21,7 +21,7 @@ SYMBOLS = [
     "mth_upload", "mth_download", "mth_apply_bcs", "mth_prims_to_all", "mth_c2p",
     "mth_flux_F", "mth_source", "mth_flux_vector", "mth_c2p_cells", "mth_step", "mth_update_time", "mth_evolve", "mth_sync",
     "mth_get_stats", "mth_reset_stats", "mth_step_host", "mth_pin_host", "mth_unpin_host",
-    "mth_set_stream", "mth_profile_step", "mth_device_state",
+    "mth_set_stream", "mth_profile_step", "mth_c2p_srmhd_noalloc", "mth_device_state",
 ]
 
 
@@ -91,6 +91,9 @@ def load():
     L.mth_set_stream.argtypes = [H, C.c_void_p]
     L.mth_profile_step.argtypes = [H, C.c_double, C.c_int, C.POINTER(KernelTime), C.c_int,
                                    C.POINTER(C.c_int)]
+    L.mth_c2p_srmhd_noalloc.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
+                                         C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                         C.c_void_p, C.c_void_p, C.c_void_p]
     for n in SYMBOLS:
         if n != "mth_last_error":
             getattr(L, n).restype = C.c_int

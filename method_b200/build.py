@@ -34,6 +34,7 @@ UNITS = [
     ("kernels_mixed.cu", []),
     ("mlp.cu", []),
     ("api.cu", []),
+    ("noalloc.cu", []),
     ("shim.cc", []),
 ]
 

@@ -1,0 +1,96 @@
+"""The allocation-free SRMHD primitive recovery, checked against mth_c2p.
+
+mth_c2p_srmhd_noalloc exists for callers that may not allocate device memory
+themselves -- an application that owns every device buffer through its own
+fixed-budget pool, or a stepping loop that cannot afford cudaMalloc and the
+synchronisation it may bring.  Such a caller passes its own device arrays;
+the entry point keeps its failure queue and counters in one fixed device
+array instead of allocating them.
+
+The test gives both entry points the same state and the same guesses (a few
+isolated cells get an unphysical guess, so that the Powell-hybrid solve fails
+there and the neighbour-average retry -- the part that uses the fixed array
+-- runs), on two calls in a row, and asks for agreement to 1e-12 relative,
+the tolerance of the other GPU parity tests.  The device buffers of the
+allocation-free call come from torch: the test is the caller that owns memory.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 1e-12
+
+
+def rel_err(a, b):
+    d = np.abs(a - b)
+    return float(np.max(np.where(np.abs(b) > 1e-12, d / np.maximum(np.abs(b), 1e-300), d)))
+
+
+def test_noalloc_c2p_matches_existing_entry_point():
+    import torch
+
+    import method_b200 as mb
+    from method_b200 import _lib, initial
+    from oracle import port
+
+    n, Ng, gamma = 128, 4, 4.0 / 3.0
+    cfg = dict(model="srmhd", nx=n, ny=n, xmin=0.0, xmax=1.0, ymin=0.0, ymax=1.0, endTime=1.0,
+               cfl=0.4, Ng=Ng, gamma=gamma, weno=5, bcs="periodic", integrator="rk2")
+    sim = mb.Simulation(**cfg)
+    sim.set_prims(initial.orszag_tang(n, Ng=Ng))
+    sim.update_time(3)
+    cons, prims, aux = sim.state()
+    L = _lib.load()
+    Ntot = cons.shape[1] * cons.shape[2] * cons.shape[3]
+    sol = torch.zeros(2 * Ntot, dtype=torch.float64, device="cuda")
+    bad = [(20, 30), (47, 90), (100, 11), (64, 64)]  # isolated interior cells
+    for call in range(2):
+        rng = np.random.default_rng(call)
+        pg = np.ascontiguousarray(prims * (1.0 + 0.02 * (rng.random(prims.shape) - 0.5)))
+        ag = np.ascontiguousarray(aux.copy())
+        for (i, j) in bad:
+            pg[1, Ng + i, Ng + j, 0] = 1.5  # v^2 > 1: the residual is flat, hybrd1 fails
+        # the failing cells really take the retry path
+        cells = np.array([[cons[v, Ng + i, Ng + j, 0] for v in range(9)] for (i, j) in bad])
+        guess = []
+        for (i, j) in bad:  # the kernel's guess (srmhd.cc:438-442)
+            v2 = sum(pg[v, Ng + i, Ng + j, 0] ** 2 for v in (1, 2, 3))
+            guess.append([v2, pg[0, Ng + i, Ng + j, 0] * ag[0, Ng + i, Ng + j, 0] / (1 - v2)])
+        guess = np.array(guess)
+        _, info, _ = port.srmhd_c2p_cells(cells, guess, gamma)
+        assert np.all(info != 1)
+
+        # existing entry point: the handle's own scratch
+        sim.upload(cons, pg, ag)
+        sim.c2p()
+        _, p_ref, a_ref = sim.state()
+
+        # allocation-free entry point on caller-owned device arrays
+        dc = torch.from_numpy(cons).cuda()
+        dpg = torch.from_numpy(pg).cuda()
+        dag = torch.from_numpy(ag).cuda()
+        dp = dpg.clone()
+        da = dag.clone()
+        stream = torch.cuda.current_stream().cuda_stream
+        rc = L.mth_c2p_srmhd_noalloc(n, n, 0, Ng, gamma, dc.data_ptr(), dpg.data_ptr(),
+                                     dag.data_ptr(), dp.data_ptr(), da.data_ptr(),
+                                     sol.data_ptr(), stream)
+        assert rc == 0
+        torch.cuda.synchronize()
+        assert rel_err(dp.cpu().numpy(), p_ref) <= RTOL, f"call {call}: prims"
+        assert rel_err(da.cpu().numpy(), a_ref) <= RTOL, f"call {call}: aux"
+    sim.close()
+
+
+def test_noalloc_rejects_grids_beyond_capacity():
+    import torch
+
+    from method_b200 import _lib
+
+    L = _lib.load()
+    x = torch.zeros(16, dtype=torch.float64, device="cuda")
+    p = x.data_ptr()
+    # 2048 x 1024 interior cells exceed MTH_NOALLOC_MAX_CELLS (1 << 20); rejected before any launch
+    rc = L.mth_c2p_srmhd_noalloc(2048, 1024, 0, 4, 4.0 / 3.0, p, p, p, p, p, p, None)
+    assert rc == 3
