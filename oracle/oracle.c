@@ -1129,10 +1129,11 @@ void orc_set_state(void* h, const double* cons, const double* prims, const doubl
   if (aux) memcpy(s->aux, aux, (size_t)s->NA * s->Ntot * 8);
 }
 
-/* Per-cell SRMHD primitive recovery from a (v^2, rho h W^2) guess: the
- * single solve of getPrimitiveVars (srmhd.cc:438-447) without the grid. */
-int orc_srmhd_c2p_cells(int n, double gamma, const double* cons, const double* guess, double* sol,
-                        int* info, int* nfev) {
+/* Per-cell SRMHD primitive recovery from a (v^2, rho h W^2) guess: one
+ * hybrd1 solve per cell at tolerance tol (the grid C2P uses 1.49011612e-7,
+ * srmhd.cc:380; the single-cell C2P 1.4e-8, srmhd.cc:308). */
+int orc_srmhd_c2p_cells(int n, double gamma, double tol, const double* cons, const double* guess,
+                        double* sol, int* info, int* nfev) {
   int bad = 0;
   for (int q = 0; q < n; q++) {
     const double* c = cons + 9 * q;
@@ -1142,7 +1143,7 @@ int orc_srmhd_c2p_cells(int n, double gamma, const double* cons, const double* g
     a.BS = c[5] * c[1] + c[6] * c[2] + c[7] * c[3];
     a.Bsq = c[5] * c[5] + c[6] * c[6] + c[7] * c[7];
     a.Ssq = c[1] * c[1] + c[2] * c[2] + c[3] * c[3];
-    info[q] = orc_hybrd1(srmhd_residual, &a, 2, x, r, 1.49011612e-7, &nfev[q]);
+    info[q] = orc_hybrd1(srmhd_residual, &a, 2, x, r, tol, &nfev[q]);
     if (info[q] != 1) bad++;
     sol[2 * q] = x[0];
     sol[2 * q + 1] = x[1];

@@ -67,7 +67,7 @@ def lib():
     L.orc_weno5_upwind.restype = C.c_double
     L.orc_weno5_upwind.argtypes = [C.c_double] * 5
     L.orc_hybrd1_kat.argtypes = [C.c_int, C.c_int, D, D, C.c_double, C.c_int]
-    L.orc_srmhd_c2p_cells.argtypes = [C.c_int, C.c_double, D, D, D, I, I]
+    L.orc_srmhd_c2p_cells.argtypes = [C.c_int, C.c_double, C.c_double, D, D, D, I, I]
     _LIB = L
     return L
 
@@ -179,15 +179,16 @@ def hybrd1_kat(which, x0, tol=1.49011612e-8, n=2, lwa=19):
     return info, xx[:2], fvec[:2]
 
 
-def srmhd_c2p_cells(cons, guess, gamma):
-    """Per-cell SRMHD hybrd1 solves; cons (n, 9), guess (n, 2) -> (sol, info, nfev)."""
+def srmhd_c2p_cells(cons, guess, gamma, tol=1.49011612e-7):
+    """Per-cell SRMHD hybrd1 solves; cons (n, 9), guess (n, 2) -> (sol, info, nfev).
+    tol 1.49011612e-7 is the grid C2P's (srmhd.cc:380), 1.4e-8 the single-cell one."""
     cons = np.ascontiguousarray(cons, dtype=np.float64)
     guess = np.ascontiguousarray(guess, dtype=np.float64)
     n = cons.shape[0]
     sol = np.zeros((n, 2))
     info = np.zeros(n, dtype=np.int32)
     nfev = np.zeros(n, dtype=np.int32)
-    lib().orc_srmhd_c2p_cells(n, gamma, _ptr(cons), _ptr(guess), _ptr(sol),
+    lib().orc_srmhd_c2p_cells(n, gamma, tol, _ptr(cons), _ptr(guess), _ptr(sol),
                               info.ctypes.data_as(C.POINTER(C.c_int)),
                               nfev.ctypes.data_as(C.POINTER(C.c_int)))
     return sol, info, nfev

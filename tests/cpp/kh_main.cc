@@ -2,7 +2,8 @@
 // Examples/KelvinHelmholtz/SingleFluidIdealSerial/main.cc) built against the
 // drop-in headers of include/method_b200/ and linked with libmethod_b200.so.
 // Runs the SRMHD Kelvin-Helmholtz shear-layer workload for a few steps and
-// writes the final interior state as raw doubles to argv[1] (when given).
+// writes the final cons and prims as raw doubles to argv[1] and the initial
+// prims (after Simulation::set) to argv[2] (when given).
 #include "simData.h"
 #include "simulation.h"
 #include "initFunc.h"
@@ -30,6 +31,11 @@ int main(int argc, char* argv[]) {
   KHShearLayerSingleFluid init(&data, 1234);
   RK2 timeInt(&data, &model, &bcs, &fluxMethod);
   sim.set(&init, &model, &timeInt, &bcs, &fluxMethod, NULL);
+  FILE* f0 = argc > 2 ? std::fopen(argv[2], "wb") : NULL;
+  if (f0) {
+    std::fwrite(data.prims, sizeof(double), (size_t)data.Nprims * data.Ntot, f0);
+    std::fclose(f0);
+  }
   for (int s = 0; s < 20; ++s) sim.updateTime();
   std::printf("t = %.17g iters = %d rho[center] = %.17g\n", data.t, data.iters,
               data.prims[data.id(0, data.Nx / 2, data.Ny / 2, 0)]);
