@@ -31,7 +31,8 @@ enum { MTH_SRMHD = 0, MTH_SRRMHD = 1 };                       /* Model subclasse
 enum { MTH_OUTFLOW = 0, MTH_PERIODIC = 1, MTH_FLOW = 2 };     /* Bcs subclasses */
 enum { MTH_RK2 = 0, MTH_RKSPLIT = 1, MTH_SSP2 = 2 };          /* TimeIntegrator subclasses */
 enum { MTH_PLAIN_FP64 = 0, MTH_MIXED = 1 };                   /* precision of the flux path */
-enum { MTH_GUESS_PREVIOUS = 0, MTH_GUESS_MLP = 1 };           /* C2P initial guess */
+enum { MTH_GUESS_PREVIOUS = 0, MTH_GUESS_MLP = 1, MTH_GUESS_COLD = 2 }; /* C2P initial guess */
+enum { MTH_C2P_HYBRD = 0, MTH_C2P_NEWTON = 1 };               /* C2P solver */
 
 /* The Data constructor arguments (Project/CPU/Include/simData.h:205-218) plus
  * the choice of Model, WENO order, Bcs and TimeIntegrator. */
@@ -149,6 +150,54 @@ typedef struct {
 } mth_kernel_time;
 mth_status mth_profile_step(mth_handle* h, double dt, int reps, mth_kernel_time* out,
                             int max_out, int* n_out);
+
+/* ---- Learned C2P guess (no counterpart in the reference) ------------------
+ * An 8 -> 64 -> 64 -> 64 -> 2 ReLU network maps scale-free features of an
+ * SRMHD conserved state to (log10(rho h W^2 / D), v^2).  Parameters are FP32
+ * master values in a packed layout of MTH_MLP_NPARAM floats; the device runs
+ * it with BF16 weights and activations and FP32 accumulation.  Statistics
+ * are MTH_MLP_NSTAT floats: feature mean[8], 1/std[8], target mean[2], std[2]. */
+#define MTH_MLP_NPARAM 9928
+#define MTH_MLP_NSTAT 20
+typedef struct {
+  unsigned long long seed;
+  long long n_samples;  /* training pairs the solver generates (primsToAll of random states) */
+  int iterations;       /* Adam steps */
+  int batch;            /* samples per step (multiple of 128 recommended) */
+  float lr;             /* peak learning rate, cosine decay */
+  double gamma;         /* adiabatic index */
+} mth_mlp_train_config;
+/* Trains on the device with the project's forward/backward kernels. */
+mth_status mth_mlp_train(const mth_mlp_train_config* cfg, float* params, float* stats,
+                         float* final_loss, int device);
+/* Gradient of the mean-squared error over n samples (host arrays: x [n][8]
+ * standardised features, t [n][2] standardised targets) -> grad[MTH_MLP_NPARAM]. */
+mth_status mth_mlp_grad(const float* params, int n, const float* x, const float* t, float* grad,
+                        float* loss, int device);
+/* Standardised outputs y [n][2] of standardised features x [n][8]. */
+mth_status mth_mlp_forward(const float* params, int n, const float* x, float* y, int device);
+/* Solver-generated training pairs: features [n][8], targets [n][2] (raw,
+ * not standardised), optionally the conserved [9][n] and generating
+ * primitive [8][n] states. */
+mth_status mth_mlp_make_pairs(long long n, unsigned long long seed, double gamma, float* feat,
+                              float* tgt, double* cons, double* prims, int device);
+/* Installs a trained network in a handle (precision MTH_MIXED, guess MTH_GUESS_MLP). */
+mth_status mth_set_mlp(mth_handle* h, const float* params, const float* stats);
+
+/* Batched SRMHD primitive recovery of n independent cells (device arrays,
+ * variable-major with stride n): cons [9][n] in; prims [8][n] / aux [13][n]
+ * carry the previous-state guess in and the solution out.  method
+ * MTH_C2P_HYBRD is the reference's Powell hybrid (tol 1.49011612e-7);
+ * MTH_C2P_NEWTON is the 1D Newton in rho h W^2, falling back to the
+ * previous-state guess and then to the Powell hybrid.  guess selects the
+ * start: previous state, the network (mlp_params / mlp_stats, host arrays),
+ * or a cold start from the conserved state alone. */
+typedef struct {
+  long long cells, iterations, unconverged, fallbacks;
+} mth_c2p_batch_stats;
+mth_status mth_c2p_batch(double gamma, long long n, const double* cons, double* prims,
+                         double* aux, int method, int guess, const float* mlp_params,
+                         const float* mlp_stats, void* stream, mth_c2p_batch_stats* stats);
 
 /* Largest number of interior cells mth_c2p_srmhd_noalloc accepts per call. */
 #define MTH_NOALLOC_MAX_CELLS (1 << 20)

@@ -193,6 +193,14 @@ class Simulation:
         self._check(self.L.mth_step_host(self.h, _dptr(cons), _dptr(prims), _dptr(aux),
                                          float(dt)), "step")
 
+    def set_mlp(self, params, stats):
+        """Installs a trained C2P guess network (mixed form with guess='mlp')."""
+        params = np.ascontiguousarray(params, dtype=np.float32)
+        stats = np.ascontiguousarray(stats, dtype=np.float32)
+        F = C.POINTER(C.c_float)
+        self._check(self.L.mth_set_mlp(self.h, params.ctypes.data_as(F), stats.ctypes.data_as(F)),
+                    "set_mlp")
+
     def set_stream(self, stream_ptr):
         """Orders this simulation's work on an external cudaStream_t (int / None)."""
         self._check(self.L.mth_set_stream(self.h, stream_ptr), "set_stream")

@@ -21,8 +21,23 @@ SYMBOLS = [
     "mth_upload", "mth_download", "mth_apply_bcs", "mth_prims_to_all", "mth_c2p",
     "mth_flux_F", "mth_source", "mth_flux_vector", "mth_c2p_cells", "mth_step", "mth_update_time", "mth_evolve", "mth_sync",
     "mth_get_stats", "mth_reset_stats", "mth_step_host", "mth_pin_host", "mth_unpin_host",
-    "mth_set_stream", "mth_profile_step", "mth_c2p_srmhd_noalloc", "mth_device_state",
+    "mth_set_stream", "mth_profile_step", "mth_mlp_train", "mth_mlp_grad", "mth_mlp_forward",
+    "mth_mlp_make_pairs", "mth_set_mlp", "mth_c2p_batch", "mth_c2p_srmhd_noalloc",
+    "mth_device_state",
 ]
+
+MLP_NPARAM = 9928
+MLP_NSTAT = 20
+
+
+class MlpTrainConfig(C.Structure):
+    _fields_ = [("seed", C.c_ulonglong), ("n_samples", C.c_longlong), ("iterations", C.c_int),
+                ("batch", C.c_int), ("lr", C.c_float), ("gamma", C.c_double)]
+
+
+class C2PBatchStats(C.Structure):
+    _fields_ = [("cells", C.c_longlong), ("iterations", C.c_longlong),
+                ("unconverged", C.c_longlong), ("fallbacks", C.c_longlong)]
 
 
 class Config(C.Structure):
@@ -91,6 +106,14 @@ def load():
     L.mth_set_stream.argtypes = [H, C.c_void_p]
     L.mth_profile_step.argtypes = [H, C.c_double, C.c_int, C.POINTER(KernelTime), C.c_int,
                                    C.POINTER(C.c_int)]
+    F = C.POINTER(C.c_float)
+    L.mth_mlp_train.argtypes = [C.POINTER(MlpTrainConfig), F, F, F, C.c_int]
+    L.mth_mlp_grad.argtypes = [F, C.c_int, F, F, F, F, C.c_int]
+    L.mth_mlp_forward.argtypes = [F, C.c_int, F, F, C.c_int]
+    L.mth_mlp_make_pairs.argtypes = [C.c_longlong, C.c_ulonglong, C.c_double, F, F, D, D, C.c_int]
+    L.mth_set_mlp.argtypes = [H, F, F]
+    L.mth_c2p_batch.argtypes = [C.c_double, C.c_longlong, C.c_void_p, C.c_void_p, C.c_void_p,
+                                C.c_int, C.c_int, F, F, C.c_void_p, C.POINTER(C2PBatchStats)]
     L.mth_c2p_srmhd_noalloc.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
                                          C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                          C.c_void_p, C.c_void_p, C.c_void_p]

@@ -689,6 +689,70 @@ mth_status mth_profile_step(mth_handle* h, double dt, int reps, mth_kernel_time*
   return read_status(h);
 }
 
+mth_status mth_set_mlp(mth_handle* h, const float* params, const float* stats) {
+  if (!h || !params || !stats) return MTH_ERR_INVALID;
+  if (!h->mixed.mlp_params) return fail(h, MTH_ERR_INVALID, "handle has no mixed-form work");
+  CU(h, cudaSetDevice(h->device));
+  CU(h, cudaMemcpyAsync(h->mixed.mlp_params, params, sizeof(float) * MLP_NPARAM,
+                        cudaMemcpyHostToDevice, h->st));
+  CU(h, cudaMemcpyAsync(h->mixed.feat_stats, stats, sizeof(float) * MLP_NSTAT,
+                        cudaMemcpyHostToDevice, h->st));
+  CU(h, cudaStreamSynchronize(h->st));
+  h->mixed.has_mlp = 1;
+  for (auto& kv : h->graphs) cudaGraphExecDestroy(kv.second);  // re-capture with the network
+  h->graphs.clear();
+  return MTH_OK;
+}
+
+mth_status mth_c2p_batch(double gamma, long long n, const double* cons, double* prims,
+                         double* aux, int method, int guess, const float* mlp_params,
+                         const float* mlp_stats, void* stream, mth_c2p_batch_stats* stats) {
+  if (n <= 0 || !cons || !prims || !aux || method < 0 || method > 1 || guess < 0 || guess > 2 ||
+      (guess == MTH_GUESS_MLP && (!mlp_params || !mlp_stats)))
+    return MTH_ERR_INVALID;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  float *P = nullptr, *S = nullptr;
+  double* zg = nullptr;
+  long long* cnt = nullptr;
+  mth_status rc = MTH_OK;
+  auto bad = [&](cudaError_t e) { return e != cudaSuccess; };
+  if (bad(cudaMalloc(&cnt, sizeof(long long) * 4)) ||
+      bad(cudaMemsetAsync(cnt, 0, sizeof(long long) * 4, st))) {
+    rc = MTH_ERR_CUDA;
+  } else if (guess == MTH_GUESS_MLP) {
+    Grid g{};
+    g.Ntot = n;
+    if (bad(mlp::configure()) || bad(cudaMalloc(&P, sizeof(float) * MLP_NPARAM)) ||
+        bad(cudaMalloc(&S, sizeof(float) * MLP_NSTAT)) ||
+        bad(cudaMalloc(&zg, sizeof(double) * 2 * n)) ||
+        bad(cudaMemcpyAsync(P, mlp_params, sizeof(float) * MLP_NPARAM, cudaMemcpyHostToDevice,
+                            st)) ||
+        bad(cudaMemcpyAsync(S, mlp_stats, sizeof(float) * MLP_NSTAT, cudaMemcpyHostToDevice,
+                            st)) ||
+        bad(mlp::launch_zguess(g, n, true, cons, P, S, zg, st)))
+      rc = MTH_ERR_CUDA;
+  }
+  if (rc == MTH_OK &&
+      bad(launch_c2p_batch(n, gamma, method, guess, cons, prims, aux, zg, cnt, st)))
+    rc = MTH_ERR_CUDA;
+  long long h[4] = {0, 0, 0, 0};
+  if (rc == MTH_OK && (bad(cudaMemcpyAsync(h, cnt, sizeof h, cudaMemcpyDeviceToHost, st)) ||
+                       bad(cudaStreamSynchronize(st))))
+    rc = MTH_ERR_CUDA;
+  if (stats) {
+    stats->cells = h[0];
+    stats->iterations = h[1];
+    stats->unconverged = h[2];
+    stats->fallbacks = h[3];
+  }
+  cudaFree(P);
+  cudaFree(S);
+  cudaFree(zg);
+  cudaFree(cnt);
+  if (rc == MTH_OK && h[2] > 0) rc = MTH_ERR_C2P;
+  return rc;
+}
+
 mth_status mth_device_state(mth_handle* h, double** cons, double** prims, double** aux) {
   if (!h) return MTH_ERR_INVALID;
   if (cons) *cons = h->cons;

@@ -38,47 +38,70 @@ __device__ __forceinline__ long long n_interior(const Grid& g) {
   return (long long)(g.ie - g.is) * (g.je - g.js) * (g.ke - g.ks);
 }
 
-// Newton in Z for SRMHD.  On success Z and vsq hold the root.
+// Newton in Z for SRMHD, safeguarded by a bracket.  v^2(Z) above is strictly
+// decreasing for Z > 0, so "v^2 >= 1 or g < 0" marks the left of the root
+// and g > 0 its right; a Newton step that leaves the bracket (or a zero or
+// negative slope) is replaced by bisection (geometric while the bracket spans
+// decades).  On success Z and vsq hold the root.
+__device__ __forceinline__ bool srmhd_g(double Z, double D, double tau, double BS2, double Bsq,
+                                        double Ssq, double k, double& gv, double& dg,
+                                        double& v2) {
+  const double Z2 = Z * Z, ZB = Z + Bsq;
+  const double Dn = Z2 * ZB * ZB;
+  v2 = fma(Ssq, Z2, (2 * Z + Bsq) * BS2) / Dn;
+  if (!(v2 < 1.0)) return false;
+  const double om = 1 - v2;
+  const double s = sqrt(om);
+  const double p = k * (Z * om - D * s);
+  gv = Z + Bsq - p - 0.5 * Bsq * om - BS2 / (2 * Z2) - D - tau;
+  const double dv2 = (fma(2 * Ssq, Z, 2 * BS2) - v2 * (2 * Z * ZB * (2 * Z + Bsq))) / Dn;
+  const double dp = k * (om - Z * dv2 + D * dv2 / (2 * s));
+  dg = 1 - dp + 0.5 * Bsq * dv2 + BS2 / (Z2 * Z);
+  return true;
+}
+
 __device__ __forceinline__ bool newton_srmhd(double D, double tau, double BS2, double Bsq,
                                              double Ssq, double g, double& Z, double& vsq,
                                              int& iters) {
   const double k = (g - 1) / g;
-  double Zc = Z;
-  if (!(Zc > 0) || !isfinite(Zc)) return false;
-  for (int it = 0; it < 60; ++it) {
+  double gv, dg, v2;
+  // right end of the bracket: g(Z) ~ (1 - k) Z for large Z
+  double hi = fmax(g * (tau + D + Bsq), 1e-300);
+  for (int q = 0; q < 64; ++q) {
+    if (srmhd_g(hi, D, tau, BS2, Bsq, Ssq, k, gv, dg, v2) && gv > 0) break;
+    hi *= 2;
+  }
+  double lo = 0.0;
+  double Zc = (Z > 0 && Z < hi && isfinite(Z)) ? Z : 0.5 * hi;
+  for (int it = 0; it < 100; ++it) {
     ++iters;
-    const double Z2 = Zc * Zc, ZB = Zc + Bsq;
-    const double N = fma(Ssq, Z2, (2 * Zc + Bsq) * BS2);
-    const double Dn = Z2 * ZB * ZB;
-    const double v2 = N / Dn;
-    if (!(v2 < 1.0)) {  // Z below the physical range: v^2(Z) decreases with Z
-      Zc *= 2;
-      continue;
+    double Zn;
+    if (!srmhd_g(Zc, D, tau, BS2, Bsq, Ssq, k, gv, dg, v2)) {
+      lo = Zc;  // v^2 >= 1: left of the root
+      Zn = lo > 0 ? sqrt(lo * hi) : 0.5 * hi;
+    } else {
+      if (gv == 0) {
+        Z = Zc;
+        vsq = v2;
+        break;
+      }
+      if (gv < 0) lo = Zc; else hi = Zc;
+      Zn = Zc - gv / dg;
+      if (!(dg > 0) || !(Zn > lo && Zn < hi)) Zn = (lo > 0 && hi > 4 * lo) ? sqrt(lo * hi) : 0.5 * (lo + hi);
     }
-    const double om = 1 - v2;
-    const double s = sqrt(om);
-    const double rho = D * s;
-    const double p = k * (Zc * om - rho);
-    const double gv = Zc + Bsq - p - 0.5 * Bsq * om - BS2 / (2 * Z2) - D - tau;
-    const double dv2 = (fma(2 * Ssq, Zc, 2 * BS2) - v2 * (2 * Zc * ZB * (2 * Zc + Bsq))) / Dn;
-    const double dp = k * (om - Zc * dv2 + D * dv2 / (2 * s));
-    const double dg = 1 - dp + 0.5 * Bsq * dv2 + BS2 / (Z2 * Zc);
-    double Zn = Zc - gv / dg;
-    if (!(Zn > 0) || !isfinite(Zn)) Zn = 0.5 * Zc;
-    if (fabs(Zn - Zc) <= 1e-13 * Zn) {
-      const double Z2n = Zn * Zn, ZBn = Zn + Bsq;
-      const double v2n = fma(Ssq, Z2n, (2 * Zn + Bsq) * BS2) / (Z2n * ZBn * ZBn);
-      if (!(v2n < 1.0)) return false;
-      const double rn = D * sqrt(1 - v2n);
-      const double pn = k * (Zn * (1 - v2n) - rn);
-      if (pn < 0 || rn < 0) return false;
-      Z = Zn;
-      vsq = v2n;
-      return true;
+    if (fabs(Zn - Zc) <= 1e-14 * Zn || hi - lo <= 1e-15 * hi) {
+      Zc = Zn;
+      if (!srmhd_g(Zc, D, tau, BS2, Bsq, Ssq, k, gv, dg, v2)) return false;
+      Z = Zc;
+      vsq = v2;
+      break;
     }
     Zc = Zn;
+    if (it == 99) return false;
   }
-  return false;
+  const double rn = D * sqrt(1 - vsq);
+  const double pn = k * (Z * (1 - vsq) - rn);
+  return pn >= 0 && rn >= 0;
 }
 
 // Newton in Z for SRRMHD's residual (srrmhd.cc:512-537).
@@ -251,6 +274,87 @@ __global__ void __launch_bounds__(128)
   }
 }
 
+// Batched SRMHD primitive recovery for independent cells.
+__global__ void __launch_bounds__(128)
+    k_c2p_batch_srmhd(long long n, double gamma, int method, int guess,
+                      const double* __restrict__ cons, double* prims, double* aux,
+                      const double* __restrict__ zguess, long long* counters) {
+  const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  long long its = 0, bad = 0, fb = 0;
+  if (q < n) {
+    double c[9];
+#pragma unroll
+    for (int v = 0; v < 9; ++v) c[v] = cons[v * n + q];
+    srmhd::Residual R = srmhd::residual_args(c, gamma);
+    double prev[2];
+    {
+      double pg[4];
+#pragma unroll
+      for (int v = 0; v < 4; ++v) pg[v] = prims[v * n + q];
+      srmhd::guess_from_prims(pg, aux[q], prev);
+    }
+    double x0[2];
+    if (guess == 1) {
+      x0[0] = zguess[n + q];
+      x0[1] = zguess[q];
+    } else if (guess == 2) {
+      const double E = R.tau + R.D;
+      x0[1] = fmax(E, sqrt(R.Ssq) * 1.0000001);
+      x0[0] = fmin(R.Ssq / (x0[1] * x0[1]), 0.999999);
+    } else {
+      x0[0] = prev[0];
+      x0[1] = prev[1];
+    }
+    double x[2] = {x0[0], x0[1]}, fv[2];
+    int it = 0;
+    bool ok = false;
+    if (method == 1) {
+      double Z = x0[1], vsq = x0[0];
+      ok = newton_srmhd(R.D, R.tau, R.BS * R.BS, R.Bsq, R.Ssq, gamma, Z, vsq, it);
+      if (!ok && guess != 0) {
+        fb = 1;
+        Z = prev[1];
+        ok = newton_srmhd(R.D, R.tau, R.BS * R.BS, R.Bsq, R.Ssq, gamma, Z, vsq, it);
+      }
+      if (ok) {
+        x[0] = vsq;
+        x[1] = Z;
+      } else {
+        fb = 1;
+        x[0] = prev[0];
+        x[1] = prev[1];
+        HybrdResult r = Hybrd<2>::solve(R, x, fv, 1.49011612e-7);
+        it += r.nfev;
+        ok = r.info == 1;
+      }
+    } else {
+      HybrdResult r = Hybrd<2>::solve(R, x, fv, 1.49011612e-7);
+      it = r.nfev;
+      ok = r.info == 1;
+    }
+    bad = ok ? 0 : 1;
+    its = it;
+    double p[8], a[13];
+    srmhd::from_solution(c, x, gamma, R.BS, R.Bsq, R.Ssq, p, a);
+#pragma unroll
+    for (int v = 0; v < 8; ++v) prims[v * n + q] = p[v];
+#pragma unroll
+    for (int v = 0; v < 13; ++v) aux[v * n + q] = a[v];
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    its += __shfl_down_sync(0xffffffffu, its, o);
+    bad += __shfl_down_sync(0xffffffffu, bad, o);
+    fb += __shfl_down_sync(0xffffffffu, fb, o);
+  }
+  const unsigned mask = __ballot_sync(0xffffffffu, q < n);
+  if ((threadIdx.x & 31) == 0 && mask) {
+    atomicAdd((unsigned long long*)&counters[0], (unsigned long long)__popc(mask));
+    atomicAdd((unsigned long long*)&counters[1], (unsigned long long)its);
+    if (bad) atomicAdd((unsigned long long*)&counters[2], (unsigned long long)bad);
+    if (fb) atomicAdd((unsigned long long*)&counters[3], (unsigned long long)fb);
+  }
+}
+
 template <class M, int ORDER, int TI>
 cudaError_t fvs2d_fp32_instance(const Grid& g, const double* cons, const double* prims,
                                 const double* aux, const double* u0, double* out, double dt,
@@ -281,12 +385,25 @@ cudaError_t launch_fvs2d_fp32(const Grid& g, int model, int order, const double*
   return fvs2d_fp32_instance<SRRMHD, 5, 8>(g, cons, prims, aux, u0, out, dt, mode, st);
 }
 
+cudaError_t launch_c2p_batch(long long n, double gamma, int method, int guess,
+                             const double* cons, double* prims, double* aux,
+                             const double* zguess, long long* counters, cudaStream_t st) {
+  k_c2p_batch_srmhd<<<(int)((n + 127) / 128), 128, 0, st>>>(n, gamma, method, guess, cons, prims,
+                                                              aux, zguess, counters);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_c2p_mixed(const Grid& g, int model, int guess, const double* cons,
                              const double* prims_guess, const double* aux_guess, double* prims,
                              double* aux, double* solution, C2PWork w, const MixedWork& mw,
                              cudaStream_t st) {
   const long long nI = (long long)(g.ie - g.is) * (g.je - g.js) * (g.ke - g.ks);
   const int blocks = (int)((nI + 127) / 128);
+  if (model == MODEL_SRMHD && guess == 1 && mw.has_mlp) {
+    cudaError_t e = mlp::launch_zguess(g, nI, false, cons, mw.mlp_params, mw.feat_stats,
+                                       mw.zguess, st);
+    if (e != cudaSuccess) return e;
+  }
   if (model == MODEL_SRMHD) {
     k_c2p_newton_srmhd<<<blocks, 128, 0, st>>>(
         g, (guess == 1 && mw.has_mlp) ? 1 : 0, cons, prims_guess, aux_guess, prims, aux, solution,
@@ -298,15 +415,14 @@ cudaError_t launch_c2p_mixed(const Grid& g, int model, int guess, const double* 
 }
 
 cudaError_t mixed_init(MixedWork* w, const Grid& g, int model, cudaStream_t st) {
-  (void)g;
   (void)model;
-  cudaError_t e = cudaMalloc(&w->mlp_params, sizeof(__nv_bfloat16) * MLP_NPARAM);
-  if (e != cudaSuccess) return e;
-  e = cudaMemsetAsync(w->mlp_params, 0, sizeof(__nv_bfloat16) * MLP_NPARAM, st);
-  if (e != cudaSuccess) return e;
-  e = cudaMalloc(&w->feat_stats, sizeof(float) * 32);
-  if (e != cudaSuccess) return e;
-  e = cudaMemsetAsync(w->feat_stats, 0, sizeof(float) * 32, st);
+  cudaError_t e = cudaMalloc(&w->mlp_params, sizeof(float) * MLP_NPARAM);
+  if (e == cudaSuccess) e = cudaMemsetAsync(w->mlp_params, 0, sizeof(float) * MLP_NPARAM, st);
+  if (e == cudaSuccess) e = cudaMalloc(&w->feat_stats, sizeof(float) * 32);
+  if (e == cudaSuccess) e = cudaMemsetAsync(w->feat_stats, 0, sizeof(float) * 32, st);
+  if (e == cudaSuccess) e = cudaMalloc(&w->zguess, sizeof(double) * 2 * g.Ntot);
+  if (e == cudaSuccess) e = cudaMemsetAsync(w->zguess, 0, sizeof(double) * 2 * g.Ntot, st);
+  if (e == cudaSuccess) e = mlp::configure();
   w->has_mlp = 0;
   return e;
 }
@@ -314,8 +430,10 @@ cudaError_t mixed_init(MixedWork* w, const Grid& g, int model, cudaStream_t st) 
 void mixed_free(MixedWork* w) {
   if (w->mlp_params) cudaFree(w->mlp_params);
   if (w->feat_stats) cudaFree(w->feat_stats);
+  if (w->zguess) cudaFree(w->zguess);
   w->mlp_params = nullptr;
   w->feat_stats = nullptr;
+  w->zguess = nullptr;
   w->has_mlp = 0;
 }
 

@@ -8,17 +8,32 @@
 
 namespace mth {
 
-// Guess network 8 -> 64 -> 64 -> 64 -> 2 (BF16 weights, FP32 accumulate).
-constexpr int MLP_IN = 8, MLP_H = 64, MLP_OUT = 2;
-constexpr int MLP_NPARAM = MLP_IN * MLP_H + MLP_H + MLP_H * MLP_H + MLP_H + MLP_H * MLP_H + MLP_H +
-                           MLP_H * MLP_OUT + MLP_OUT;
+// Guess network 8 -> 64 -> 64 -> 64 -> 2 (BF16 weights, FP32 accumulate);
+// packed parameter count of the layout in mlp.cuh (padding included).
+constexpr int MLP_NPARAM = 9928;
+constexpr int MLP_NSTAT = 20;
 
 struct MixedWork {
-  void* mlp_params = nullptr;   // bf16 parameters, packed (W1,b1,W2,b2,W3,b3,W4,b4)
-  float* feat_stats = nullptr;  // input normalisation: mean[8], inv_std[8]; output: mean[2], std[2]
-  double* zguess = nullptr;     // per-cell Z guess written by the network (Ntot)
+  float* mlp_params = nullptr;  // FP32 master parameters (mlp.cuh layout), cast to BF16 on load
+  float* feat_stats = nullptr;  // feature mean[8], inv_std[8]; target mean[2], std[2]
+  double* zguess = nullptr;     // per-cell (Z, v^2) guesses written by the network (2 x Ntot)
   int has_mlp = 0;
 };
+
+namespace mlp {
+size_t smem_bytes();
+cudaError_t configure();
+cudaError_t launch_zguess(const Grid& g, long long n_cells, bool batch, const double* cons,
+                          const float* P, const float* st, double* zguess, cudaStream_t s);
+}  // namespace mlp
+
+// Batched primitive recovery of independent cells (variable-major, stride n).
+// method: 0 Powell hybrid (reference), 1 Newton; guess: 0 previous state,
+// 1 network (zguess planes), 2 cold start.  counters: cells, iterations,
+// unconverged, fallbacks.
+cudaError_t launch_c2p_batch(long long n, double gamma, int method, int guess,
+                             const double* cons, double* prims, double* aux,
+                             const double* zguess, long long* counters, cudaStream_t st);
 
 cudaError_t mixed_init(MixedWork* w, const Grid& g, int model, cudaStream_t st);
 void mixed_free(MixedWork* w);

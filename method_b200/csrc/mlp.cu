@@ -1,0 +1,598 @@
+// Guess network kernels: data generation from the solver's own primsToAll,
+// forward (inference), forward + backward (training) and Adam, all with BF16
+// tensor-core tiles (mlp.cuh) and FP32 accumulation.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+#include <vector>
+
+#include "common.cuh"
+#include "launch.h"
+#include "mixed.h"
+#include "mlp.cuh"
+#include "srmhd.cuh"
+
+namespace mth {
+namespace mlp {
+
+namespace {
+
+// ------------------------------------------------------------- shared memory
+struct Smem {
+  __nv_bfloat16 W1[INP * H], W2[H * H], W3[H * H], W4[H * OUTP];
+  float b1[H], b2[H], b3[H], b4[OUTP];
+  __nv_bfloat16 X[ROWS * INP];
+  __nv_bfloat16 H1[ROWS * H], H2[ROWS * H], H3[ROWS * H];
+  __nv_bfloat16 dZa[ROWS * H], dZb[ROWS * H];
+  __nv_bfloat16 dY[ROWS * OUTP];
+  float Y[ROWS * OUTP];
+  float stats[NSTAT];
+};
+
+__device__ void load_weights(Smem& s, const float* __restrict__ P, const float* __restrict__ st) {
+  for (int i = threadIdx.x; i < INP * H; i += blockDim.x) s.W1[i] = __float2bfloat16(P[OFF_W1 + i]);
+  for (int i = threadIdx.x; i < H * H; i += blockDim.x) {
+    s.W2[i] = __float2bfloat16(P[OFF_W2 + i]);
+    s.W3[i] = __float2bfloat16(P[OFF_W3 + i]);
+  }
+  for (int i = threadIdx.x; i < H * OUTP; i += blockDim.x) s.W4[i] = __float2bfloat16(P[OFF_W4 + i]);
+  for (int i = threadIdx.x; i < H; i += blockDim.x) {
+    s.b1[i] = P[OFF_B1 + i];
+    s.b2[i] = P[OFF_B2 + i];
+    s.b3[i] = P[OFF_B3 + i];
+  }
+  for (int i = threadIdx.x; i < OUTP; i += blockDim.x) s.b4[i] = P[OFF_B4 + i];
+  for (int i = threadIdx.x; i < NSTAT; i += blockDim.x) s.stats[i] = st ? st[i] : 0.f;
+}
+
+// Dense layer for this warp's 16 rows: out = act(in W + b), N = 64 outputs.
+template <int K, bool RELU>
+__device__ __forceinline__ void layer_fwd(const __nv_bfloat16* in, int in_ld,
+                                          const __nv_bfloat16* W, const float* b,
+                                          __nv_bfloat16* out, int r0) {
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+#pragma unroll
+  for (int nt = 0; nt < H / 8; ++nt) {
+    const int n0 = nt * 8;
+    float c[4] = {b[n0 + 2 * t], b[n0 + 2 * t + 1], b[n0 + 2 * t], b[n0 + 2 * t + 1]};
+    tile_mma<K>(
+        c, [&](int r, int k) { return in[(r0 + r) * in_ld + k]; },
+        [&](int k, int n) { return W[k * H + n0 + n]; });
+    if (RELU) {
+#pragma unroll
+      for (int q = 0; q < 4; ++q) c[q] = fmaxf(c[q], 0.f);
+    }
+    out[(r0 + g) * H + n0 + 2 * t] = __float2bfloat16(c[0]);
+    out[(r0 + g) * H + n0 + 2 * t + 1] = __float2bfloat16(c[1]);
+    out[(r0 + g + 8) * H + n0 + 2 * t] = __float2bfloat16(c[2]);
+    out[(r0 + g + 8) * H + n0 + 2 * t + 1] = __float2bfloat16(c[3]);
+  }
+}
+
+// Forward pass of the CTA's 128 rows (X already in shared memory); Y in FP32.
+__device__ void forward(Smem& s) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  const int r0 = warp * 16;
+  layer_fwd<INP, true>(s.X, INP, s.W1, s.b1, s.H1, r0);
+  __syncwarp();
+  layer_fwd<H, true>(s.H1, H, s.W2, s.b2, s.H2, r0);
+  __syncwarp();
+  layer_fwd<H, true>(s.H2, H, s.W3, s.b3, s.H3, r0);
+  __syncwarp();
+  float c[4] = {s.b4[2 * t], s.b4[2 * t + 1], s.b4[2 * t], s.b4[2 * t + 1]};
+  tile_mma<H>(
+      c, [&](int r, int k) { return s.H3[(r0 + r) * H + k]; },
+      [&](int k, int n) { return s.W4[k * OUTP + n]; });
+  s.Y[(r0 + g) * OUTP + 2 * t] = c[0];
+  s.Y[(r0 + g) * OUTP + 2 * t + 1] = c[1];
+  s.Y[(r0 + g + 8) * OUTP + 2 * t] = c[2];
+  s.Y[(r0 + g + 8) * OUTP + 2 * t + 1] = c[3];
+}
+
+// dH = dZ W^T masked by (Hprev > 0), for this warp's rows; W is [64 in][N out].
+template <int KOUT, int WLD>
+__device__ __forceinline__ void back_act(const __nv_bfloat16* dZ, int dz_ld,
+                                         const __nv_bfloat16* W, const __nv_bfloat16* Hprev,
+                                         __nv_bfloat16* out, int r0) {
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+#pragma unroll
+  for (int nt = 0; nt < H / 8; ++nt) {
+    const int n0 = nt * 8;
+    float c[4] = {0.f, 0.f, 0.f, 0.f};
+    tile_mma<KOUT>(
+        c,
+        [&](int r, int k) {
+          return k < dz_ld ? dZ[(r0 + r) * dz_ld + k] : __float2bfloat16(0.f);
+        },
+        [&](int k, int n) {
+          return k < WLD ? W[(n0 + n) * WLD + k] : __float2bfloat16(0.f);
+        });
+    const int rr[4] = {g, g, g + 8, g + 8}, cc[4] = {2 * t, 2 * t + 1, 2 * t, 2 * t + 1};
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int idx = (r0 + rr[q]) * H + n0 + cc[q];
+      const float m = __bfloat162float(Hprev[idx]) > 0.f ? 1.f : 0.f;
+      out[idx] = __float2bfloat16(c[q] * m);
+    }
+  }
+}
+
+// dW[Kin][N] += A^T dZ over the CTA's 128 rows; tiles spread over the warps.
+template <int KIN, int N>
+__device__ void weight_grad(const __nv_bfloat16* A, int a_ld, const __nv_bfloat16* dZ, int dz_ld,
+                            float* __restrict__ gW) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  constexpr int MT = KIN / 16, NT = N / 8;
+  for (int tile = warp; tile < MT * NT; tile += WARPS) {
+    const int m0 = (tile / NT) * 16, n0 = (tile % NT) * 8;
+    float c[4] = {0.f, 0.f, 0.f, 0.f};
+    tile_mma<ROWS>(
+        c, [&](int r, int k) { return A[k * a_ld + m0 + r]; },
+        [&](int k, int n) { return dZ[k * dz_ld + n0 + n]; });
+    atomicAdd(&gW[(m0 + g) * N + n0 + 2 * t], c[0]);
+    atomicAdd(&gW[(m0 + g) * N + n0 + 2 * t + 1], c[1]);
+    atomicAdd(&gW[(m0 + g + 8) * N + n0 + 2 * t], c[2]);
+    atomicAdd(&gW[(m0 + g + 8) * N + n0 + 2 * t + 1], c[3]);
+  }
+}
+
+__device__ void bias_grad(const __nv_bfloat16* dZ, int ld, int ncol, float* __restrict__ gb) {
+  for (int j = threadIdx.x; j < ncol; j += blockDim.x) {
+    float s = 0.f;
+    for (int r = 0; r < ROWS; ++r) s += __bfloat162float(dZ[r * ld + j]);
+    atomicAdd(&gb[j], s);
+  }
+}
+
+// --------------------------------------------------------------- kernels
+// Forward + backward of a mini-batch.  x: standardised features [n][8],
+// t: standardised targets [n][2].  Gradients of the mean-squared error over
+// `denom` samples accumulate into grad; the loss sum into loss.
+__global__ void __launch_bounds__(256) k_mlp_train(const float* __restrict__ P, int n,
+                                                    const float* __restrict__ x,
+                                                    const float* __restrict__ tgt, float denom,
+                                                    float* __restrict__ grad,
+                                                    float* __restrict__ loss) {
+  extern __shared__ __align__(16) unsigned char raw[];
+  Smem& s = *reinterpret_cast<Smem*>(raw);
+  load_weights(s, P, nullptr);
+  const long long base = (long long)blockIdx.x * ROWS;
+  for (int i = threadIdx.x; i < ROWS * INP; i += blockDim.x) {
+    const int r = i / INP, k = i % INP;
+    const long long q = base + r;
+    float v = 0.f;
+    if (k < IN && q < n) v = x[q * IN + k];
+    s.X[i] = __float2bfloat16(v);
+  }
+  __syncthreads();
+  forward(s);
+  __syncthreads();
+  // output gradient and loss
+  float lsum = 0.f;
+  for (int i = threadIdx.x; i < ROWS * OUTP; i += blockDim.x) {
+    const int r = i / OUTP, j = i % OUTP;
+    const long long q = base + r;
+    float d = 0.f;
+    if (j < OUT && q < n) {
+      const float e = s.Y[i] - tgt[q * OUT + j];
+      lsum += e * e;
+      d = 2.f * e / denom;
+    }
+    s.dY[i] = __float2bfloat16(d);
+  }
+  for (int o = 16; o > 0; o >>= 1) lsum += __shfl_down_sync(0xffffffffu, lsum, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(loss, lsum);
+  __syncthreads();
+  const int r0 = (threadIdx.x >> 5) * 16;
+  // layer 4
+  weight_grad<H, OUTP>(s.H3, H, s.dY, OUTP, grad + OFF_W4);
+  bias_grad(s.dY, OUTP, OUTP, grad + OFF_B4);
+  back_act<16, OUTP>(s.dY, OUTP, s.W4, s.H3, s.dZa, r0);  // dZ3
+  __syncthreads();
+  // layer 3
+  weight_grad<H, H>(s.H2, H, s.dZa, H, grad + OFF_W3);
+  bias_grad(s.dZa, H, H, grad + OFF_B3);
+  back_act<H, H>(s.dZa, H, s.W3, s.H2, s.dZb, r0);  // dZ2
+  __syncthreads();
+  // layer 2
+  weight_grad<H, H>(s.H1, H, s.dZb, H, grad + OFF_W2);
+  bias_grad(s.dZb, H, H, grad + OFF_B2);
+  back_act<H, H>(s.dZb, H, s.W2, s.H1, s.dZa, r0);  // dZ1
+  __syncthreads();
+  // layer 1
+  weight_grad<INP, H>(s.X, INP, s.dZa, H, grad + OFF_W1);
+  bias_grad(s.dZa, H, H, grad + OFF_B1);
+}
+
+// Forward only: y[n][2] (standardised outputs) from standardised features.
+__global__ void __launch_bounds__(256) k_mlp_forward(const float* __restrict__ P, int n,
+                                                      const float* __restrict__ x,
+                                                      float* __restrict__ y) {
+  extern __shared__ __align__(16) unsigned char raw[];
+  Smem& s = *reinterpret_cast<Smem*>(raw);
+  load_weights(s, P, nullptr);
+  const long long base = (long long)blockIdx.x * ROWS;
+  for (int i = threadIdx.x; i < ROWS * INP; i += blockDim.x) {
+    const int r = i / INP, k = i % INP;
+    const long long q = base + r;
+    s.X[i] = __float2bfloat16((k < IN && q < n) ? x[q * IN + k] : 0.f);
+  }
+  __syncthreads();
+  forward(s);
+  __syncthreads();
+  for (int i = threadIdx.x; i < ROWS * OUT; i += blockDim.x) {
+    const int r = i / OUT, j = i % OUT;
+    const long long q = base + r;
+    if (q < n) y[q * OUT + j] = s.Y[r * OUTP + j];
+  }
+}
+
+// Guess of Z = rho h W^2 and v^2 for every interior cell of a grid, or for
+// the n cells of a variable-major batch (batch = 1).  zguess holds two
+// planes: Z, then v^2, each with the stride of the cons array.
+__global__ void __launch_bounds__(256) k_mlp_zguess(Grid g, long long n_cells, int batch,
+                                                     const double* __restrict__ cons,
+                                                     const float* __restrict__ P,
+                                                     const float* __restrict__ st,
+                                                     double* __restrict__ zguess) {
+  extern __shared__ __align__(16) unsigned char raw[];
+  Smem& s = *reinterpret_cast<Smem*>(raw);
+  load_weights(s, P, st);
+  __shared__ double Dcell[ROWS];
+  __shared__ long long cellid[ROWS];
+  const long long base = (long long)blockIdx.x * ROWS;
+  if (threadIdx.x < ROWS) {
+    const long long t = base + threadIdx.x;
+    float f[IN] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    long long cell = -1;
+    double D = 1.0;
+    if (t < n_cells) {
+      if (batch) {
+        cell = t;
+      } else {
+        const int nk = g.ke - g.ks, nj = g.je - g.js;
+        const int k = g.ks + (int)(t % nk);
+        const int j = g.js + (int)((t / nk) % nj);
+        const int i = g.is + (int)(t / ((long long)nk * nj));
+        cell = cell_id(g, i, j, k);
+      }
+      const long long N = batch ? n_cells : g.Ntot;
+      double c[9];
+#pragma unroll
+      for (int v = 0; v < 9; ++v) c[v] = cons[v * N + cell];
+      D = c[0];
+      features_srmhd(c, f);
+    }
+    cellid[threadIdx.x] = cell;
+    Dcell[threadIdx.x] = D;
+#pragma unroll
+    for (int k = 0; k < INP; ++k)
+      s.X[threadIdx.x * INP + k] =
+          __float2bfloat16(k < IN ? (f[k] - s.stats[k]) * s.stats[IN + k] : 0.f);
+  }
+  __syncthreads();
+  forward(s);
+  __syncthreads();
+  if (threadIdx.x < ROWS && cellid[threadIdx.x] >= 0) {
+    const float y0 = s.Y[threadIdx.x * OUTP] * s.stats[2 * IN + 2] + s.stats[2 * IN];
+    const float y1 = s.Y[threadIdx.x * OUTP + 1] * s.stats[2 * IN + 3] + s.stats[2 * IN + 1];
+    const long long stride = batch ? n_cells : g.Ntot;
+    zguess[cellid[threadIdx.x]] = Dcell[threadIdx.x] * exp10((double)y0);
+    zguess[stride + cellid[threadIdx.x]] = fmin(fmax((double)y1, 0.0), 0.999999);
+  }
+}
+
+// Adam on the FP32 master parameters.
+__global__ void k_adam(float* __restrict__ P, float* __restrict__ m, float* __restrict__ v,
+                       const float* __restrict__ grad, float lr, float b1t, float b2t) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= NPARAM) return;
+  const float g = grad[i];
+  const float mi = 0.9f * m[i] + 0.1f * g;
+  const float vi = 0.999f * v[i] + 0.001f * g * g;
+  m[i] = mi;
+  v[i] = vi;
+  const float mh = mi / (1.f - b1t), vh = vi / (1.f - b2t);
+  P[i] -= lr * mh / (sqrtf(vh) + 1e-8f);
+}
+
+// Counter-based uniform in [0, 1) (splitmix64 finaliser).
+__device__ __forceinline__ double u01(unsigned long long seed, unsigned long long i) {
+  unsigned long long z = seed + 0x9E3779B97F4A7C15ull * (i + 1);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  z ^= z >> 31;
+  return (double)(z >> 11) * (1.0 / 9007199254740992.0);
+}
+
+// Training pairs from the solver: random primitive states (W, rho, p/rho,
+// b^2/rho log-uniform, isotropic directions) mapped to conserved variables
+// by the model's primsToAll; features of the conserved state, targets
+// log10(Z/D) and v^2 of the generating state.
+__global__ void k_make_pairs(long long n, unsigned long long seed, double gamma,
+                             float* __restrict__ feat, float* __restrict__ tgt,
+                             double* __restrict__ cons_out, double* __restrict__ prims_out) {
+  const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const unsigned long long b = (unsigned long long)q * 16;
+  const double W = pow(10.0, u01(seed, b));
+  const double rho = pow(10.0, -3.0 + 3.0 * u01(seed, b + 1));
+  const double prs = rho * pow(10.0, -3.0 + 4.0 * u01(seed, b + 2));
+  const double sig = pow(10.0, -2.0 + 4.0 * u01(seed, b + 3));
+  const double cv = 2.0 * u01(seed, b + 4) - 1.0, pv = 6.283185307179586 * u01(seed, b + 5);
+  const double cb = 2.0 * u01(seed, b + 6) - 1.0, pb = 6.283185307179586 * u01(seed, b + 7);
+  const double sv = sqrt(fmax(0.0, 1.0 - cv * cv)), sb = sqrt(fmax(0.0, 1.0 - cb * cb));
+  const double vh[3] = {sv * cos(pv), sv * sin(pv), cv}, bh[3] = {sb * cos(pb), sb * sin(pb), cb};
+  const double vmag = sqrt(1.0 - 1.0 / (W * W));
+  const double vb = (vh[0] * bh[0] + vh[1] * bh[1] + vh[2] * bh[2]) * vmag;
+  const double Bmag = sqrt(sig * rho * W * W / (1.0 + W * W * vb * vb));
+  double p[8] = {rho, vh[0] * vmag, vh[1] * vmag, vh[2] * vmag, prs, bh[0] * Bmag, bh[1] * Bmag,
+                 bh[2] * Bmag};
+  double c[9], a[13];
+  srmhd::prims_to_all(p, gamma, c, a);
+  float f[IN];
+  features_srmhd(c, f);
+#pragma unroll
+  for (int k = 0; k < IN; ++k) feat[q * IN + k] = f[k];
+  const double Z = p[0] * a[0] * a[1] * a[1];
+  tgt[q * OUT + 0] = (float)log10(Z / c[0]);
+  tgt[q * OUT + 1] = (float)a[9];
+  if (cons_out)
+    for (int v = 0; v < 9; ++v) cons_out[v * n + q] = c[v];
+  if (prims_out)
+    for (int v = 0; v < 8; ++v) prims_out[v * n + q] = p[v];
+}
+
+__global__ void k_standardise(long long n, float* __restrict__ feat, float* __restrict__ tgt,
+                              const float* __restrict__ st) {
+  const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (q >= n) return;
+#pragma unroll
+  for (int k = 0; k < IN; ++k) feat[q * IN + k] = (feat[q * IN + k] - st[k]) * st[IN + k];
+  tgt[q * OUT + 0] = (tgt[q * OUT + 0] - st[2 * IN]) / st[2 * IN + 2];
+  tgt[q * OUT + 1] = (tgt[q * OUT + 1] - st[2 * IN + 1]) / st[2 * IN + 3];
+}
+
+}  // namespace
+
+static_assert(NPARAM == MLP_NPARAM, "parameter layout");
+static_assert(NSTAT == MLP_NSTAT, "statistics layout");
+
+size_t smem_bytes() { return sizeof(Smem) + 16; }
+
+cudaError_t configure() {
+  const int b = (int)sizeof(Smem);
+  cudaError_t e = cudaFuncSetAttribute(k_mlp_train, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_mlp_zguess, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+  return e;
+}
+
+cudaError_t launch_train(const float* P, int n, const float* x, const float* t, float denom,
+                         float* grad, float* loss, cudaStream_t st) {
+  k_mlp_train<<<(n + ROWS - 1) / ROWS, 256, sizeof(Smem), st>>>(P, n, x, t, denom, grad, loss);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_forward(const float* P, int n, const float* x, float* y, cudaStream_t st) {
+  k_mlp_forward<<<(n + ROWS - 1) / ROWS, 256, sizeof(Smem), st>>>(P, n, x, y);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_zguess(const Grid& g, long long n_cells, bool batch, const double* cons,
+                          const float* P, const float* st, double* zguess, cudaStream_t s) {
+  const int blocks = (int)((n_cells + ROWS - 1) / ROWS);
+  k_mlp_zguess<<<blocks, 256, sizeof(Smem), s>>>(g, n_cells, batch ? 1 : 0, cons, P, st, zguess);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_adam(float* P, float* m, float* v, const float* grad, float lr, float b1t,
+                        float b2t, cudaStream_t st) {
+  k_adam<<<(NPARAM + 255) / 256, 256, 0, st>>>(P, m, v, grad, lr, b1t, b2t);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_make_pairs(long long n, unsigned long long seed, double gamma, float* feat,
+                              float* tgt, double* cons, double* prims, cudaStream_t st) {
+  k_make_pairs<<<(int)((n + 255) / 256), 256, 0, st>>>(n, seed, gamma, feat, tgt, cons, prims);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_standardise(long long n, float* feat, float* tgt, const float* stats,
+                               cudaStream_t st) {
+  k_standardise<<<(int)((n + 255) / 256), 256, 0, st>>>(n, feat, tgt, stats);
+  return cudaGetLastError();
+}
+
+}  // namespace mlp
+}  // namespace mth
+
+// ------------------------------------------------------------------ C ABI
+#include <algorithm>
+#include <random>
+
+#include "../../include/method_b200.h"
+
+namespace {
+
+using namespace mth;
+
+struct DevBuf {
+  void* p = nullptr;
+  ~DevBuf() {
+    if (p) cudaFree(p);
+  }
+  template <class T>
+  T* as() {
+    return static_cast<T*>(p);
+  }
+};
+
+#define MLP_CU(x)                            \
+  do {                                       \
+    if ((x) != cudaSuccess) return MTH_ERR_CUDA; \
+  } while (0)
+
+// He-uniform initialisation; padding rows / columns are zero.
+void init_params(std::vector<float>& P, unsigned long long seed) {
+  std::mt19937_64 gen(seed);
+  P.assign(mlp::NPARAM, 0.f);
+  auto fill = [&](int off, int rows, int cols, int real_rows, int real_cols, int fan_in) {
+    std::uniform_real_distribution<float> U(-std::sqrt(6.f / fan_in), std::sqrt(6.f / fan_in));
+    for (int r = 0; r < rows; ++r)
+      for (int c = 0; c < cols; ++c) P[off + r * cols + c] = (r < real_rows && c < real_cols) ? U(gen) : 0.f;
+  };
+  fill(mlp::OFF_W1, mlp::INP, mlp::H, mlp::IN, mlp::H, mlp::IN);
+  fill(mlp::OFF_W2, mlp::H, mlp::H, mlp::H, mlp::H, mlp::H);
+  fill(mlp::OFF_W3, mlp::H, mlp::H, mlp::H, mlp::H, mlp::H);
+  fill(mlp::OFF_W4, mlp::H, mlp::OUTP, mlp::H, mlp::OUT, mlp::H);
+}
+
+}  // namespace
+
+extern "C" mth_status mth_mlp_train(const mth_mlp_train_config* c, float* params, float* stats,
+                                    float* final_loss, int device) {
+  if (!c || !params || !stats || c->n_samples < mlp::ROWS || c->batch < mlp::ROWS ||
+      c->batch > c->n_samples || c->iterations <= 0)
+    return MTH_ERR_INVALID;
+  MLP_CU(cudaSetDevice(device));
+  MLP_CU(mlp::configure());
+  const long long n = c->n_samples;
+  DevBuf feat, tgt, P, m, v, grad, loss, st;
+  MLP_CU(cudaMalloc(&feat.p, sizeof(float) * n * mlp::IN));
+  MLP_CU(cudaMalloc(&tgt.p, sizeof(float) * n * mlp::OUT));
+  MLP_CU(cudaMalloc(&P.p, sizeof(float) * mlp::NPARAM));
+  MLP_CU(cudaMalloc(&m.p, sizeof(float) * mlp::NPARAM));
+  MLP_CU(cudaMalloc(&v.p, sizeof(float) * mlp::NPARAM));
+  MLP_CU(cudaMalloc(&grad.p, sizeof(float) * mlp::NPARAM));
+  MLP_CU(cudaMalloc(&loss.p, sizeof(float)));
+  MLP_CU(cudaMalloc(&st.p, sizeof(float) * mlp::NSTAT));
+  cudaStream_t s;
+  MLP_CU(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  MLP_CU(mlp::launch_make_pairs(n, c->seed, c->gamma, feat.as<float>(), tgt.as<float>(), nullptr,
+                                nullptr, s));
+  // normalisation statistics on the host
+  std::vector<float> hf(n * mlp::IN), ht(n * mlp::OUT);
+  MLP_CU(cudaMemcpyAsync(hf.data(), feat.p, sizeof(float) * hf.size(), cudaMemcpyDeviceToHost, s));
+  MLP_CU(cudaMemcpyAsync(ht.data(), tgt.p, sizeof(float) * ht.size(), cudaMemcpyDeviceToHost, s));
+  MLP_CU(cudaStreamSynchronize(s));
+  std::vector<double> mean(mlp::IN + mlp::OUT, 0.0), var(mlp::IN + mlp::OUT, 0.0);
+  for (long long q = 0; q < n; ++q) {
+    for (int k = 0; k < mlp::IN; ++k) mean[k] += hf[q * mlp::IN + k];
+    for (int k = 0; k < mlp::OUT; ++k) mean[mlp::IN + k] += ht[q * mlp::OUT + k];
+  }
+  for (auto& x : mean) x /= (double)n;
+  for (long long q = 0; q < n; ++q) {
+    for (int k = 0; k < mlp::IN; ++k) {
+      double d = hf[q * mlp::IN + k] - mean[k];
+      var[k] += d * d;
+    }
+    for (int k = 0; k < mlp::OUT; ++k) {
+      double d = ht[q * mlp::OUT + k] - mean[mlp::IN + k];
+      var[mlp::IN + k] += d * d;
+    }
+  }
+  for (int k = 0; k < mlp::IN; ++k) {
+    stats[k] = (float)mean[k];
+    stats[mlp::IN + k] = (float)(1.0 / std::sqrt(var[k] / (double)n + 1e-12));
+  }
+  for (int k = 0; k < mlp::OUT; ++k) {
+    stats[2 * mlp::IN + k] = (float)mean[mlp::IN + k];
+    stats[2 * mlp::IN + 2 + k] = (float)std::sqrt(var[mlp::IN + k] / (double)n + 1e-12);
+  }
+  MLP_CU(cudaMemcpyAsync(st.p, stats, sizeof(float) * mlp::NSTAT, cudaMemcpyHostToDevice, s));
+  MLP_CU(mlp::launch_standardise(n, feat.as<float>(), tgt.as<float>(), st.as<float>(), s));
+  std::vector<float> P0;
+  init_params(P0, c->seed ^ 0x5DEECE66Dull);
+  MLP_CU(cudaMemcpyAsync(P.p, P0.data(), sizeof(float) * mlp::NPARAM, cudaMemcpyHostToDevice, s));
+  MLP_CU(cudaMemsetAsync(m.p, 0, sizeof(float) * mlp::NPARAM, s));
+  MLP_CU(cudaMemsetAsync(v.p, 0, sizeof(float) * mlp::NPARAM, s));
+  std::mt19937_64 pick(c->seed + 17);
+  std::uniform_int_distribution<long long> start(0, n - c->batch);
+  float b1t = 1.f, b2t = 1.f;
+  for (int it = 0; it < c->iterations; ++it) {
+    const long long off = start(pick);
+    MLP_CU(cudaMemsetAsync(grad.p, 0, sizeof(float) * mlp::NPARAM, s));
+    MLP_CU(cudaMemsetAsync(loss.p, 0, sizeof(float), s));
+    MLP_CU(mlp::launch_train(P.as<float>(), c->batch, feat.as<float>() + off * mlp::IN,
+                             tgt.as<float>() + off * mlp::OUT, (float)c->batch * mlp::OUT,
+                             grad.as<float>(), loss.as<float>(), s));
+    b1t *= 0.9f;
+    b2t *= 0.999f;
+    const float frac = (float)it / (float)c->iterations;
+    const float lr = c->lr * (0.05f + 0.95f * 0.5f * (1.f + std::cos(3.14159265f * frac)));
+    MLP_CU(mlp::launch_adam(P.as<float>(), m.as<float>(), v.as<float>(), grad.as<float>(), lr,
+                            b1t, b2t, s));
+  }
+  float lsum = 0.f;
+  MLP_CU(cudaMemcpyAsync(&lsum, loss.p, sizeof(float), cudaMemcpyDeviceToHost, s));
+  MLP_CU(cudaMemcpyAsync(params, P.p, sizeof(float) * mlp::NPARAM, cudaMemcpyDeviceToHost, s));
+  MLP_CU(cudaStreamSynchronize(s));
+  cudaStreamDestroy(s);
+  if (final_loss) *final_loss = lsum / ((float)c->batch * mlp::OUT);
+  return MTH_OK;
+}
+
+extern "C" mth_status mth_mlp_grad(const float* params, int n, const float* x, const float* t,
+                                   float* grad, float* loss, int device) {
+  if (!params || n <= 0 || !x || !t || !grad) return MTH_ERR_INVALID;
+  MLP_CU(cudaSetDevice(device));
+  MLP_CU(mlp::configure());
+  DevBuf P, dx, dt, g, l;
+  MLP_CU(cudaMalloc(&P.p, sizeof(float) * mlp::NPARAM));
+  MLP_CU(cudaMalloc(&dx.p, sizeof(float) * n * mlp::IN));
+  MLP_CU(cudaMalloc(&dt.p, sizeof(float) * n * mlp::OUT));
+  MLP_CU(cudaMalloc(&g.p, sizeof(float) * mlp::NPARAM));
+  MLP_CU(cudaMalloc(&l.p, sizeof(float)));
+  MLP_CU(cudaMemcpy(P.p, params, sizeof(float) * mlp::NPARAM, cudaMemcpyHostToDevice));
+  MLP_CU(cudaMemcpy(dx.p, x, sizeof(float) * n * mlp::IN, cudaMemcpyHostToDevice));
+  MLP_CU(cudaMemcpy(dt.p, t, sizeof(float) * n * mlp::OUT, cudaMemcpyHostToDevice));
+  MLP_CU(cudaMemset(g.p, 0, sizeof(float) * mlp::NPARAM));
+  MLP_CU(cudaMemset(l.p, 0, sizeof(float)));
+  MLP_CU(mlp::launch_train(P.as<float>(), n, dx.as<float>(), dt.as<float>(), (float)n * mlp::OUT,
+                           g.as<float>(), l.as<float>(), 0));
+  MLP_CU(cudaMemcpy(grad, g.p, sizeof(float) * mlp::NPARAM, cudaMemcpyDeviceToHost));
+  float ls = 0.f;
+  MLP_CU(cudaMemcpy(&ls, l.p, sizeof(float), cudaMemcpyDeviceToHost));
+  if (loss) *loss = ls / ((float)n * mlp::OUT);
+  return MTH_OK;
+}
+
+extern "C" mth_status mth_mlp_forward(const float* params, int n, const float* x, float* y,
+                                      int device) {
+  if (!params || n <= 0 || !x || !y) return MTH_ERR_INVALID;
+  MLP_CU(cudaSetDevice(device));
+  MLP_CU(mlp::configure());
+  DevBuf P, dx, dy;
+  MLP_CU(cudaMalloc(&P.p, sizeof(float) * mlp::NPARAM));
+  MLP_CU(cudaMalloc(&dx.p, sizeof(float) * n * mlp::IN));
+  MLP_CU(cudaMalloc(&dy.p, sizeof(float) * n * mlp::OUT));
+  MLP_CU(cudaMemcpy(P.p, params, sizeof(float) * mlp::NPARAM, cudaMemcpyHostToDevice));
+  MLP_CU(cudaMemcpy(dx.p, x, sizeof(float) * n * mlp::IN, cudaMemcpyHostToDevice));
+  MLP_CU(mlp::launch_forward(P.as<float>(), n, dx.as<float>(), dy.as<float>(), 0));
+  MLP_CU(cudaMemcpy(y, dy.p, sizeof(float) * n * mlp::OUT, cudaMemcpyDeviceToHost));
+  return MTH_OK;
+}
+
+extern "C" mth_status mth_mlp_make_pairs(long long n, unsigned long long seed, double gamma,
+                                         float* feat, float* tgt, double* cons, double* prims,
+                                         int device) {
+  if (n <= 0 || !feat || !tgt) return MTH_ERR_INVALID;
+  MLP_CU(cudaSetDevice(device));
+  DevBuf df, dt, dc, dp;
+  MLP_CU(cudaMalloc(&df.p, sizeof(float) * n * mlp::IN));
+  MLP_CU(cudaMalloc(&dt.p, sizeof(float) * n * mlp::OUT));
+  if (cons) MLP_CU(cudaMalloc(&dc.p, sizeof(double) * n * 9));
+  if (prims) MLP_CU(cudaMalloc(&dp.p, sizeof(double) * n * 8));
+  MLP_CU(mlp::launch_make_pairs(n, seed, gamma, df.as<float>(), dt.as<float>(), dc.as<double>(),
+                                dp.as<double>(), 0));
+  MLP_CU(cudaMemcpy(feat, df.p, sizeof(float) * n * mlp::IN, cudaMemcpyDeviceToHost));
+  MLP_CU(cudaMemcpy(tgt, dt.p, sizeof(float) * n * mlp::OUT, cudaMemcpyDeviceToHost));
+  if (cons) MLP_CU(cudaMemcpy(cons, dc.p, sizeof(double) * n * 9, cudaMemcpyDeviceToHost));
+  if (prims) MLP_CU(cudaMemcpy(prims, dp.p, sizeof(double) * n * 8, cudaMemcpyDeviceToHost));
+  return MTH_OK;
+}

@@ -1,0 +1,148 @@
+"""GPU tests of the learned C2P guess: device forward/backward against the CPU
+oracle, training on solver-generated pairs, and what the trained network
+gains over primitive recovery without it (config: random SRMHD states with
+Lorentz factor 1-10, rho 1e-3-1, p/rho 1e-3-10, b^2/rho 1e-2-1e2)."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from oracle import mlp_oracle as M
+
+pytestmark = pytest.mark.gpu
+
+F = C.POINTER(C.c_float)
+
+
+def fptr(a):
+    return a.ctypes.data_as(F)
+
+
+def test_forward_matches_oracle():
+    from method_b200 import _lib
+    L = _lib.load()
+    rng = np.random.default_rng(0)
+    P = M.init_params(1).astype(np.float32)
+    n = 300  # not a multiple of the 128-sample tile
+    x = rng.normal(size=(n, M.IN)).astype(np.float32)
+    y = np.zeros((n, M.OUT), dtype=np.float32)
+    assert L.mth_mlp_forward(fptr(P), n, fptr(x), fptr(y), 0) == 0
+    _, _, y_ref = M.loss_and_grad(P.astype(np.float64), x.astype(np.float64),
+                                  np.zeros((n, M.OUT)), bf=True)
+    err = np.abs(y - y_ref)
+    assert np.median(err) < 1e-4
+    assert np.all(err <= 2e-2 * (1 + np.abs(y_ref)))
+
+
+def test_gradient_matches_oracle():
+    from method_b200 import _lib
+    L = _lib.load()
+    rng = np.random.default_rng(5)
+    P = M.init_params(2).astype(np.float32)
+    n = 512
+    x = rng.normal(size=(n, M.IN)).astype(np.float32)
+    t = rng.normal(size=(n, M.OUT)).astype(np.float32)
+    g = np.zeros(M.NPARAM, dtype=np.float32)
+    loss = np.zeros(1, dtype=np.float32)
+    assert L.mth_mlp_grad(fptr(P), n, fptr(x), fptr(t), fptr(g), fptr(loss), 0) == 0
+    l_ref, g_ref, _ = M.loss_and_grad(P.astype(np.float64), x.astype(np.float64),
+                                      t.astype(np.float64), bf=True)
+    assert abs(loss[0] - l_ref) <= 1e-3 * l_ref
+    d, dr = M.unpack(g), M.unpack(g_ref)
+    for name, _ in M.SHAPES:
+        a, b = d[name].ravel(), dr[name].ravel()
+        if np.linalg.norm(b) == 0:
+            assert np.all(a == 0), name
+            continue
+        rel = np.linalg.norm(a - b) / np.linalg.norm(b)
+        cos = float(a @ b / (np.linalg.norm(a) * np.linalg.norm(b)))
+        assert rel < 2e-2 and cos > 0.9995, (name, rel, cos)
+
+
+@pytest.fixture(scope="module")
+def trained():
+    from method_b200 import _lib
+    L = _lib.load()
+    cfg = _lib.MlpTrainConfig(seed=7, n_samples=1 << 19, iterations=4000, batch=8192, lr=3e-3,
+                              gamma=4.0 / 3.0)
+    P = np.zeros(M.NPARAM, dtype=np.float32)
+    S = np.zeros(20, dtype=np.float32)
+    loss = np.zeros(1, dtype=np.float32)
+    assert L.mth_mlp_train(C.byref(cfg), fptr(P), fptr(S), fptr(loss), 0) == 0
+    return P, S, float(loss[0])
+
+
+def test_training_converges(trained):
+    _, _, loss = trained
+    # standardised targets: an untrained network sits near 1
+    assert loss < 2e-2, loss
+
+
+def test_network_guess_gain_over_cold_start(trained):
+    """Newton iterations per cell from the network's guess vs a cold start and
+    vs the previous-state guess (generating state perturbed by 1%); every cell
+    must converge and reproduce the generating state."""
+    import torch
+
+    from method_b200 import _lib
+    L = _lib.load()
+    P, S, _ = trained
+    n = 1 << 18
+    feat = np.zeros((n, 8), dtype=np.float32)
+    tgt = np.zeros((n, 2), dtype=np.float32)
+    cons = np.zeros((9, n))
+    prims = np.zeros((8, n))
+    D = C.POINTER(C.c_double)
+    assert L.mth_mlp_make_pairs(n, 12345, 4.0 / 3.0, fptr(feat), fptr(tgt),
+                                cons.ctypes.data_as(D), prims.ctypes.data_as(D), 0) == 0
+    gamma = 4.0 / 3.0
+    h = 1 + prims[4] / prims[0] * (gamma / (gamma - 1))
+    dc = torch.from_numpy(cons).cuda()
+    results = {}
+    for name, method, guess in (("hybrd_previous", 0, 0), ("newton_cold", 1, 2),
+                                ("newton_previous", 1, 0), ("newton_mlp", 1, 1)):
+        pg = prims.copy()  # previous state: rho, h 1% high, speed 1% low (stays below c)
+        pg[0] *= 1.01
+        pg[1:4] *= 0.99
+        ag = np.zeros((13, n))
+        ag[0] = h * 1.01
+        dp = torch.from_numpy(pg).cuda()
+        da = torch.from_numpy(ag).cuda()
+        st = _lib.C2PBatchStats()
+        rc = L.mth_c2p_batch(gamma, n, dc.data_ptr(), dp.data_ptr(), da.data_ptr(), method, guess,
+                             fptr(P), fptr(S), None, C.byref(st))
+        out = dp.cpu().numpy()
+        err = np.abs(out[0] - prims[0]) / prims[0]
+        results[name] = dict(rc=rc, iters=st.iterations / st.cells, unconverged=st.unconverged,
+                             fallbacks=st.fallbacks, med_rel_err_rho=float(np.nanmedian(err)),
+                             max_rel_err_rho=float(np.nanmax(err)))
+    print(results)
+    for name in ("newton_cold", "newton_previous", "newton_mlp"):
+        assert results[name]["unconverged"] == 0, (name, results[name])
+        assert results[name]["max_rel_err_rho"] < 1e-8, (name, results[name])
+    assert results["newton_mlp"]["iters"] < results["newton_cold"]["iters"]
+
+
+def test_mixed_form_with_network_guess(trained):
+    """OT 128^2 WENO5: the mixed form with the network guess converges every
+    cell and stays within 1e-6 (L1, relative) of the plain FP64 result."""
+    import method_b200 as mb
+    from method_b200 import initial
+    P, S, _ = trained
+    cfg = dict(model="srmhd", nx=128, ny=128, xmin=0.0, xmax=1.0, ymin=0.0, ymax=1.0, endTime=1.0,
+               cfl=0.4, Ng=4, gamma=4.0 / 3.0, weno=5, bcs="periodic", integrator="rk2")
+    prims0 = initial.orszag_tang(128, Ng=4)
+    plain = mb.Simulation(**cfg)
+    plain.set_prims(prims0)
+    plain.update_time(40)
+    net = mb.Simulation(precision="mixed", guess="mlp", **cfg)
+    net.set_mlp(P, S)
+    net.set_prims(prims0)
+    net.update_time(40)
+    st = net.stats()
+    assert st["c2p_unconverged"] == 0
+    cp, pp, _ = plain.state()
+    cn, pn, _ = net.state()
+    sl = (slice(None), slice(4, -4), slice(4, -4))
+    l1 = np.abs(cn[sl] - cp[sl]).sum() / np.abs(cp[sl]).sum()
+    assert l1 < 1e-6, l1
