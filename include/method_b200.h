@@ -61,6 +61,8 @@ typedef struct {
   long long steps;            /* time steps taken */
   double t, dt;               /* simulation time and last time step */
   int iters;                  /* Data::iters */
+  long long c2p_fallbacks;    /* mixed form: Newton cells that fell back (guess / Powell hybrid) */
+  long long implicit_fallbacks; /* mixed form: implicit cells re-solved by the Powell hybrid */
 } mth_stats;
 
 typedef struct mth_handle mth_handle;

@@ -58,6 +58,7 @@ class Stats(C.Structure):
         ("c2p_unconverged", C.c_longlong), ("implicit_cells", C.c_longlong),
         ("implicit_evals", C.c_longlong), ("implicit_failed", C.c_longlong),
         ("steps", C.c_longlong), ("t", C.c_double), ("dt", C.c_double), ("iters", C.c_int),
+        ("c2p_fallbacks", C.c_longlong), ("implicit_fallbacks", C.c_longlong),
     ]
 
 

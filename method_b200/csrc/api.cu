@@ -185,9 +185,12 @@ cudaError_t enqueue_step(mth_handle* h, double dt) {
     return cudaSuccess;
   }
   // SSP2::step (SSP2.cc:53-173).
-  if ((e = timed(h, "imex_stage1", 29, [&] {
-         return launch_imex_stage(h->g, 1, h->cons, h->aux, nullptr, nullptr, nullptr, h->u1, dt,
-                                  imex_work(h), h->st);
+  const bool fast = h->cfg.precision == MTH_MIXED;
+  if ((e = timed(h, fast ? "imex_newton_stage1" : "imex_hybrd_stage1", 29, [&] {
+         return fast ? launch_imex_fast(h->g, 1, h->cons, h->aux, nullptr, nullptr, nullptr,
+                                        h->u1, dt, imex_work(h), h->st)
+                     : launch_imex_stage(h->g, 1, h->cons, h->aux, nullptr, nullptr, nullptr,
+                                         h->u1, dt, imex_work(h), h->st);
        })))
     return e;
   if ((e = c2p(h, h->u1, h->prims, h->aux, h->prims, h->aux))) return e;
@@ -196,9 +199,11 @@ cudaError_t enqueue_step(mth_handle* h, double dt) {
        })))
     return e;
   if ((e = flux_stage(h, h->u1, h->prims, h->aux, nullptr, h->flux1, dt, STAGE_FNET))) return e;
-  if ((e = timed(h, "imex_stage2", 71, [&] {
-         return launch_imex_stage(h->g, 2, h->cons, h->aux, h->u1, h->flux1, h->src1, h->u2, dt,
-                                  imex_work(h), h->st);
+  if ((e = timed(h, fast ? "imex_newton_stage2" : "imex_hybrd_stage2", 71, [&] {
+         return fast ? launch_imex_fast(h->g, 2, h->cons, h->aux, h->u1, h->flux1, h->src1,
+                                        h->u2, dt, imex_work(h), h->st)
+                     : launch_imex_stage(h->g, 2, h->cons, h->aux, h->u1, h->flux1, h->src1,
+                                         h->u2, dt, imex_work(h), h->st);
        })))
     return e;
   if ((e = c2p(h, h->u2, h->prims, h->aux, h->prims, h->aux))) return e;
@@ -611,6 +616,8 @@ mth_status mth_get_stats(mth_handle* h, mth_stats* s) {
   s->t = h->t;
   s->dt = h->dt;
   s->iters = h->iters;
+  s->c2p_fallbacks = cnt[8] + cnt[9];
+  s->implicit_fallbacks = cnt[12];
   return st;
 }
 

@@ -442,6 +442,54 @@ constexpr double kImexTol = 0.000000149011612;
 constexpr double kImexGam = 0.2928932188134525;
 constexpr double kImexOm2Gam = 0.4142135623730950;
 
+// One cell of the implicit stage; returns the residual evaluations and sets
+// the error flag when hybrd1 did not converge.
+template <int STAGE>
+__device__ __forceinline__ long long imex_cell(const Grid& g, long long cell,
+                                               const double* __restrict__ cons,
+                                               const double* __restrict__ aux_guess,
+                                               const double* __restrict__ u1,
+                                               const double* __restrict__ flux1,
+                                               const double* __restrict__ source1,
+                                               double* __restrict__ out, double dt, C2PWork w) {
+  const long long N = g.Ntot;
+  double u[14], f1[14], s1[14], x[14], fv[14];
+#pragma unroll
+  for (int v = 0; v < 14; ++v) u[v] = cons[v * N + cell];
+  if (STAGE == 1) {
+#pragma unroll
+    for (int v = 0; v < 14; ++v) x[v] = u[v];
+  } else {
+#pragma unroll
+    for (int v = 0; v < 14; ++v) {
+      f1[v] = flux1[v * N + cell];
+      s1[v] = source1[v * N + cell];
+      x[v] = 0.5 * (u[v] + u1[v * N + cell] - dt * f1[v]);
+    }
+  }
+  srrmhd::ImexResidual R;
+  R.u = u;
+  R.flux1 = f1;
+  R.source1 = s1;
+  R.dt = dt;
+  R.gam = kImexGam;
+  R.om2gam = kImexOm2Gam;
+  R.g = g.gamma;
+  R.sigma = g.sigma;
+  R.cp = g.cp;
+  R.Z = aux_guess[10 * N + cell];
+  R.stage = STAGE;
+  R.evals = 0;
+  HybrdResult res = Hybrd<14>::solve(R, x, fv, kImexTol);
+#pragma unroll
+  for (int v = 0; v < 14; ++v) out[v * N + cell] = x[v];
+  if (res.info != 1) {
+    atomicAdd((unsigned long long*)&w.counters[2], 1ull);
+    atomicOr((unsigned long long*)&w.counters[3], (unsigned long long)ERR_IMPLICIT);
+  }
+  return res.nfev;
+}
+
 template <int STAGE>
 __global__ void __launch_bounds__(64)
     k_imex_stage(Grid g, const double* __restrict__ cons, const double* __restrict__ aux_guess,
@@ -453,42 +501,8 @@ __global__ void __launch_bounds__(64)
   if (t < n_interior(g)) {
     int i, j, k;
     interior_ijk(g, t, i, j, k);
-    const long long N = g.Ntot, cell = cell_id(g, i, j, k);
-    double u[14], f1[14], s1[14], x[14], fv[14];
-#pragma unroll
-    for (int v = 0; v < 14; ++v) u[v] = cons[v * N + cell];
-    if (STAGE == 1) {
-#pragma unroll
-      for (int v = 0; v < 14; ++v) x[v] = u[v];
-    } else {
-#pragma unroll
-      for (int v = 0; v < 14; ++v) {
-        f1[v] = flux1[v * N + cell];
-        s1[v] = source1[v * N + cell];
-        x[v] = 0.5 * (u[v] + u1[v * N + cell] - dt * f1[v]);
-      }
-    }
-    srrmhd::ImexResidual R;
-    R.u = u;
-    R.flux1 = f1;
-    R.source1 = s1;
-    R.dt = dt;
-    R.gam = kImexGam;
-    R.om2gam = kImexOm2Gam;
-    R.g = g.gamma;
-    R.sigma = g.sigma;
-    R.cp = g.cp;
-    R.Z = aux_guess[10 * N + cell];
-    R.stage = STAGE;
-    R.evals = 0;
-    HybrdResult res = Hybrd<14>::solve(R, x, fv, kImexTol);
-    evals = res.nfev;
-#pragma unroll
-    for (int v = 0; v < 14; ++v) out[v * N + cell] = x[v];
-    if (res.info != 1) {
-      atomicAdd((unsigned long long*)&w.counters[2], 1ull);
-      atomicOr((unsigned long long*)&w.counters[3], (unsigned long long)ERR_IMPLICIT);
-    }
+    evals = imex_cell<STAGE>(g, cell_id(g, i, j, k), cons, aux_guess, u1, flux1, source1, out,
+                             dt, w);
   }
   unsigned mask = __ballot_sync(0xffffffffu, t < n_interior(g));
   for (int o = 16; o > 0; o >>= 1) evals += __shfl_down_sync(0xffffffffu, evals, o);
@@ -497,6 +511,24 @@ __global__ void __launch_bounds__(64)
     atomicAdd((unsigned long long*)&w.counters[1], (unsigned long long)evals);
   }
 }
+
+// The same solve for the cells of a queue (mixed-form fallback).  One block
+// of 64 threads strides over the queue; the count is reset at the end by the
+// block after all threads finished reading it.
+template <int STAGE>
+__global__ void __launch_bounds__(64)
+    k_imex_stage_queued(Grid g, const double* __restrict__ cons,
+                        const double* __restrict__ aux_guess, const double* __restrict__ u1,
+                        const double* __restrict__ flux1, const double* __restrict__ source1,
+                        double* __restrict__ out, double dt, C2PWork w) {
+  const int n = *w.fail_count;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+    imex_cell<STAGE>(g, w.fail_list[q], cons, aux_guess, u1, flux1, source1, out, dt, w);
+    atomicAdd((unsigned long long*)&w.counters[3 + 5], 1ull);  // fallbacks (counters[8])
+  }
+}
+
+__global__ void k_reset_count(int* c) { *c = 0; }
 
 // SSP2 combination U += -0.5 dt (flux1 + flux2 - source1 - source2)
 // (SSP2.cc:155-166).
@@ -738,6 +770,18 @@ cudaError_t launch_imex_stage(const Grid& g, int stage, const double* cons,
   else
     k_imex_stage<2><<<blocks_for(nI, 64), 64, 0, st>>>(g, cons, aux_guess, u1, flux1, source1,
                                                         out, dt, w);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_imex_stage_queued(const Grid& g, int stage, const double* cons,
+                                     const double* aux_guess, const double* u1,
+                                     const double* flux1, const double* source1, double* out,
+                                     double dt, C2PWork w, cudaStream_t st) {
+  if (stage == 1)
+    k_imex_stage_queued<1><<<148, 64, 0, st>>>(g, cons, aux_guess, u1, flux1, source1, out, dt, w);
+  else
+    k_imex_stage_queued<2><<<148, 64, 0, st>>>(g, cons, aux_guess, u1, flux1, source1, out, dt, w);
+  k_reset_count<<<1, 1, 0, st>>>(w.fail_count);
   return cudaGetLastError();
 }
 

@@ -355,6 +355,111 @@ __global__ void __launch_bounds__(128)
   }
 }
 
+// SSP2 implicit stage of the mixed form (SRRMHD).  Both stages solve
+//   x = c + a S(x),  a = dt * gam,
+// with c = U^n (stage 1) or U^n - dt (flux1 - om2gam source1) (stage 2),
+// the residuals of SSP2.cc:194-264 rearranged.  Only E, psi, phi have
+// sources (srrmhd.cc:194-206): phi and psi are linear and solved in closed
+// form, charge and the other variables equal c, and E solves
+//   R(E) = E - c_E + a J(E),  J = q v + W sigma (E + v x B - (v.E) v),
+// by Newton steps with the Jacobian of the stiff term at frozen velocity,
+// (1 + a W sigma) I - a W sigma v v^T, inverted by Sherman-Morrison.  Every
+// residual runs the 1D Newton primitive recovery in Z.  A cell that does not
+// converge is queued for the reference Powell-hybrid stage kernel.
+constexpr double kGam = 0.2928932188134525;
+constexpr double kOm2Gam = 0.4142135623730950;
+
+__device__ __forceinline__ bool srrmhd_prims_newton(const double* x, double g, double& Z,
+                                                    double* v, double& W, int& its) {
+  const double Sb0 = x[1] - (x[9] * x[7] - x[10] * x[6]);
+  const double Sb1 = x[2] - (x[10] * x[5] - x[8] * x[7]);
+  const double Sb2 = x[3] - (x[8] * x[6] - x[9] * x[5]);
+  const double Sbsq = Sb0 * Sb0 + Sb1 * Sb1 + Sb2 * Sb2;
+  const double Bsq = x[5] * x[5] + x[6] * x[6] + x[7] * x[7];
+  const double Esq = x[8] * x[8] + x[9] * x[9] + x[10] * x[10];
+  const double tauB = x[4] - 0.5 * (Bsq + Esq);
+  if (!newton_srrmhd(Sbsq, x[0], tauB, g, Z, its)) return false;
+  const double vsq = Sbsq / (Z * Z);
+  W = 1.0 / sqrt(1 - vsq);
+  v[0] = Sb0 / Z;
+  v[1] = Sb1 / Z;
+  v[2] = Sb2 / Z;
+  return true;
+}
+
+template <int STAGE>
+__global__ void __launch_bounds__(128)
+    k_imex_fast(Grid g, const double* __restrict__ cons, const double* __restrict__ aux_guess,
+                const double* __restrict__ u1, const double* __restrict__ flux1,
+                const double* __restrict__ source1, double* __restrict__ out, double dt,
+                C2PWork w) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  long long its_total = 0;
+  if (t < n_interior(g)) {
+    int i, j, k;
+    interior_ijk(g, t, i, j, k);
+    const long long N = g.Ntot, cell = cell_id(g, i, j, k);
+    double c[14], x[14];
+#pragma unroll
+    for (int v = 0; v < 14; ++v) {
+      const double u = cons[v * N + cell];
+      c[v] = (STAGE == 1) ? u : u - dt * (flux1[v * N + cell] - kOm2Gam * source1[v * N + cell]);
+      x[v] = c[v];
+    }
+    const double a = dt * kGam, cp2 = g.cp * g.cp, sg = g.sigma;
+    x[12] = c[12] / (1 + a / cp2);
+    x[11] = (c[11] + a * c[13]) / (1 + a / cp2);
+    double Z = aux_guess[10 * N + cell];
+    int its = 0;
+    bool ok = false;
+    for (int it = 0; it < 50; ++it) {
+      double v[3], W;
+      if (!srrmhd_prims_newton(x, g.gamma, Z, v, W, its)) break;
+      const double q = x[13];
+      const double vE = v[0] * x[8] + v[1] * x[9] + v[2] * x[10];
+      const double vxB0 = v[1] * x[7] - v[2] * x[6];
+      const double vxB1 = v[2] * x[5] - v[0] * x[7];
+      const double vxB2 = v[0] * x[6] - v[1] * x[5];
+      const double Ws = W * sg;
+      double R[3];
+      R[0] = x[8] - c[8] + a * (q * v[0] + Ws * (x[8] + vxB0 - vE * v[0]));
+      R[1] = x[9] - c[9] + a * (q * v[1] + Ws * (x[9] + vxB1 - vE * v[1]));
+      R[2] = x[10] - c[10] + a * (q * v[2] + Ws * (x[10] + vxB2 - vE * v[2]));
+      // (alpha I - beta v v^T)^-1 R, alpha = 1 + a W sigma, beta = a W sigma
+      const double beta = a * Ws, alpha = 1 + beta;
+      const double vv = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+      const double vR = v[0] * R[0] + v[1] * R[1] + v[2] * R[2];
+      const double f = beta * vR / (alpha * (alpha - beta * vv));
+      double dE[3];
+      dE[0] = -(R[0] / alpha + f * v[0]);
+      dE[1] = -(R[1] / alpha + f * v[1]);
+      dE[2] = -(R[2] / alpha + f * v[2]);
+      x[8] += dE[0];
+      x[9] += dE[1];
+      x[10] += dE[2];
+      const double en = fabs(x[8]) + fabs(x[9]) + fabs(x[10]);
+      const double dn = fabs(dE[0]) + fabs(dE[1]) + fabs(dE[2]);
+      if (dn <= 1e-14 * en + 1e-300) {
+        ok = true;
+        break;
+      }
+    }
+    its_total = its;
+#pragma unroll
+    for (int v = 0; v < 14; ++v) out[v * N + cell] = x[v];
+    if (!ok) {
+      const int slot = atomicAdd(w.fail_count, 1);
+      w.fail_list[slot] = (int)cell;
+    }
+  }
+  const unsigned mask = __ballot_sync(0xffffffffu, t < n_interior(g));
+  for (int o = 16; o > 0; o >>= 1) its_total += __shfl_down_sync(0xffffffffu, its_total, o);
+  if ((threadIdx.x & 31) == 0 && mask) {
+    atomicAdd((unsigned long long*)&w.counters[0], (unsigned long long)__popc(mask));
+    atomicAdd((unsigned long long*)&w.counters[1], (unsigned long long)its_total);
+  }
+}
+
 template <class M, int ORDER, int TI>
 cudaError_t fvs2d_fp32_instance(const Grid& g, const double* cons, const double* prims,
                                 const double* aux, const double* u0, double* out, double dt,
@@ -412,6 +517,22 @@ cudaError_t launch_c2p_mixed(const Grid& g, int model, int guess, const double* 
     k_c2p_newton_srrmhd<<<blocks, 128, 0, st>>>(g, cons, aux_guess, prims, aux, w);
   }
   return cudaGetLastError();
+}
+
+cudaError_t launch_imex_fast(const Grid& g, int stage, const double* cons,
+                             const double* aux_guess, const double* u1, const double* flux1,
+                             const double* source1, double* out, double dt, C2PWork w,
+                             cudaStream_t st) {
+  const long long nI = (long long)(g.ie - g.is) * (g.je - g.js) * (g.ke - g.ks);
+  const int blocks = (int)((nI + 127) / 128);
+  if (stage == 1)
+    k_imex_fast<1><<<blocks, 128, 0, st>>>(g, cons, aux_guess, u1, flux1, source1, out, dt, w);
+  else
+    k_imex_fast<2><<<blocks, 128, 0, st>>>(g, cons, aux_guess, u1, flux1, source1, out, dt, w);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  // cells the fast solve could not converge: the reference stage solve
+  return launch_imex_stage_queued(g, stage, cons, aux_guess, u1, flux1, source1, out, dt, w, st);
 }
 
 cudaError_t mixed_init(MixedWork* w, const Grid& g, int model, cudaStream_t st) {

@@ -54,6 +54,12 @@ cudaError_t launch_imex_stage(const Grid& g, int stage, const double* cons,
                               const double* aux_guess, const double* u1, const double* flux1,
                               const double* source1, double* out, double dt, C2PWork w,
                               cudaStream_t st);
+// Reference SSP2 stage solve for the cells queued in w.fail_list (count in
+// w.fail_count, reset to zero afterwards).
+cudaError_t launch_imex_stage_queued(const Grid& g, int stage, const double* cons,
+                                     const double* aux_guess, const double* u1,
+                                     const double* flux1, const double* source1, double* out,
+                                     double dt, C2PWork w, cudaStream_t st);
 cudaError_t launch_ssp2_combine(const Grid& g, int nc, double* cons, const double* flux1,
                                 const double* flux2, const double* source1,
                                 const double* source2, double dt, cudaStream_t st);

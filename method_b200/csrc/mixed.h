@@ -27,6 +27,12 @@ cudaError_t launch_zguess(const Grid& g, long long n_cells, bool batch, const do
                           const float* P, const float* st, double* zguess, cudaStream_t s);
 }  // namespace mlp
 
+// SSP2 implicit stage of the mixed form (closed-form psi/phi, Newton on E).
+cudaError_t launch_imex_fast(const Grid& g, int stage, const double* cons,
+                             const double* aux_guess, const double* u1, const double* flux1,
+                             const double* source1, double* out, double dt, C2PWork w,
+                             cudaStream_t st);
+
 // Batched primitive recovery of independent cells (variable-major, stride n).
 // method: 0 Powell hybrid (reference), 1 Newton; guess: 0 previous state,
 // 1 network (zguess planes), 2 cold start.  counters: cells, iterations,
