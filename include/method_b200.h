@@ -232,6 +232,50 @@ mth_status mth_c2p_srmhd_noalloc(int nx, int ny, int nz, int Ng, double gamma,
  * mth_destroy. */
 mth_status mth_device_state(mth_handle* h, double** cons, double** prims, double** aux);
 
+/* ---- Ensembles: independent 2D simulations of uneven sizes advanced together.
+ * No counterpart in the reference, where each Simulation owns one grid and
+ * a parameter study runs them one after another.  Every member is a
+ * Simulation of its own configuration (its own grid, dt from its own CFL
+ * condition, t, iters: Simulation::updateTime per member); one ensemble step
+ * advances every member by one of its own time steps.  Members are SRMHD with
+ * MTH_RK2 (either precision) or SRRMHD with MTH_SSP2 (MTH_MIXED only); all
+ * share precision, WENO order and device; nz must be 0, ny > 0.  Each phase
+ * of the step is one persistent launch over a work list spanning all
+ * members, and the whole step is one CUDA graph (dt is computed on the
+ * device).  A member's results are identical to a single Simulation of the
+ * same configuration (plain: the reference's, bit for bit). */
+typedef struct mth_ensemble mth_ensemble;
+mth_status mth_ensemble_create(const mth_config* cfgs, int n, mth_ensemble** out);
+mth_status mth_ensemble_destroy(mth_ensemble* e);
+const char* mth_ensemble_last_error(const mth_ensemble* e);
+/* Initial primitive state of member m (host, Nprims*Nx*Ny*Nz doubles of that
+ * member); derives cons/aux, applies the boundaries, resets t and iters. */
+mth_status mth_ensemble_set_prims(mth_ensemble* e, int m, const double* prims_host);
+/* Host copies of member m's state (any pointer may be NULL). */
+mth_status mth_ensemble_download(mth_ensemble* e, int m, double* cons, double* prims,
+                                 double* aux);
+/* Installs a trained guess network (host arrays, MLP_NPARAM parameters and
+ * MLP_NSTAT statistics as mth_mlp_train returns them) for ensembles created
+ * with guess MTH_GUESS_MLP (precision MTH_MIXED): SRMHD members then start
+ * every primitive recovery from its guess, as mth_set_mlp does for one
+ * simulation. */
+mth_status mth_ensemble_set_mlp(mth_ensemble* e, const float* params, const float* stats);
+mth_status mth_ensemble_set_stream(mth_ensemble* e, void* stream);
+/* Times tile heights 4, 8, 16 (rows of 32 cells per flux tile) for each
+ * member size class (nx <= 96, <= 192, larger) on the ensemble's first flux
+ * phase, `reps` timed launches each, and keeps the fastest; the choice is
+ * returned in ti3 (may be NULL).  Runs flux kernels on the current state but
+ * changes no member's state. */
+mth_status mth_ensemble_autotune(mth_ensemble* e, int reps, int* ti3);
+/* Enqueues n_steps ensemble steps (asynchronous; see mth_ensemble_sync). */
+mth_status mth_ensemble_step(mth_ensemble* e, int n_steps);
+/* Waits for the enqueued steps; returns MTH_ERR_C2P / MTH_ERR_IMPLICIT if any
+ * member's solve failed (the reference's exceptions). */
+mth_status mth_ensemble_sync(mth_ensemble* e);
+mth_status mth_ensemble_stats(mth_ensemble* e, int m, mth_stats* s);
+/* Total interior cells of all members, and the tile heights in use. */
+mth_status mth_ensemble_info(const mth_ensemble* e, long long* interior_cells, int* ti3);
+
 #ifdef __cplusplus
 }
 #endif

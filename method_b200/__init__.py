@@ -25,7 +25,7 @@ INTEGRATORS = {"rk2": 0, "rksplit": 1, "ssp2": 2}
 PRECISIONS = {"fp64": 0, "mixed": 1}
 GUESSES = {"previous": 0, "mlp": 1}
 
-__all__ = ["Simulation", "MODELS", "BCS", "INTEGRATORS", "pin_host", "unpin_host"]
+__all__ = ["Simulation", "Ensemble", "MODELS", "BCS", "INTEGRATORS", "pin_host", "unpin_host"]
 
 
 def pin_host(arr):
@@ -47,6 +47,27 @@ def _dptr(a):
     return a.ctypes.data_as(C.POINTER(C.c_double))
 
 
+def _config(nx, ny, nz=0, xmin=0.0, xmax=1.0, ymin=0.0, ymax=1.0, zmin=0.0, zmax=1.0,
+            endTime=1.0, cfl=0.5, Ng=4, gamma=5.0 / 3.0, sigma=1e3, cp=0.1, model="srmhd",
+            weno=3, bcs="periodic", integrator="rk2", precision="fp64", guess="previous",
+            device=0):
+    """mth_config from the reference Data constructor's arguments plus the
+    class choices of a reference main.cc."""
+    c = _lib.Config()
+    c.model = MODELS[model]
+    c.nx, c.ny, c.nz = nx, ny, nz
+    c.xmin, c.xmax, c.ymin, c.ymax, c.zmin, c.zmax = xmin, xmax, ymin, ymax, zmin, zmax
+    c.endTime, c.cfl, c.Ng = endTime, cfl, Ng
+    c.gamma, c.sigma, c.cp = gamma, sigma, cp
+    c.weno_order = weno
+    c.bcs = BCS[bcs]
+    c.integrator = INTEGRATORS[integrator]
+    c.precision = PRECISIONS[precision]
+    c.guess = GUESSES[guess]
+    c.device = device
+    return c
+
+
 class Simulation:
     """One device-resident simulation (Data + Model + FVS + Bcs + integrator).
 
@@ -55,23 +76,9 @@ class Simulation:
     ``bcs``, ``integrator``, ``precision`` and ``guess``.
     """
 
-    def __init__(self, nx, ny, nz=0, xmin=0.0, xmax=1.0, ymin=0.0, ymax=1.0, zmin=0.0,
-                 zmax=1.0, endTime=1.0, cfl=0.5, Ng=4, gamma=5.0 / 3.0, sigma=1e3, cp=0.1,
-                 model="srmhd", weno=3, bcs="periodic", integrator="rk2", precision="fp64",
-                 guess="previous", device=0):
+    def __init__(self, nx, ny, nz=0, **kw):
         self.L = _lib.load()
-        c = _lib.Config()
-        c.model = MODELS[model]
-        c.nx, c.ny, c.nz = nx, ny, nz
-        c.xmin, c.xmax, c.ymin, c.ymax, c.zmin, c.zmax = xmin, xmax, ymin, ymax, zmin, zmax
-        c.endTime, c.cfl, c.Ng = endTime, cfl, Ng
-        c.gamma, c.sigma, c.cp = gamma, sigma, cp
-        c.weno_order = weno
-        c.bcs = BCS[bcs]
-        c.integrator = INTEGRATORS[integrator]
-        c.precision = PRECISIONS[precision]
-        c.guess = GUESSES[guess]
-        c.device = device
+        c = _config(nx, ny, nz, **kw)
         self.cfg = c
         h = C.c_void_p()
         rc = self.L.mth_create(C.byref(c), C.byref(h))
@@ -225,3 +232,110 @@ class Simulation:
     @property
     def t(self):
         return self.stats()["t"]
+
+
+class Ensemble:
+    """Independent 2D simulations of uneven sizes advanced together on one GPU.
+
+    ``members`` is a list of keyword dicts, each what ``Simulation`` takes.
+    One ``step()`` advances every member by one of its own time steps
+    (Simulation::updateTime per member: dt from each member's CFL condition,
+    clipped to its endTime).  Supported members: SRMHD + RK2 (fp64 or mixed)
+    and SRRMHD + SSP2 (mixed); all share precision, WENO order and device.
+    """
+
+    _NV = {0: (9, 8, 13), 1: (14, 11, 17)}
+
+    def __init__(self, members):
+        self.L = _lib.load()
+        cfgs = (_lib.Config * len(members))()
+        for i, kw in enumerate(members):
+            kw = dict(kw)
+            cfgs[i] = _config(kw.pop("nx"), kw.pop("ny"), kw.pop("nz", 0), **kw)
+        self.cfgs = cfgs
+        e = C.c_void_p()
+        rc = self.L.mth_ensemble_create(cfgs, len(members), C.byref(e))
+        if rc == 3:
+            raise ValueError("invalid ensemble configuration")
+        if rc != 0:
+            raise RuntimeError(f"mth_ensemble_create failed: {_lib.STATUS.get(rc, rc)}")
+        self.e = e
+        self.n = len(members)
+
+    def close(self):
+        if getattr(self, "e", None):
+            self.L.mth_ensemble_destroy(self.e)
+            self.e = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __len__(self):
+        return self.n
+
+    def _check(self, rc, what):
+        if rc == 0:
+            return
+        msg = self.L.mth_ensemble_last_error(self.e).decode()
+        if rc in (1, 2):
+            raise RuntimeError(f"{what}: {msg}")
+        if rc == 3:
+            raise ValueError(f"{what}: {msg}")
+        raise RuntimeError(f"{what}: CUDA error: {msg}")
+
+    def shape(self, m, which):
+        c = self.cfgs[m]
+        ng = 2 * c.Ng
+        nv = self._NV[c.model][which]
+        return (nv, c.nx + ng, c.ny + ng, 1)
+
+    def set_prims(self, m, prims):
+        prims = np.ascontiguousarray(prims, dtype=np.float64)
+        if prims.shape != self.shape(m, 1):
+            raise ValueError(f"prims of member {m} must have shape {self.shape(m, 1)}")
+        self._check(self.L.mth_ensemble_set_prims(self.e, m, _dptr(prims)), "set")
+
+    def state(self, m):
+        c, p, a = (np.zeros(self.shape(m, w)) for w in range(3))
+        self._check(self.L.mth_ensemble_download(self.e, m, _dptr(c), _dptr(p), _dptr(a)),
+                    "download")
+        return c, p, a
+
+    def autotune(self, reps=3):
+        """Picks the flux tile height per member size class; returns the three choices."""
+        ti = (C.c_int * 3)()
+        self._check(self.L.mth_ensemble_autotune(self.e, int(reps), ti), "autotune")
+        return list(ti)
+
+    def step(self, n=1, sync=True):
+        self._check(self.L.mth_ensemble_step(self.e, int(n)), "step")
+        if sync:
+            self.sync()
+
+    def sync(self):
+        self._check(self.L.mth_ensemble_sync(self.e), "step")
+
+    def set_mlp(self, params, stats):
+        """Installs a trained C2P guess network (members created with guess='mlp')."""
+        params = np.ascontiguousarray(params, dtype=np.float32)
+        stats = np.ascontiguousarray(stats, dtype=np.float32)
+        F = C.POINTER(C.c_float)
+        self._check(self.L.mth_ensemble_set_mlp(self.e, params.ctypes.data_as(F),
+                                                stats.ctypes.data_as(F)), "set_mlp")
+
+    def set_stream(self, stream_ptr):
+        self._check(self.L.mth_ensemble_set_stream(self.e, stream_ptr), "set_stream")
+
+    def stats(self, m):
+        s = _lib.Stats()
+        self._check(self.L.mth_ensemble_stats(self.e, m, C.byref(s)), "stats")
+        return {k: getattr(s, k) for k, _ in _lib.Stats._fields_}
+
+    def info(self):
+        n = C.c_longlong()
+        ti = (C.c_int * 3)()
+        self._check(self.L.mth_ensemble_info(self.e, C.byref(n), ti), "info")
+        return dict(interior_cells=n.value, tile_heights=list(ti))

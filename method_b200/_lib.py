@@ -23,7 +23,10 @@ SYMBOLS = [
     "mth_get_stats", "mth_reset_stats", "mth_step_host", "mth_pin_host", "mth_unpin_host",
     "mth_set_stream", "mth_profile_step", "mth_mlp_train", "mth_mlp_grad", "mth_mlp_forward",
     "mth_mlp_make_pairs", "mth_set_mlp", "mth_c2p_batch", "mth_c2p_srmhd_noalloc",
-    "mth_device_state",
+    "mth_device_state", "mth_ensemble_create", "mth_ensemble_destroy",
+    "mth_ensemble_last_error", "mth_ensemble_set_prims", "mth_ensemble_download",
+    "mth_ensemble_set_mlp", "mth_ensemble_set_stream", "mth_ensemble_autotune", "mth_ensemble_step",
+    "mth_ensemble_sync", "mth_ensemble_stats", "mth_ensemble_info",
 ]
 
 MLP_NPARAM = 9928
@@ -118,8 +121,22 @@ def load():
     L.mth_c2p_srmhd_noalloc.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
                                          C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                          C.c_void_p, C.c_void_p, C.c_void_p]
+    E = C.c_void_p
+    L.mth_ensemble_create.argtypes = [C.POINTER(Config), C.c_int, C.POINTER(E)]
+    L.mth_ensemble_destroy.argtypes = [E]
+    L.mth_ensemble_last_error.argtypes = [E]
+    L.mth_ensemble_set_prims.argtypes = [E, C.c_int, D]
+    L.mth_ensemble_download.argtypes = [E, C.c_int, D, D, D]
+    L.mth_ensemble_set_mlp.argtypes = [E, F, F]
+    L.mth_ensemble_set_stream.argtypes = [E, C.c_void_p]
+    L.mth_ensemble_autotune.argtypes = [E, C.c_int, C.POINTER(C.c_int)]
+    L.mth_ensemble_step.argtypes = [E, C.c_int]
+    L.mth_ensemble_sync.argtypes = [E]
+    L.mth_ensemble_stats.argtypes = [E, C.c_int, C.POINTER(Stats)]
+    L.mth_ensemble_info.argtypes = [E, C.POINTER(C.c_longlong), C.POINTER(C.c_int)]
     for n in SYMBOLS:
-        if n != "mth_last_error":
+        if n not in ("mth_last_error", "mth_ensemble_last_error"):
             getattr(L, n).restype = C.c_int
+    L.mth_ensemble_last_error.restype = C.c_char_p
     _LIB = L
     return L

@@ -9,6 +9,7 @@ Translation units and their floating-point contracts:
   kernels_mixed.cu  FMA allowed: FP32 flux path, Newton primitive recovery.
   mlp.cu            FMA allowed: guess-network inference / training kernels.
   api.cu            C-ABI, host logic only.
+  ensemble.cu       C-ABI of ensembles (work lists, autotuner, step graph).
   shim.cc           C++ mirror of the reference's class API over the C-ABI.
 """
 from __future__ import annotations
@@ -35,6 +36,7 @@ UNITS = [
     ("mlp.cu", []),
     ("api.cu", []),
     ("noalloc.cu", []),
+    ("ensemble.cu", []),
     ("shim.cc", []),
 ]
 

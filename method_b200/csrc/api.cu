@@ -287,29 +287,11 @@ mth_status read_status(mth_handle* h) {
 
 }  // namespace
 
-extern "C" {
-
-mth_status mth_create(const mth_config* cfg, mth_handle** out) {
-  if (!cfg || !out) return MTH_ERR_INVALID;
-  *out = nullptr;
-  mth_handle* h = new mth_handle();
-  h->cfg = *cfg;
-  const mth_config& c = *cfg;
-  // Validation of Data::initData (simData.cc:98-107) and the WENO ghost rule
-  // (weno.cc:13-20).
-  if (c.model != MTH_SRMHD && c.model != MTH_SRRMHD) {
-    delete h;
-    return MTH_ERR_INVALID;
-  }
-  if (c.sigma < 0.0 || (c.weno_order != 3 && c.weno_order != 5) ||
-      c.Ng < (c.weno_order + 1) / 2 + 1 || c.nx <= 0 || c.ny < 0 || c.nz < 0 ||
-      (c.ny == 0 && c.nz != 0) || c.bcs < 0 || c.bcs > 2 || c.integrator < 0 ||
-      c.integrator > 2 || (c.integrator == MTH_SSP2 && c.model != MTH_SRRMHD) ||
-      c.precision < 0 || c.precision > 1 || c.guess < 0 || c.guess > 1) {
-    delete h;
-    return MTH_ERR_INVALID;
-  }
-  Grid& g = h->g;
+namespace mth {
+bool grid_from_config(const void* cfg, Grid* out) {
+  const mth_config& c = *static_cast<const mth_config*>(cfg);
+  Grid& g = *out;
+  g = Grid{};
   g.nx = c.nx;
   g.ny = c.ny;
   g.nz = c.nz;
@@ -337,10 +319,9 @@ mth_status mth_create(const mth_config* cfg, mth_handle** out) {
   if (g.dims < 3) { g.ks = 0; g.ke = 1; }
   if (g.dims < 2) { g.js = 0; g.je = 1; }
   // Periodic ghost copies must come from interior cells.
-  if ((c.bcs == MTH_PERIODIC || c.bcs == MTH_FLOW) && c.nx < c.Ng) { delete h; return MTH_ERR_INVALID; }
+  if ((c.bcs == MTH_PERIODIC || c.bcs == MTH_FLOW) && c.nx < c.Ng) { return false; }
   if (c.bcs == MTH_PERIODIC && ((g.dims > 1 && c.ny < c.Ng) || (g.dims > 2 && c.nz < c.Ng))) {
-    delete h;
-    return MTH_ERR_INVALID;
+    return false;
   }
   g.bcx = c.bcs == MTH_OUTFLOW ? DIM_OUTFLOW : DIM_PERIODIC;
   g.bcy = g.dims > 1 ? (c.bcs == MTH_PERIODIC ? DIM_PERIODIC : DIM_OUTFLOW) : DIM_NONE;
@@ -352,6 +333,37 @@ mth_status mth_create(const mth_config* cfg, mth_handle** out) {
   g.sigma = c.sigma;
   g.cp = c.cp;
   g.Ntot = (long long)g.Nx * g.Ny * g.Nz;
+  return true;
+}
+}  // namespace mth
+
+extern "C" {
+
+mth_status mth_create(const mth_config* cfg, mth_handle** out) {
+  if (!cfg || !out) return MTH_ERR_INVALID;
+  *out = nullptr;
+  mth_handle* h = new mth_handle();
+  h->cfg = *cfg;
+  const mth_config& c = *cfg;
+  // Validation of Data::initData (simData.cc:98-107) and the WENO ghost rule
+  // (weno.cc:13-20).
+  if (c.model != MTH_SRMHD && c.model != MTH_SRRMHD) {
+    delete h;
+    return MTH_ERR_INVALID;
+  }
+  if (c.sigma < 0.0 || (c.weno_order != 3 && c.weno_order != 5) ||
+      c.Ng < (c.weno_order + 1) / 2 + 1 || c.nx <= 0 || c.ny < 0 || c.nz < 0 ||
+      (c.ny == 0 && c.nz != 0) || c.bcs < 0 || c.bcs > 2 || c.integrator < 0 ||
+      c.integrator > 2 || (c.integrator == MTH_SSP2 && c.model != MTH_SRRMHD) ||
+      c.precision < 0 || c.precision > 1 || c.guess < 0 || c.guess > 1) {
+    delete h;
+    return MTH_ERR_INVALID;
+  }
+  if (!grid_from_config(&c, &h->g)) {
+    delete h;
+    return MTH_ERR_INVALID;
+  }
+  const Grid& g = h->g;
   h->NC = c.model == MTH_SRMHD ? 9 : 14;
   h->NP = c.model == MTH_SRMHD ? 8 : 11;
   h->NA = c.model == MTH_SRMHD ? 13 : 17;

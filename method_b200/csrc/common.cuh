@@ -40,6 +40,19 @@ __host__ __device__ inline long long cell_id(const Grid& g, int i, int j, int k)
   return ((long long)i * g.Ny + j) * g.Nz + k;
 }
 
+// Interior cell number t (k fastest) -> (i, j, k), and the interior count.
+__device__ __forceinline__ void interior_ijk(const Grid& g, long long t, int& i, int& j, int& k) {
+  const int nk = g.ke - g.ks, nj = g.je - g.js;
+  k = g.ks + (int)(t % nk);
+  t /= nk;
+  j = g.js + (int)(t % nj);
+  i = g.is + (int)(t / nj);
+}
+
+__device__ __forceinline__ long long n_interior(const Grid& g) {
+  return (long long)(g.ie - g.is) * (g.je - g.js) * (g.ke - g.ks);
+}
+
 // Maps an index of one direction onto the interior cell whose value the
 // reference's boundary pass would have copied there.
 __host__ __device__ inline int map_dim(int i, int n, int Ng, int kind) {

@@ -87,20 +87,22 @@ __device__ __forceinline__ void split_cell(const Grid& g, const double* __restri
   }
 }
 
+// One TI x 32 tile (tile row ti, tile column tj) of the fused stage; the
+// whole CTA participates and `smem_raw` holds Fvs2dSmem::bytes.
 template <class M, typename R, int ORDER, int TI>
-__global__ void __launch_bounds__(32 * TI)
-    k_fvs2d(Grid g, const double* __restrict__ cons, const double* __restrict__ prims,
-            const double* __restrict__ aux, const double* u0, double* out, double dt,
-            int mode) {
+__device__ __forceinline__ void fvs2d_tile(const Grid& g, const double* __restrict__ cons,
+                                           const double* __restrict__ prims,
+                                           const double* __restrict__ aux, const double* u0,
+                                           double* out, double dt, int mode, int ti, int tj,
+                                           unsigned char* smem_raw) {
   using S = Fvs2dSmem<M, R, ORDER, TI>;
   constexpr int NC = M::NC, TJ = S::TJ, H = S::H, NT = 32 * TI;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
   R* sp = reinterpret_cast<R*>(smem_raw);
   R* sm = sp + NC * S::RMAX;
   R* sr = sm + NC * S::RMAX;
 
   const int lane = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + lane;
-  const int i0 = g.is + blockIdx.y * TI, j0 = g.js + blockIdx.x * TJ;
+  const int i0 = g.is + ti * TI, j0 = g.js + tj * TJ;
   const int ci = i0 + ty, cj = j0 + lane;
   R acc[NC];
 
@@ -146,29 +148,38 @@ __global__ void __launch_bounds__(32 * TI)
     sr[v * S::FY + rem] = weno_face<ORDER, R>(P, Mm, 1, fj + H - (ORDER == 3 ? 2 : 3));
   }
   __syncthreads();
-  if (ci >= g.ie || cj >= g.je) return;
-  {
+  if (ci < g.ie && cj < g.je) {
     const R dy = R(g.dy);
 #pragma unroll
     for (int v = 0; v < NC; ++v)
       acc[v] = acc[v] + (sr[v * S::FY + ty * (TJ + 1) + lane + 1] / dy -
                          sr[v * S::FY + ty * (TJ + 1) + lane] / dy);
-  }
 
-  // ---------------- stage update ----------------
-  const long long cell = cell_id(g, ci, cj, 0);
+    // ---------------- stage update ----------------
+    const long long cell = cell_id(g, ci, cj, 0);
 #pragma unroll
-  for (int v = 0; v < NC; ++v) {
-    const long long o = (long long)v * g.Ntot + cell;
-    const double fn = (double)acc[v];
-    if (mode == STAGE_FNET) {
-      out[o] = fn;
-    } else if (mode == STAGE_EULER) {
-      out[o] = cons[o] - dt * fn;
-    } else {
-      out[o] = 0.5 * (u0[o] + cons[o] - dt * fn);
+    for (int v = 0; v < NC; ++v) {
+      const long long o = (long long)v * g.Ntot + cell;
+      const double fn = (double)acc[v];
+      if (mode == STAGE_FNET) {
+        out[o] = fn;
+      } else if (mode == STAGE_EULER) {
+        out[o] = cons[o] - dt * fn;
+      } else {
+        out[o] = 0.5 * (u0[o] + cons[o] - dt * fn);
+      }
     }
   }
+}
+
+template <class M, typename R, int ORDER, int TI>
+__global__ void __launch_bounds__(32 * TI)
+    k_fvs2d(Grid g, const double* __restrict__ cons, const double* __restrict__ prims,
+            const double* __restrict__ aux, const double* u0, double* out, double dt,
+            int mode) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  fvs2d_tile<M, R, ORDER, TI>(g, cons, prims, aux, u0, out, dt, mode, blockIdx.y, blockIdx.x,
+                              smem_raw);
 }
 
 }  // namespace mth

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include "common.cuh"
+#include "ensemble.h"
 #include "fvs2d.cuh"
 #include "launch.h"
 #include "minpack.cuh"
@@ -18,18 +19,6 @@ namespace {
 constexpr int kThreads = 256;
 
 inline int blocks_for(long long n, int t = kThreads) { return (int)((n + t - 1) / t); }
-
-__device__ __forceinline__ void interior_ijk(const Grid& g, long long t, int& i, int& j, int& k) {
-  const int nk = g.ke - g.ks, nj = g.je - g.js;
-  k = g.ks + (int)(t % nk);
-  t /= nk;
-  j = g.js + (int)(t % nj);
-  i = g.is + (int)(t / nj);
-}
-
-__device__ __forceinline__ long long n_interior(const Grid& g) {
-  return (long long)(g.ie - g.is) * (g.je - g.js) * (g.ke - g.ks);
-}
 
 // ---------------------------------------------------------------------------
 // primsToAll over every cell (srmhd.cc:573-673, srrmhd.cc:358-510).
@@ -159,6 +148,48 @@ __global__ void k_stage_update(Grid g, int nc, int mode, const double* u0,
 // for the neighbour-average retry.
 constexpr double kSrmhdTol = 1.49011612e-7;
 
+// One interior cell: returns the residual evaluations; a failure is queued.
+__device__ __forceinline__ long long c2p_srmhd_hybrd_cell(const Grid& g, long long cell,
+                                                          const double* __restrict__ cons,
+                                                          const double* prims_guess,
+                                                          const double* aux_guess,
+                                                          double* prims, double* aux,
+                                                          double* __restrict__ solution,
+                                                          int* fail_list, int* fail_count) {
+  const long long N = g.Ntot;
+  double c[9];
+#pragma unroll
+  for (int v = 0; v < 9; ++v) c[v] = cons[v * N + cell];
+  double pg[4];
+#pragma unroll
+  for (int v = 0; v < 4; ++v) pg[v] = prims_guess[v * N + cell];
+  double hg = aux_guess[cell];
+  srmhd::Residual R = srmhd::residual_args(c, g.gamma);
+  double x[2], fv[2];
+  srmhd::guess_from_prims(pg, hg, x);
+  HybrdResult res = Hybrd<2>::solve(R, x, fv, kSrmhdTol);
+  if (res.info == 1) {
+    solution[cell] = x[0];
+    solution[N + cell] = x[1];
+    double p[8], a[13];
+    srmhd::from_solution(c, x, g.gamma, R.BS, R.Bsq, R.Ssq, p, a);
+#pragma unroll
+    for (int v = 0; v < 8; ++v) prims[v * N + cell] = p[v];
+#pragma unroll
+    for (int v = 0; v < 13; ++v) aux[v * N + cell] = a[v];
+  } else {
+    prims[5 * N + cell] = c[5];
+    prims[6 * N + cell] = c[6];
+    prims[7 * N + cell] = c[7];
+    aux[10 * N + cell] = R.BS;
+    aux[11 * N + cell] = R.Bsq;
+    aux[12 * N + cell] = R.Ssq;
+    int slot = atomicAdd(fail_count, 1);
+    fail_list[slot] = (int)cell;
+  }
+  return res.nfev;
+}
+
 __global__ void __launch_bounds__(128)
     k_c2p_srmhd(Grid g, const double* __restrict__ cons, const double* prims_guess,
                 const double* aux_guess, double* prims, double* aux,
@@ -168,38 +199,8 @@ __global__ void __launch_bounds__(128)
   if (t < n_interior(g)) {
     int i, j, k;
     interior_ijk(g, t, i, j, k);
-    const long long N = g.Ntot, cell = cell_id(g, i, j, k);
-    double c[9];
-#pragma unroll
-    for (int v = 0; v < 9; ++v) c[v] = cons[v * N + cell];
-    double pg[4];
-#pragma unroll
-    for (int v = 0; v < 4; ++v) pg[v] = prims_guess[v * N + cell];
-    double hg = aux_guess[cell];
-    srmhd::Residual R = srmhd::residual_args(c, g.gamma);
-    double x[2], fv[2];
-    srmhd::guess_from_prims(pg, hg, x);
-    HybrdResult res = Hybrd<2>::solve(R, x, fv, kSrmhdTol);
-    nfev = res.nfev;
-    if (res.info == 1) {
-      solution[cell] = x[0];
-      solution[N + cell] = x[1];
-      double p[8], a[13];
-      srmhd::from_solution(c, x, g.gamma, R.BS, R.Bsq, R.Ssq, p, a);
-#pragma unroll
-      for (int v = 0; v < 8; ++v) prims[v * N + cell] = p[v];
-#pragma unroll
-      for (int v = 0; v < 13; ++v) aux[v * N + cell] = a[v];
-    } else {
-      prims[5 * N + cell] = c[5];
-      prims[6 * N + cell] = c[6];
-      prims[7 * N + cell] = c[7];
-      aux[10 * N + cell] = R.BS;
-      aux[11 * N + cell] = R.Bsq;
-      aux[12 * N + cell] = R.Ssq;
-      int slot = atomicAdd(w.fail_count, 1);
-      w.fail_list[slot] = (int)cell;
-    }
+    nfev = c2p_srmhd_hybrd_cell(g, cell_id(g, i, j, k), cons, prims_guess, aux_guess, prims, aux,
+                                solution, w.fail_list, w.fail_count);
   }
   // one atomic per warp for the statistics
   unsigned mask = __ballot_sync(0xffffffffu, t < n_interior(g));
@@ -214,12 +215,12 @@ __global__ void __launch_bounds__(128)
 // at a time in (i, j, k) order as the reference does.  The reference solves
 // the retry with the residual arguments left over from the last interior cell
 // of the first pass; that behaviour is kept so that results stay identical.
-__global__ void k_c2p_retry_srmhd(Grid g, const double* __restrict__ cons, double* prims,
-                                  double* aux, double* solution, C2PWork w) {
-  if (threadIdx.x != 0) return;
-  const int n = *w.fail_count;
+__device__ void c2p_retry_body(const Grid& g, const double* __restrict__ cons, double* prims,
+                               double* aux, double* solution, int* fail_list, int* fail_count,
+                               long long* counters) {
+  const int n = *fail_count;
   if (n == 0) return;
-  int* L = w.fail_list;
+  int* L = fail_list;
   // heap sort of the failed cell ids (ascending = the reference's loop order)
   for (int s = n / 2 - 1; s >= 0; --s) {
     for (int r = s;;) {
@@ -282,9 +283,15 @@ __global__ void k_c2p_retry_srmhd(Grid g, const double* __restrict__ cons, doubl
     for (int v = 0; v < 8; ++v) prims[v * N + cell] = p[v];
     for (int v = 0; v < 13; ++v) aux[v * N + cell] = a[v];
   }
-  w.counters[1] += nfev;
-  w.counters[2] += still;
-  *w.fail_count = 0;
+  counters[1] += nfev;
+  counters[2] += still;
+  *fail_count = 0;
+}
+
+__global__ void k_c2p_retry_srmhd(Grid g, const double* __restrict__ cons, double* prims,
+                                  double* aux, double* solution, C2PWork w) {
+  if (threadIdx.x != 0) return;
+  c2p_retry_body(g, cons, prims, aux, solution, w.fail_list, w.fail_count, w.counters);
 }
 
 // RKSplit source step: target += dt * S(cons) on the interior (rkSplit.cc:31-53).
@@ -630,6 +637,158 @@ cudaError_t fvs2d_instance(const Grid& g, const double* cons, const double* prim
   return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// Ensemble kernels: CTAs stride over a work list covering every member.
+template <class M, int ORDER, int TI>
+__global__ void __launch_bounds__(32 * TI)
+    k_ens_fvs_fp64(const Member* __restrict__ mem, const Item* __restrict__ items, int n_items,
+                   int ic, int ip, int ia, int iu0, int iout, int mode) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
+    const Item w = items[it];
+    const Member& d = mem[w.m];
+    const Grid g = d.g;
+    fvs2d_tile<M, double, ORDER, TI>(g, d.a[ic], d.a[ip], d.a[ia], iu0 >= 0 ? d.a[iu0] : nullptr,
+                                     d.a[iout], d.dt, mode, w.a, w.b, smem_raw);
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(128)
+    k_ens_c2p_srmhd_hybrd(const Member* __restrict__ mem, const Item* __restrict__ items,
+                          int n_items, int ic, int ipg, int iag, int ip, int ia) {
+  for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
+    const Item w = items[it];
+    const Member& d = mem[w.m];
+    const Grid g = d.g;
+    const long long t = w.a + threadIdx.x;
+    long long nfev = 0;
+    if (t < n_interior(g)) {
+      int i, j, k;
+      interior_ijk(g, t, i, j, k);
+      nfev = c2p_srmhd_hybrd_cell(g, cell_id(g, i, j, k), d.a[ic], d.a[ipg], d.a[iag], d.a[ip],
+                                  d.a[ia], d.a[EA_SOL], d.fail_list, d.fail_count);
+    }
+    const unsigned mask = __ballot_sync(0xffffffffu, t < n_interior(g));
+    for (int o = 16; o > 0; o >>= 1) nfev += __shfl_down_sync(0xffffffffu, nfev, o);
+    if ((threadIdx.x & 31) == 0 && mask) {
+      atomicAdd((unsigned long long*)&d.counters[0], (unsigned long long)__popc(mask));
+      atomicAdd((unsigned long long*)&d.counters[1], (unsigned long long)nfev);
+    }
+  }
+}
+
+// One CTA per member: the member's neighbour-average retry.
+__global__ void k_ens_c2p_retry(const Member* __restrict__ mem, int ic, int ip, int ia) {
+  if (threadIdx.x != 0) return;
+  const Member& d = mem[blockIdx.x];
+  if (d.model != MODEL_SRMHD) return;
+  const Grid g = d.g;
+  c2p_retry_body(g, d.a[ic], d.a[ip], d.a[ia], d.a[EA_SOL], d.fail_list, d.fail_count,
+                 d.counters);
+}
+
+// One CTA per SRRMHD member: the cells of the member's queue that the
+// mixed-form implicit solve left unconverged, solved as the reference does
+// (the ensemble counterpart of k_imex_stage_queued).
+template <int STAGE>
+__global__ void __launch_bounds__(64) k_ens_imex_queued(const Member* __restrict__ mem) {
+  const Member& d = mem[blockIdx.x];
+  if (d.model != MODEL_SRRMHD) return;
+  const Grid g = d.g;
+  const C2PWork w{d.fail_list, d.fail_count, d.counters + 4};
+  const int n = *d.fail_count;
+  for (int q = threadIdx.x; q < n; q += blockDim.x) {
+    imex_cell<STAGE>(g, d.fail_list[q], d.a[EA_CONS], d.a[EA_AUX], d.a[EA_U1], d.a[EA_F1],
+                     d.a[EA_S1], d.a[STAGE == 1 ? EA_U1 : EA_U2], d.dt, w);
+    atomicAdd((unsigned long long*)&w.counters[8], 1ull);  // implicit fallbacks
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) *d.fail_count = 0;
+}
+
+// SRRMHD source of the interior cells of every SRRMHD member (srrmhd.cc:194-206);
+// here, without contraction, so that members match k_source bit for bit.
+__global__ void __launch_bounds__(128)
+    k_ens_source(const Member* __restrict__ mem, const Item* __restrict__ items, int n_items,
+                 int ic, int ia, int iout) {
+  for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
+    const Item w = items[it];
+    const Member& d = mem[w.m];
+    const Grid g = d.g;
+    const long long t = w.a + threadIdx.x;
+    if (t >= n_interior(g)) continue;
+    int i, j, k;
+    interior_ijk(g, t, i, j, k);
+    const long long N = g.Ntot, cell = cell_id(g, i, j, k);
+    double c[14], a[17], s[14];
+#pragma unroll
+    for (int v = 0; v < 14; ++v) c[v] = d.a[ic][v * N + cell];
+#pragma unroll
+    for (int v = 0; v < 17; ++v) a[v] = d.a[ia][v * N + cell];
+    srrmhd::source(c, a, g.cp, s);
+#pragma unroll
+    for (int v = 0; v < 14; ++v) d.a[iout][v * N + cell] = s[v];
+  }
+}
+
+// SSP2 combination (SSP2.cc:155-166) of every SRRMHD member, as k_ssp2_combine.
+__global__ void __launch_bounds__(128)
+    k_ens_combine(const Member* __restrict__ mem, const Item* __restrict__ items, int n_items) {
+  for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
+    const Item w = items[it];
+    const Member& d = mem[w.m];
+    const Grid g = d.g;
+    const long long t = w.a + threadIdx.x;
+    if (t >= n_interior(g)) continue;
+    int i, j, k;
+    interior_ijk(g, t, i, j, k);
+    const long long cell = cell_id(g, i, j, k);
+    for (int v = 0; v < 14; ++v) {
+      const long long o = v * g.Ntot + cell;
+      d.a[EA_CONS][o] += -0.5 * d.dt *
+                         (d.a[EA_F1][o] + d.a[EA_F2][o] - d.a[EA_S1][o] - d.a[EA_S2][o]);
+    }
+  }
+}
+
+// Simulation::updateTime's dt for every member (simulation.cc:113-124); the
+// expression is the host's, compiled without contraction.
+__global__ void k_ens_dt(Member* mem, int n) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= n) return;
+  Member& d = mem[m];
+  const Grid& g = d.g;
+  double dtX(d.cfl * g.dx / (1.0 * sqrt((double)g.dims)));
+  double dtY(d.cfl * g.dy / (1.0 * sqrt((double)g.dims)));
+  double dtZ(d.cfl * g.dz / (1.0 * sqrt((double)g.dims)));
+  double dt = (dtX <= dtY && dtX <= dtZ) ? dtX : ((dtY < dtZ) ? dtY : dtZ);
+  if (d.iters < 15) dt *= 0.1;
+  if (d.iters >= 15 && d.iters < 30) dt *= 0.25;
+  if (d.t + dt > d.endTime) dt = d.endTime - d.t;
+  d.dt = dt;
+}
+
+__global__ void k_ens_advance(Member* mem, int n) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= n) return;
+  mem[m].t += mem[m].dt;
+  mem[m].iters++;
+}
+
+template <class M, int ORDER, int TI>
+cudaError_t ens_fvs_fp64_instance(const Member* mem, const Item* items, int n, int ic, int ip,
+                                  int ia, int iu0, int iout, int mode, int grid,
+                                  cudaStream_t st) {
+  using S = Fvs2dSmem<M, double, ORDER, TI>;
+  auto kern = k_ens_fvs_fp64<M, ORDER, TI>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)S::bytes);
+  if (e != cudaSuccess) return e;
+  kern<<<grid, dim3(32, TI), S::bytes, st>>>(mem, items, n, ic, ip, ia, iu0, iout, mode);
+  return cudaGetLastError();
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -791,6 +950,66 @@ cudaError_t launch_ssp2_combine(const Grid& g, int nc, double* cons, const doubl
   const long long nI = (long long)(g.ie - g.is) * (g.je - g.js) * (g.ke - g.ks);
   k_ssp2_combine<<<blocks_for(nI), kThreads, 0, st>>>(g, nc, cons, flux1, flux2, source1, source2,
                                                       dt);
+  return cudaGetLastError();
+}
+
+cudaError_t ens_fvs_fp64(const Member* mem, const Item* items, int n, int model, int order,
+                         int TI, int ic, int ip, int ia, int iu0, int iout, int mode, int grid,
+                         cudaStream_t st) {
+#define ENS_FVS(MM, O, T) \
+  return ens_fvs_fp64_instance<MM, O, T>(mem, items, n, ic, ip, ia, iu0, iout, mode, grid, st)
+  if (model == MODEL_SRMHD) {
+    if (order == 3) {
+      if (TI == 4) ENS_FVS(SRMHD, 3, 4);
+      if (TI == 16) ENS_FVS(SRMHD, 3, 16);
+      ENS_FVS(SRMHD, 3, 8);
+    }
+    if (TI == 4) ENS_FVS(SRMHD, 5, 4);
+    if (TI == 16) ENS_FVS(SRMHD, 5, 16);
+    ENS_FVS(SRMHD, 5, 8);
+  }
+  return cudaErrorInvalidValue;  // plain-form ensembles are SRMHD
+#undef ENS_FVS
+}
+
+cudaError_t ens_c2p_srmhd_hybrd(const Member* mem, const Item* items, int n, int ic, int ipg,
+                                int iag, int ip, int ia, int grid, cudaStream_t st) {
+  k_ens_c2p_srmhd_hybrd<<<grid, 128, 0, st>>>(mem, items, n, ic, ipg, iag, ip, ia);
+  return cudaGetLastError();
+}
+
+cudaError_t ens_c2p_retry(const Member* mem, int n_members, int ic, int ip, int ia,
+                          cudaStream_t st) {
+  k_ens_c2p_retry<<<n_members, 32, 0, st>>>(mem, ic, ip, ia);
+  return cudaGetLastError();
+}
+
+cudaError_t ens_imex_queued(const Member* mem, int n_members, int stage, cudaStream_t st) {
+  if (stage == 1)
+    k_ens_imex_queued<1><<<n_members, 64, 0, st>>>(mem);
+  else
+    k_ens_imex_queued<2><<<n_members, 64, 0, st>>>(mem);
+  return cudaGetLastError();
+}
+
+cudaError_t ens_source(const Member* mem, const Item* items, int n, int ic, int ia, int iout,
+                       int grid, cudaStream_t st) {
+  k_ens_source<<<grid, 128, 0, st>>>(mem, items, n, ic, ia, iout);
+  return cudaGetLastError();
+}
+
+cudaError_t ens_combine(const Member* mem, const Item* items, int n, int grid, cudaStream_t st) {
+  k_ens_combine<<<grid, 128, 0, st>>>(mem, items, n);
+  return cudaGetLastError();
+}
+
+cudaError_t ens_dt(Member* mem, int n, cudaStream_t st) {
+  k_ens_dt<<<(n + 127) / 128, 128, 0, st>>>(mem, n);
+  return cudaGetLastError();
+}
+
+cudaError_t ens_advance(Member* mem, int n, cudaStream_t st) {
+  k_ens_advance<<<(n + 127) / 128, 128, 0, st>>>(mem, n);
   return cudaGetLastError();
 }
 

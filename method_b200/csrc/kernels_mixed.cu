@@ -15,6 +15,7 @@
 #include <cuda_runtime.h>
 
 #include "common.cuh"
+#include "ensemble.h"
 #include "fvs2d.cuh"
 #include "launch.h"
 #include "minpack.cuh"
@@ -25,18 +26,6 @@
 namespace mth {
 
 namespace {
-
-__device__ __forceinline__ void interior_ijk(const Grid& g, long long t, int& i, int& j, int& k) {
-  const int nk = g.ke - g.ks, nj = g.je - g.js;
-  k = g.ks + (int)(t % nk);
-  t /= nk;
-  j = g.js + (int)(t % nj);
-  i = g.is + (int)(t / nj);
-}
-
-__device__ __forceinline__ long long n_interior(const Grid& g) {
-  return (long long)(g.ie - g.is) * (g.je - g.js) * (g.ke - g.ks);
-}
 
 // Newton in Z for SRMHD, safeguarded by a bracket.  v^2(Z) above is strictly
 // decreasing for Z > 0, so "v^2 >= 1 or g < 0" marks the left of the root
@@ -133,72 +122,153 @@ __device__ __forceinline__ bool newton_srrmhd(double Sb2, double D, double tauT,
   return false;
 }
 
+struct NewtonTally {
+  long long its = 0, fb_prev = 0, fb_hybrd = 0, bad = 0;
+};
+
+// Mixed-form SRMHD recovery of one cell (Newton in Z, fallbacks).
+__device__ __forceinline__ void c2p_srmhd_newton_cell(const Grid& g, long long cell,
+                                                      int guess_mode,
+                                                      const double* __restrict__ cons,
+                                                      const double* prims_guess,
+                                                      const double* aux_guess, double* prims,
+                                                      double* aux, double* __restrict__ solution,
+                                                      const double* __restrict__ zguess,
+                                                      NewtonTally& tl) {
+  const long long N = g.Ntot;
+  double c[9];
+#pragma unroll
+  for (int v = 0; v < 9; ++v) c[v] = cons[v * N + cell];
+  srmhd::Residual R = srmhd::residual_args(c, g.gamma);
+  const double BS2 = R.BS * R.BS;
+  double pg[4];
+#pragma unroll
+  for (int v = 0; v < 4; ++v) pg[v] = prims_guess[v * N + cell];
+  double prev[2];
+  srmhd::guess_from_prims(pg, aux_guess[cell], prev);
+  double Z = prev[1], vsq = prev[0];
+  int it = 0;
+  bool ok = false;
+  if (guess_mode == 1 && zguess) {
+    Z = zguess[cell];
+    ok = newton_srmhd(R.D, R.tau, BS2, R.Bsq, R.Ssq, g.gamma, Z, vsq, it);
+    if (!ok) {
+      tl.fb_prev += 1;
+      Z = prev[1];
+    }
+  }
+  if (!ok) ok = newton_srmhd(R.D, R.tau, BS2, R.Bsq, R.Ssq, g.gamma, Z, vsq, it);
+  double x[2] = {vsq, Z};
+  if (!ok) {
+    tl.fb_hybrd += 1;
+    x[0] = prev[0];
+    x[1] = prev[1];
+    double fv[2];
+    HybrdResult res = Hybrd<2>::solve(R, x, fv, 1.49011612e-7);
+    it += res.nfev;
+    if (res.info != 1) tl.bad += 1;
+  }
+  tl.its += it;
+  solution[cell] = x[0];
+  solution[N + cell] = x[1];
+  double p[8], a[13];
+  srmhd::from_solution(c, x, g.gamma, R.BS, R.Bsq, R.Ssq, p, a);
+#pragma unroll
+  for (int v = 0; v < 8; ++v) prims[v * N + cell] = p[v];
+#pragma unroll
+  for (int v = 0; v < 13; ++v) aux[v * N + cell] = a[v];
+}
+
+__device__ __forceinline__ void tally_flush(NewtonTally tl, bool active, long long* counters) {
+  const unsigned mask = __ballot_sync(0xffffffffu, active);
+  for (int o = 16; o > 0; o >>= 1) {
+    tl.its += __shfl_down_sync(0xffffffffu, tl.its, o);
+    tl.fb_prev += __shfl_down_sync(0xffffffffu, tl.fb_prev, o);
+    tl.fb_hybrd += __shfl_down_sync(0xffffffffu, tl.fb_hybrd, o);
+    tl.bad += __shfl_down_sync(0xffffffffu, tl.bad, o);
+  }
+  if ((threadIdx.x & 31) == 0 && mask) {
+    atomicAdd((unsigned long long*)&counters[0], (unsigned long long)__popc(mask));
+    atomicAdd((unsigned long long*)&counters[1], (unsigned long long)tl.its);
+    if (tl.bad) {
+      atomicAdd((unsigned long long*)&counters[2], (unsigned long long)tl.bad);
+    }
+    if (tl.fb_prev) atomicAdd((unsigned long long*)&counters[8], (unsigned long long)tl.fb_prev);
+    if (tl.fb_hybrd) atomicAdd((unsigned long long*)&counters[9], (unsigned long long)tl.fb_hybrd);
+  }
+}
+
 __global__ void __launch_bounds__(128)
     k_c2p_newton_srmhd(Grid g, int guess_mode, const double* __restrict__ cons,
                        const double* prims_guess, const double* aux_guess, double* prims,
                        double* aux, double* __restrict__ solution, C2PWork w,
                        const double* __restrict__ zguess) {
   long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  long long its = 0, fb_prev = 0, fb_hybrd = 0, bad = 0;
+  NewtonTally tl;
   if (t < n_interior(g)) {
     int i, j, k;
     interior_ijk(g, t, i, j, k);
-    const long long N = g.Ntot, cell = cell_id(g, i, j, k);
-    double c[9];
-#pragma unroll
-    for (int v = 0; v < 9; ++v) c[v] = cons[v * N + cell];
-    srmhd::Residual R = srmhd::residual_args(c, g.gamma);
-    const double BS2 = R.BS * R.BS;
-    double pg[4];
-#pragma unroll
-    for (int v = 0; v < 4; ++v) pg[v] = prims_guess[v * N + cell];
-    double prev[2];
-    srmhd::guess_from_prims(pg, aux_guess[cell], prev);
-    double Z = prev[1], vsq = prev[0];
-    int it = 0;
-    bool ok = false;
-    if (guess_mode == 1 && zguess) {
-      Z = zguess[cell];
-      ok = newton_srmhd(R.D, R.tau, BS2, R.Bsq, R.Ssq, g.gamma, Z, vsq, it);
-      if (!ok) {
-        fb_prev = 1;
-        Z = prev[1];
-      }
-    }
-    if (!ok) ok = newton_srmhd(R.D, R.tau, BS2, R.Bsq, R.Ssq, g.gamma, Z, vsq, it);
-    double x[2] = {vsq, Z};
-    if (!ok) {
-      fb_hybrd = 1;
-      x[0] = prev[0];
-      x[1] = prev[1];
-      double fv[2];
-      HybrdResult res = Hybrd<2>::solve(R, x, fv, 1.49011612e-7);
-      it += res.nfev;
-      if (res.info != 1) bad = 1;
-    }
-    its = it;
-    solution[cell] = x[0];
-    solution[N + cell] = x[1];
-    double p[8], a[13];
-    srmhd::from_solution(c, x, g.gamma, R.BS, R.Bsq, R.Ssq, p, a);
-#pragma unroll
-    for (int v = 0; v < 8; ++v) prims[v * N + cell] = p[v];
-#pragma unroll
-    for (int v = 0; v < 13; ++v) aux[v * N + cell] = a[v];
+    c2p_srmhd_newton_cell(g, cell_id(g, i, j, k), guess_mode, cons, prims_guess, aux_guess, prims,
+                          aux, solution, zguess, tl);
   }
-  unsigned mask = __ballot_sync(0xffffffffu, t < n_interior(g));
-  for (int o = 16; o > 0; o >>= 1) {
-    its += __shfl_down_sync(0xffffffffu, its, o);
-    fb_prev += __shfl_down_sync(0xffffffffu, fb_prev, o);
-    fb_hybrd += __shfl_down_sync(0xffffffffu, fb_hybrd, o);
-    bad += __shfl_down_sync(0xffffffffu, bad, o);
+  tally_flush(tl, t < n_interior(g), w.counters);
+}
+
+// Mixed-form SRRMHD recovery of one cell (Newton in Z, secant fallback).
+__device__ __forceinline__ void c2p_srrmhd_newton_cell(const Grid& g, long long cell,
+                                                       const double* __restrict__ cons,
+                                                       const double* aux_guess, double* prims,
+                                                       double* aux, NewtonTally& tl,
+                                                       long long* counters) {
+  const long long N = g.Ntot;
+  double c[14], p[11], a[17];
+#pragma unroll
+  for (int v = 0; v < 14; ++v) c[v] = cons[v * N + cell];
+  const double gm = g.gamma;
+  p[5] = c[5]; p[6] = c[6]; p[7] = c[7];
+  p[8] = c[8]; p[9] = c[9]; p[10] = c[10];
+  a[7] = c[5] * c[5] + c[6] * c[6] + c[7] * c[7];
+  a[8] = c[8] * c[8] + c[9] * c[9] + c[10] * c[10];
+  a[12] = c[1] - (c[9] * c[7] - c[10] * c[6]);
+  a[13] = c[2] - (c[10] * c[5] - c[8] * c[7]);
+  a[14] = c[3] - (c[8] * c[6] - c[9] * c[5]);
+  a[15] = a[12] * a[12] + a[13] * a[13] + a[14] * a[14];
+  a[16] = c[4] - 0.5 * (a[7] + a[8]);
+  double Z = aux_guess[10 * N + cell];
+  int it = 0;
+  bool ok = newton_srrmhd(a[15], c[0], a[16], gm, Z, it);
+  bool bad = false;
+  if (!ok) {
+    tl.fb_hybrd += 1;
+    Z = aux_guess[10 * N + cell];
+    ok = srrmhd::z_secant(Z, a[15], c[0], a[16], gm, it);
+    if (!ok) bad = true;
   }
-  if ((threadIdx.x & 31) == 0 && mask) {
-    atomicAdd((unsigned long long*)&w.counters[0], (unsigned long long)__popc(mask));
-    atomicAdd((unsigned long long*)&w.counters[1], (unsigned long long)its);
-    if (bad) atomicAdd((unsigned long long*)&w.counters[2], (unsigned long long)bad);
-    if (fb_prev) atomicAdd((unsigned long long*)&w.counters[8], (unsigned long long)fb_prev);
-    if (fb_hybrd) atomicAdd((unsigned long long*)&w.counters[9], (unsigned long long)fb_hybrd);
+  tl.its += it;
+  a[10] = Z;
+  a[9] = a[15] / (a[10] * a[10]);
+  a[1] = 1.0 / sqrt(1 - a[9]);
+  p[0] = c[0] / a[1];
+  a[0] = a[10] / (p[0] * a[1] * a[1]);
+  a[2] = (a[0] - 1) / gm;
+  a[3] = sqrt((a[2] * gm * (gm - 1)) / a[0]);
+  p[4] = p[0] * a[2] * (gm - 1);
+  p[1] = a[12] / a[10];
+  p[2] = a[13] / a[10];
+  p[3] = a[14] / a[10];
+  a[11] = p[1] * c[8] + p[2] * c[9] + p[3] * c[10];
+  const double sg = g.sigma;
+  a[4] = c[13] * p[1] + a[1] * sg * (c[8] + (p[2] * c[7] - p[3] * c[6]) - a[11] * p[1]);
+  a[5] = c[13] * p[2] + a[1] * sg * (c[9] + (p[3] * c[5] - p[1] * c[7]) - a[11] * p[2]);
+  a[6] = c[13] * p[3] + a[1] * sg * (c[10] + (p[1] * c[6] - p[2] * c[5]) - a[11] * p[3]);
+  if (bad) {
+    tl.bad += 1;
+    atomicOr((unsigned long long*)&counters[3], (unsigned long long)ERR_C2P);
+  } else {
+#pragma unroll
+    for (int v = 0; v < 11; ++v) prims[v * N + cell] = p[v];
+#pragma unroll
+    for (int v = 0; v < 17; ++v) aux[v * N + cell] = a[v];
   }
 }
 
@@ -206,72 +276,13 @@ __global__ void __launch_bounds__(128)
     k_c2p_newton_srrmhd(Grid g, const double* __restrict__ cons, const double* aux_guess,
                         double* prims, double* aux, C2PWork w) {
   long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  long long its = 0, fb = 0, bad = 0;
+  NewtonTally tl;
   if (t < n_interior(g)) {
     int i, j, k;
     interior_ijk(g, t, i, j, k);
-    const long long N = g.Ntot, cell = cell_id(g, i, j, k);
-    double c[14], p[11], a[17];
-#pragma unroll
-    for (int v = 0; v < 14; ++v) c[v] = cons[v * N + cell];
-    const double gm = g.gamma;
-    p[5] = c[5]; p[6] = c[6]; p[7] = c[7];
-    p[8] = c[8]; p[9] = c[9]; p[10] = c[10];
-    a[7] = c[5] * c[5] + c[6] * c[6] + c[7] * c[7];
-    a[8] = c[8] * c[8] + c[9] * c[9] + c[10] * c[10];
-    a[12] = c[1] - (c[9] * c[7] - c[10] * c[6]);
-    a[13] = c[2] - (c[10] * c[5] - c[8] * c[7]);
-    a[14] = c[3] - (c[8] * c[6] - c[9] * c[5]);
-    a[15] = a[12] * a[12] + a[13] * a[13] + a[14] * a[14];
-    a[16] = c[4] - 0.5 * (a[7] + a[8]);
-    double Z = aux_guess[10 * N + cell];
-    int it = 0;
-    bool ok = newton_srrmhd(a[15], c[0], a[16], gm, Z, it);
-    if (!ok) {
-      fb = 1;
-      Z = aux_guess[10 * N + cell];
-      ok = srrmhd::z_secant(Z, a[15], c[0], a[16], gm, it);
-      if (!ok) bad = 1;
-    }
-    its = it;
-    a[10] = Z;
-    a[9] = a[15] / (a[10] * a[10]);
-    a[1] = 1.0 / sqrt(1 - a[9]);
-    p[0] = c[0] / a[1];
-    a[0] = a[10] / (p[0] * a[1] * a[1]);
-    a[2] = (a[0] - 1) / gm;
-    a[3] = sqrt((a[2] * gm * (gm - 1)) / a[0]);
-    p[4] = p[0] * a[2] * (gm - 1);
-    p[1] = a[12] / a[10];
-    p[2] = a[13] / a[10];
-    p[3] = a[14] / a[10];
-    a[11] = p[1] * c[8] + p[2] * c[9] + p[3] * c[10];
-    const double sg = g.sigma;
-    a[4] = c[13] * p[1] + a[1] * sg * (c[8] + (p[2] * c[7] - p[3] * c[6]) - a[11] * p[1]);
-    a[5] = c[13] * p[2] + a[1] * sg * (c[9] + (p[3] * c[5] - p[1] * c[7]) - a[11] * p[2]);
-    a[6] = c[13] * p[3] + a[1] * sg * (c[10] + (p[1] * c[6] - p[2] * c[5]) - a[11] * p[3]);
-    if (!bad) {
-#pragma unroll
-      for (int v = 0; v < 11; ++v) prims[v * N + cell] = p[v];
-#pragma unroll
-      for (int v = 0; v < 17; ++v) aux[v * N + cell] = a[v];
-    }
+    c2p_srrmhd_newton_cell(g, cell_id(g, i, j, k), cons, aux_guess, prims, aux, tl, w.counters);
   }
-  unsigned mask = __ballot_sync(0xffffffffu, t < n_interior(g));
-  for (int o = 16; o > 0; o >>= 1) {
-    its += __shfl_down_sync(0xffffffffu, its, o);
-    fb += __shfl_down_sync(0xffffffffu, fb, o);
-    bad += __shfl_down_sync(0xffffffffu, bad, o);
-  }
-  if ((threadIdx.x & 31) == 0 && mask) {
-    atomicAdd((unsigned long long*)&w.counters[0], (unsigned long long)__popc(mask));
-    atomicAdd((unsigned long long*)&w.counters[1], (unsigned long long)its);
-    if (fb) atomicAdd((unsigned long long*)&w.counters[9], (unsigned long long)fb);
-    if (bad) {
-      atomicAdd((unsigned long long*)&w.counters[2], (unsigned long long)bad);
-      atomicOr((unsigned long long*)&w.counters[3], (unsigned long long)ERR_C2P);
-    }
-  }
+  tally_flush(tl, t < n_interior(g), w.counters);
 }
 
 // Batched SRMHD primitive recovery for independent cells.
@@ -387,70 +398,84 @@ __device__ __forceinline__ bool srrmhd_prims_newton(const double* x, double g, d
   return true;
 }
 
+// One cell of the mixed-form implicit stage; returns false when Newton on E
+// did not converge (out then holds the last iterate).
+template <int STAGE>
+__device__ __forceinline__ bool imex_fast_cell(const Grid& g, long long cell,
+                                               const double* __restrict__ cons,
+                                               const double* __restrict__ aux_guess,
+                                               const double* __restrict__ flux1,
+                                               const double* __restrict__ source1,
+                                               double* __restrict__ out, double dt, int& its) {
+  const long long N = g.Ntot;
+  double c[14], x[14];
+#pragma unroll
+  for (int v = 0; v < 14; ++v) {
+    const double u = cons[v * N + cell];
+    c[v] = (STAGE == 1) ? u : u - dt * (flux1[v * N + cell] - kOm2Gam * source1[v * N + cell]);
+    x[v] = c[v];
+  }
+  const double a = dt * kGam, cp2 = g.cp * g.cp, sg = g.sigma;
+  x[12] = c[12] / (1 + a / cp2);
+  x[11] = (c[11] + a * c[13]) / (1 + a / cp2);
+  double Z = aux_guess[10 * N + cell];
+  bool ok = false;
+  for (int it = 0; it < 50; ++it) {
+    double v[3], W;
+    if (!srrmhd_prims_newton(x, g.gamma, Z, v, W, its)) break;
+    const double q = x[13];
+    const double vE = v[0] * x[8] + v[1] * x[9] + v[2] * x[10];
+    const double vxB0 = v[1] * x[7] - v[2] * x[6];
+    const double vxB1 = v[2] * x[5] - v[0] * x[7];
+    const double vxB2 = v[0] * x[6] - v[1] * x[5];
+    const double Ws = W * sg;
+    double R[3];
+    R[0] = x[8] - c[8] + a * (q * v[0] + Ws * (x[8] + vxB0 - vE * v[0]));
+    R[1] = x[9] - c[9] + a * (q * v[1] + Ws * (x[9] + vxB1 - vE * v[1]));
+    R[2] = x[10] - c[10] + a * (q * v[2] + Ws * (x[10] + vxB2 - vE * v[2]));
+    // (alpha I - beta v v^T)^-1 R, alpha = 1 + a W sigma, beta = a W sigma
+    const double beta = a * Ws, alpha = 1 + beta;
+    const double vv = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+    const double vR = v[0] * R[0] + v[1] * R[1] + v[2] * R[2];
+    const double f = beta * vR / (alpha * (alpha - beta * vv));
+    double dE[3];
+    dE[0] = -(R[0] / alpha + f * v[0]);
+    dE[1] = -(R[1] / alpha + f * v[1]);
+    dE[2] = -(R[2] / alpha + f * v[2]);
+    x[8] += dE[0];
+    x[9] += dE[1];
+    x[10] += dE[2];
+    const double en = fabs(x[8]) + fabs(x[9]) + fabs(x[10]);
+    const double dn = fabs(dE[0]) + fabs(dE[1]) + fabs(dE[2]);
+    if (dn <= 1e-14 * en + 1e-300) {
+      ok = true;
+      break;
+    }
+  }
+#pragma unroll
+  for (int v = 0; v < 14; ++v) out[v * N + cell] = x[v];
+  return ok;
+}
+
 template <int STAGE>
 __global__ void __launch_bounds__(128)
     k_imex_fast(Grid g, const double* __restrict__ cons, const double* __restrict__ aux_guess,
                 const double* __restrict__ u1, const double* __restrict__ flux1,
                 const double* __restrict__ source1, double* __restrict__ out, double dt,
                 C2PWork w) {
+  (void)u1;
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   long long its_total = 0;
   if (t < n_interior(g)) {
     int i, j, k;
     interior_ijk(g, t, i, j, k);
-    const long long N = g.Ntot, cell = cell_id(g, i, j, k);
-    double c[14], x[14];
-#pragma unroll
-    for (int v = 0; v < 14; ++v) {
-      const double u = cons[v * N + cell];
-      c[v] = (STAGE == 1) ? u : u - dt * (flux1[v * N + cell] - kOm2Gam * source1[v * N + cell]);
-      x[v] = c[v];
-    }
-    const double a = dt * kGam, cp2 = g.cp * g.cp, sg = g.sigma;
-    x[12] = c[12] / (1 + a / cp2);
-    x[11] = (c[11] + a * c[13]) / (1 + a / cp2);
-    double Z = aux_guess[10 * N + cell];
+    const long long cell = cell_id(g, i, j, k);
     int its = 0;
-    bool ok = false;
-    for (int it = 0; it < 50; ++it) {
-      double v[3], W;
-      if (!srrmhd_prims_newton(x, g.gamma, Z, v, W, its)) break;
-      const double q = x[13];
-      const double vE = v[0] * x[8] + v[1] * x[9] + v[2] * x[10];
-      const double vxB0 = v[1] * x[7] - v[2] * x[6];
-      const double vxB1 = v[2] * x[5] - v[0] * x[7];
-      const double vxB2 = v[0] * x[6] - v[1] * x[5];
-      const double Ws = W * sg;
-      double R[3];
-      R[0] = x[8] - c[8] + a * (q * v[0] + Ws * (x[8] + vxB0 - vE * v[0]));
-      R[1] = x[9] - c[9] + a * (q * v[1] + Ws * (x[9] + vxB1 - vE * v[1]));
-      R[2] = x[10] - c[10] + a * (q * v[2] + Ws * (x[10] + vxB2 - vE * v[2]));
-      // (alpha I - beta v v^T)^-1 R, alpha = 1 + a W sigma, beta = a W sigma
-      const double beta = a * Ws, alpha = 1 + beta;
-      const double vv = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
-      const double vR = v[0] * R[0] + v[1] * R[1] + v[2] * R[2];
-      const double f = beta * vR / (alpha * (alpha - beta * vv));
-      double dE[3];
-      dE[0] = -(R[0] / alpha + f * v[0]);
-      dE[1] = -(R[1] / alpha + f * v[1]);
-      dE[2] = -(R[2] / alpha + f * v[2]);
-      x[8] += dE[0];
-      x[9] += dE[1];
-      x[10] += dE[2];
-      const double en = fabs(x[8]) + fabs(x[9]) + fabs(x[10]);
-      const double dn = fabs(dE[0]) + fabs(dE[1]) + fabs(dE[2]);
-      if (dn <= 1e-14 * en + 1e-300) {
-        ok = true;
-        break;
-      }
-    }
-    its_total = its;
-#pragma unroll
-    for (int v = 0; v < 14; ++v) out[v * N + cell] = x[v];
-    if (!ok) {
+    if (!imex_fast_cell<STAGE>(g, cell, cons, aux_guess, flux1, source1, out, dt, its)) {
       const int slot = atomicAdd(w.fail_count, 1);
       w.fail_list[slot] = (int)cell;
     }
+    its_total = its;
   }
   const unsigned mask = __ballot_sync(0xffffffffu, t < n_interior(g));
   for (int o = 16; o > 0; o >>= 1) its_total += __shfl_down_sync(0xffffffffu, its_total, o);
@@ -458,6 +483,93 @@ __global__ void __launch_bounds__(128)
     atomicAdd((unsigned long long*)&w.counters[0], (unsigned long long)__popc(mask));
     atomicAdd((unsigned long long*)&w.counters[1], (unsigned long long)its_total);
   }
+}
+
+// ---------------------------------------------------------------------------
+// Ensemble kernels (mixed form).
+template <class M, int ORDER, int TI>
+__global__ void __launch_bounds__(32 * TI)
+    k_ens_fvs_fp32(const Member* __restrict__ mem, const Item* __restrict__ items, int n_items,
+                   int ic, int ip, int ia, int iu0, int iout, int mode) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
+    const Item w = items[it];
+    const Member& d = mem[w.m];
+    const Grid g = d.g;
+    fvs2d_tile<M, float, ORDER, TI>(g, d.a[ic], d.a[ip], d.a[ia], iu0 >= 0 ? d.a[iu0] : nullptr,
+                                    d.a[iout], d.dt, mode, w.a, w.b, smem_raw);
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(128)
+    k_ens_c2p_newton(const Member* __restrict__ mem, const Item* __restrict__ items, int n_items,
+                     int guess_mode, int ic, int ipg, int iag, int ip, int ia) {
+  for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
+    const Item w = items[it];
+    const Member& d = mem[w.m];
+    const Grid g = d.g;
+    const long long t = w.a + threadIdx.x;
+    const bool act = t < n_interior(g);
+    NewtonTally tl;
+    if (act) {
+      int i, j, k;
+      interior_ijk(g, t, i, j, k);
+      const long long cell = cell_id(g, i, j, k);
+      if (d.model == MODEL_SRMHD)
+        c2p_srmhd_newton_cell(g, cell, guess_mode, d.a[ic], d.a[ipg], d.a[iag], d.a[ip],
+                              d.a[ia], d.a[EA_SOL], guess_mode ? d.a[EA_ZG] : nullptr, tl);
+      else
+        c2p_srrmhd_newton_cell(g, cell, d.a[ic], d.a[iag], d.a[ip], d.a[ia], tl, d.counters);
+    }
+    tally_flush(tl, act, d.counters);
+  }
+}
+
+template <int STAGE>
+__global__ void __launch_bounds__(128)
+    k_ens_imex_fast(const Member* __restrict__ mem, const Item* __restrict__ items, int n_items) {
+  for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
+    const Item w = items[it];
+    const Member& d = mem[w.m];
+    const Grid g = d.g;
+    const long long t = w.a + threadIdx.x;
+    const bool act = t < n_interior(g);
+    long long its_total = 0;
+    if (act) {
+      int i, j, k;
+      interior_ijk(g, t, i, j, k);
+      int its = 0;
+      const long long cell = cell_id(g, i, j, k);
+      const bool ok = imex_fast_cell<STAGE>(g, cell, d.a[EA_CONS], d.a[EA_AUX], d.a[EA_F1],
+                                            d.a[EA_S1], d.a[STAGE == 1 ? EA_U1 : EA_U2], d.dt,
+                                            its);
+      its_total = its;
+      if (!ok) {  // queued for the reference solve (ens_imex_queued)
+        const int slot = atomicAdd(d.fail_count, 1);
+        d.fail_list[slot] = (int)cell;
+      }
+    }
+    const unsigned mask = __ballot_sync(0xffffffffu, act);
+    for (int o = 16; o > 0; o >>= 1) its_total += __shfl_down_sync(0xffffffffu, its_total, o);
+    if ((threadIdx.x & 31) == 0 && mask) {
+      atomicAdd((unsigned long long*)&d.counters[4], (unsigned long long)__popc(mask));
+      atomicAdd((unsigned long long*)&d.counters[5], (unsigned long long)its_total);
+    }
+  }
+}
+
+template <class M, int ORDER, int TI>
+cudaError_t ens_fvs_fp32_instance(const Member* mem, const Item* items, int n, int ic, int ip,
+                                  int ia, int iu0, int iout, int mode, int grid,
+                                  cudaStream_t st) {
+  using S = Fvs2dSmem<M, float, ORDER, TI>;
+  auto kern = k_ens_fvs_fp32<M, ORDER, TI>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)S::bytes);
+  if (e != cudaSuccess) return e;
+  kern<<<grid, dim3(32, TI), S::bytes, st>>>(mem, items, n, ic, ip, ia, iu0, iout, mode);
+  return cudaGetLastError();
 }
 
 template <class M, int ORDER, int TI>
@@ -476,6 +588,50 @@ cudaError_t fvs2d_fp32_instance(const Grid& g, const double* cons, const double*
 }
 
 }  // namespace
+
+cudaError_t ens_fvs_fp32(const Member* mem, const Item* items, int n, int model, int order,
+                         int TI, int ic, int ip, int ia, int iu0, int iout, int mode, int grid,
+                         cudaStream_t st) {
+#define ENS_FVS(MM, O, T) \
+  return ens_fvs_fp32_instance<MM, O, T>(mem, items, n, ic, ip, ia, iu0, iout, mode, grid, st)
+  if (model == MODEL_SRMHD) {
+    if (order == 3) {
+      if (TI == 4) ENS_FVS(SRMHD, 3, 4);
+      if (TI == 16) ENS_FVS(SRMHD, 3, 16);
+      ENS_FVS(SRMHD, 3, 8);
+    }
+    if (TI == 4) ENS_FVS(SRMHD, 5, 4);
+    if (TI == 16) ENS_FVS(SRMHD, 5, 16);
+    ENS_FVS(SRMHD, 5, 8);
+  }
+  if (order == 3) {
+    if (TI == 4) ENS_FVS(SRRMHD, 3, 4);
+    if (TI == 16) ENS_FVS(SRRMHD, 3, 16);
+    ENS_FVS(SRRMHD, 3, 8);
+  }
+  if (TI == 4) ENS_FVS(SRRMHD, 5, 4);
+  if (TI == 16) ENS_FVS(SRRMHD, 5, 16);
+  ENS_FVS(SRRMHD, 5, 8);
+#undef ENS_FVS
+}
+
+cudaError_t ens_c2p_newton(const Member* mem, const Item* items, int n, int model,
+                           int guess_mode, int ic, int ipg, int iag, int ip, int ia, int grid,
+                           cudaStream_t st) {
+  k_ens_c2p_newton<<<grid, 128, 0, st>>>(mem, items, n, model == MODEL_SRMHD ? guess_mode : 0,
+                                         ic, ipg, iag, ip, ia);
+  return cudaGetLastError();
+}
+
+cudaError_t ens_imex_fast(const Member* mem, const Item* items, int n, int stage, int grid,
+                          cudaStream_t st) {
+  if (stage == 1)
+    k_ens_imex_fast<1><<<grid, 128, 0, st>>>(mem, items, n);
+  else
+    k_ens_imex_fast<2><<<grid, 128, 0, st>>>(mem, items, n);
+  return cudaGetLastError();
+}
+
 
 cudaError_t launch_fvs2d_fp32(const Grid& g, int model, int order, const double* cons,
                               const double* prims, const double* aux, const double* u0,

@@ -20,6 +20,10 @@ enum ErrFlag : long long {
   ERR_IMPLICIT = 2,  // implicit source solve did not converge
 };
 
+// Data::initData geometry (simData.cc:61-97) for a configuration; returns
+// false for a configuration the reference rejects.  `c` is an mth_config.
+bool grid_from_config(const void* c, Grid* g);
+
 // ---- plain FP64 (bit-compatible with the reference) --------------------------
 cudaError_t launch_prims_to_all(const Grid& g, int model, const double* prims, double* cons,
                                 double* aux, cudaStream_t st);

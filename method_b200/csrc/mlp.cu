@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "ensemble.h"
 #include "launch.h"
 #include "mixed.h"
 #include "mlp.cuh"
@@ -357,6 +358,61 @@ __global__ void k_standardise(long long n, float* __restrict__ feat, float* __re
 
 }  // namespace
 
+// Ensembles: the guess for the cells of every SRMHD member.  Persistent
+// CTAs load the weights once and stride over the 128-cell work items (one
+// item = one ROWS-sample tile); outputs go to the member's EA_ZG planes
+// (Z, v^2) exactly as k_mlp_zguess writes a single grid's.
+__global__ void __launch_bounds__(256) k_ens_mlp_zguess(const Member* __restrict__ mem,
+                                                        const Item* __restrict__ items,
+                                                        int n_items, int ic,
+                                                        const float* __restrict__ P,
+                                                        const float* __restrict__ st) {
+  extern __shared__ __align__(16) unsigned char raw[];
+  Smem& s = *reinterpret_cast<Smem*>(raw);
+  load_weights(s, P, st);
+  __shared__ double Dcell[ROWS];
+  __shared__ long long cellid[ROWS];
+  for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
+    const Item w = items[it];
+    const Member& d = mem[w.m];
+    const Grid g = d.g;
+    __syncthreads();  // weights loaded / previous item's outputs consumed
+    if (threadIdx.x < ROWS) {
+      const long long t = w.a + threadIdx.x;
+      float f[IN] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+      long long cell = -1;
+      double D = 1.0;
+      if (t < n_interior(g)) {
+        int i, j, k;
+        interior_ijk(g, t, i, j, k);
+        cell = cell_id(g, i, j, k);
+        const double* cons = d.a[ic];
+        double c[9];
+#pragma unroll
+        for (int v = 0; v < 9; ++v) c[v] = cons[v * g.Ntot + cell];
+        D = c[0];
+        features_srmhd(c, f);
+      }
+      cellid[threadIdx.x] = cell;
+      Dcell[threadIdx.x] = D;
+#pragma unroll
+      for (int k = 0; k < INP; ++k)
+        s.X[threadIdx.x * INP + k] =
+            __float2bfloat16(k < IN ? (f[k] - s.stats[k]) * s.stats[IN + k] : 0.f);
+    }
+    __syncthreads();
+    forward(s);
+    __syncthreads();
+    if (threadIdx.x < ROWS && cellid[threadIdx.x] >= 0) {
+      const float y0 = s.Y[threadIdx.x * OUTP] * s.stats[2 * IN + 2] + s.stats[2 * IN];
+      const float y1 = s.Y[threadIdx.x * OUTP + 1] * s.stats[2 * IN + 3] + s.stats[2 * IN + 1];
+      double* zg = d.a[EA_ZG];
+      zg[cellid[threadIdx.x]] = Dcell[threadIdx.x] * exp10((double)y0);
+      zg[g.Ntot + cellid[threadIdx.x]] = fmin(fmax((double)y1, 0.0), 0.999999);
+    }
+  }
+}
+
 static_assert(NPARAM == MLP_NPARAM, "parameter layout");
 static_assert(NSTAT == MLP_NSTAT, "statistics layout");
 
@@ -369,6 +425,8 @@ cudaError_t configure() {
     e = cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_mlp_zguess, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_ens_mlp_zguess, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
   return e;
 }
 
@@ -389,6 +447,17 @@ cudaError_t launch_zguess(const Grid& g, long long n_cells, bool batch, const do
   k_mlp_zguess<<<blocks, 256, sizeof(Smem), s>>>(g, n_cells, batch ? 1 : 0, cons, P, st, zguess);
   return cudaGetLastError();
 }
+
+}  // namespace mlp
+
+cudaError_t ens_mlp_zguess(const Member* mem, const Item* items, int n_items, int ic,
+                           const float* params, const float* stats, int grid, cudaStream_t st) {
+  mlp::k_ens_mlp_zguess<<<grid, 256, sizeof(mlp::Smem), st>>>(mem, items, n_items, ic, params,
+                                                              stats);
+  return cudaGetLastError();
+}
+
+namespace mlp {
 
 cudaError_t launch_adam(float* P, float* m, float* v, const float* grad, float lr, float b1t,
                         float b2t, cudaStream_t st) {

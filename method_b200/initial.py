@@ -122,3 +122,26 @@ def random_c2p_states(n, seed=1234, gamma=4.0 / 3.0):
     p = np.zeros((8, n))
     p[0], p[1:4], p[4], p[5:8] = rho, v, prs, B
     return p
+
+
+def kh_ensemble(n=256, seed=2024, nx_lo=64, nx_hi=512, weno=3, precision="mixed"):
+    """Members of a Kelvin-Helmholtz parameter study: per member nx uniform
+    in [nx_lo, nx_hi], ny = 2 nx, shear speed uniform in [0.2, 0.8], and with
+    probability 1/2 a resistive (SRRMHD, IMEX SSP2) member with sigma
+    log-uniform in [1e2, 1e5], else ideal (SRMHD, RK2).  Returns a list of
+    (config dict for Simulation / Ensemble, kelvin_helmholtz keyword dict)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for m in range(n):
+        nx = int(rng.integers(nx_lo, nx_hi + 1))
+        shear = float(rng.uniform(0.2, 0.8))
+        resistive = bool(rng.random() < 0.5)
+        sigma = float(10.0 ** rng.uniform(2.0, 5.0)) if resistive else 0.0
+        cfg = dict(model="srrmhd" if resistive else "srmhd",
+                   integrator="ssp2" if resistive else "rk2", nx=nx, ny=2 * nx, xmin=-0.5,
+                   xmax=0.5, ymin=-1.0, ymax=1.0, endTime=3.0, cfl=0.4, Ng=4, gamma=4.0 / 3.0,
+                   sigma=sigma, weno=weno, bcs="flow", precision=precision)
+        ic = dict(nx=nx, ny=2 * nx, Ng=4, seed=int(seed) * 1000 + m,
+                  model=cfg["model"], shear=shear)
+        out.append((cfg, ic))
+    return out

@@ -146,3 +146,31 @@ def test_mixed_form_with_network_guess(trained):
     sl = (slice(None), slice(4, -4), slice(4, -4))
     l1 = np.abs(cn[sl] - cp[sl]).sum() / np.abs(cp[sl]).sum()
     assert l1 < 1e-6, l1
+
+
+def test_ensemble_with_network_guess(trained):
+    """Ensemble members with the network guess end bit-identical to single
+    simulations with the same guess, every cell converged."""
+    import method_b200 as mb
+    from method_b200 import initial
+    P, S, _ = trained
+    members = [dict(model="srmhd", nx=n, ny=n, xmin=0.0, xmax=1.0, ymin=0.0, ymax=1.0,
+                    endTime=1.0, cfl=0.4, Ng=4, gamma=4.0 / 3.0, weno=5, bcs="periodic",
+                    integrator="rk2", precision="mixed", guess="mlp") for n in (48, 100)]
+    ens = mb.Ensemble(members)
+    ens.set_mlp(P, S)
+    for m, c in enumerate(members):
+        ens.set_prims(m, initial.orszag_tang(c["nx"], Ng=4))
+    ens.step(10)
+    for m, c in enumerate(members):
+        s = mb.Simulation(**c)
+        s.set_mlp(P, S)
+        s.set_prims(initial.orszag_tang(c["nx"], Ng=4))
+        s.update_time(10)
+        want = s.state()
+        got = ens.state(m)
+        est = ens.stats(m)
+        assert est["c2p_unconverged"] == 0
+        assert est["c2p_evals"] == s.stats()["c2p_evals"]
+        for a, b in zip(got, want):
+            assert np.array_equal(a, b)
