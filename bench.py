@@ -7,16 +7,20 @@ sin 4pi x), gamma = 4/3, FVS + WENO5, RK2, CFL 0.4 (synthetic data built on
 the host, method_b200.initial.orszag_tang).  A step is one full RK2 step
 (two fused flux stages and two primitive recoveries) over the 1024^2 grid.
 
-Two forms run on the same initial data with the same dt sequence:
-  plain : all-FP64, bit-identical to the reference CPU build
-  mixed : FP32 flux/WENO, FP64 primitive recovery (Newton) and state
-The headline `value` is the mixed form; `plain` and the mixed form's L1
-error against the plain FP64 result are on the same line.
+Three forms run on the same initial data with the same dt sequence:
+  plain     : all-FP64, bit-identical to the reference CPU build
+  mixed     : FP32 flux/WENO, FP64 primitive recovery (Newton) and state
+  mixed_mlp : mixed, Newton started from the learned guess (trained on the
+              GPU at the start of the run, its loss and time reported)
+The headline `value` is the mixed form; the other forms and their L1 error
+against the plain FP64 result are on the same line, beside the ensemble
+workload (256 uneven Kelvin-Helmholtz simulations, `ensemble`).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
-Multi-GPU: one process per GPU under torchrun, each advancing an independent
-replica (the single-domain path has no exchange step), so scaling is weak;
+Multi-GPU: one process per GPU under torchrun.  The single-domain workload
+runs an independent replica per rank (its path has no exchange step); the
+ensemble's members are split over the ranks by cost.  Scaling is weak;
 timing is the max over ranks of device time.
 """
 from __future__ import annotations
@@ -115,8 +119,11 @@ def interior(a, Ng=4):
     return a[:, Ng:-Ng, Ng:-Ng, :]
 
 
-def run_form(mb, torch, prims0, n, form, steps, warmup, dt, device):
-    sim = mb.Simulation(nx=n, ny=n, precision=form, device=device, **CFG)
+def run_form(mb, torch, prims0, n, form, steps, warmup, dt, device, guess=None):
+    sim = mb.Simulation(nx=n, ny=n, precision=form, device=device,
+                        guess="mlp" if guess else "previous", **CFG)
+    if guess:
+        sim.set_mlp(guess[0], guess[1])
     sim.set_prims(prims0)
     stream = torch.cuda.Stream(device=device)
     sim.set_stream(stream.cuda_stream)
@@ -125,6 +132,141 @@ def run_form(mb, torch, prims0, n, form, steps, warmup, dt, device):
     sim.sync()
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     return sim, stream, start, end
+
+
+ENS_MEMBERS = 256
+ENS_WORKLOAD = ("256 independent 2D Kelvin-Helmholtz simulations (ideal SRMHD + RK2 and resistive "
+                "SRRMHD + IMEX SSP2, 1/2 each by seed), nx uniform in [64, 512], ny = 2 nx, shear "
+                "U(0.2, 0.8), sigma 10^U(2, 5), FVS+WENO3, CFL 0.4, flow boundaries; mixed form; "
+                "one persistent launch per phase, step graph-captured, autotuned tile heights")
+
+
+def run_ensemble(mb, initial, torch, ranks, K, W, guess):
+    """The ensemble workload, members split over ranks by cost (LPT)."""
+    from method_b200.ranks import lpt_partition
+    mem = initial.kh_ensemble(ENS_MEMBERS, seed=2024)
+    costs = [c["nx"] * c["ny"] * (2 if c["model"] == "srrmhd" else 1) for c, _ in mem]
+    mine = lpt_partition(costs, ranks.world)[ranks.rank]
+    cfgs = []
+    for i in mine:
+        c = dict(mem[i][0], device=ranks.local)
+        if guess:
+            c["guess"] = "mlp"
+        cfgs.append(c)
+    ens = mb.Ensemble(cfgs)
+    if guess:
+        ens.set_mlp(guess[0], guess[1])
+    for k, i in enumerate(mine):
+        ens.set_prims(k, initial.kelvin_helmholtz(**mem[i][1]))
+    ti = ens.autotune(reps=2)
+    stream = torch.cuda.Stream(device=ranks.local)
+    ens.set_stream(stream.cuda_stream)
+    ens.step(W, sync=False)
+    ens.sync()
+    cells = ens.info()["interior_cells"]
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ranks.barrier()
+    ev0.record(stream)
+    ens.step(K, sync=False)
+    ev1.record(stream)
+    ranks.barrier()
+    ens.sync()
+    ms = ranks.max(ev0.elapsed_time(ev1))
+    total = ranks.sum(cells)
+    st = [ens.stats(k) for k in range(len(mine))]
+    agg = {k: sum(x[k] for x in st) for k in ("c2p_cells", "c2p_evals", "c2p_unconverged",
+                                              "c2p_fallbacks", "implicit_cells", "implicit_evals",
+                                              "implicit_fallbacks", "implicit_failed")}
+    ens.close()
+    n_res = sum(1 for c, _ in mem if c["model"] == "srrmhd")
+    return {"value": total * K / (ms * 1e-3), "unit": "zone-updates/s", "ms_per_step": ms / K,
+            "steps": K, "warmup": W, "members": ENS_MEMBERS, "resistive_members": n_res,
+            "members_this_rank": len(mine), "interior_cells_total": int(total),
+            "tile_heights_by_class": ti, "guess": "mlp" if guess else "previous",
+            "c2p_newton_iters_per_cell": agg["c2p_evals"] / max(agg["c2p_cells"], 1),
+            "implicit_iters_per_cell": agg["implicit_evals"] / max(agg["implicit_cells"], 1),
+            **{k: agg[k] for k in ("c2p_unconverged", "c2p_fallbacks", "implicit_fallbacks",
+                                   "implicit_failed")},
+            "workload": ENS_WORKLOAD}
+
+
+C2P_CELLS = 256 ** 3
+C2P_WORKLOAD = ("SRMHD primitive recovery of 256^3 independent random states (W 10^U(0,1), rho "
+                "10^U(-3,0), p/rho 10^U(-3,1), b^2/rho 10^U(-2,2), isotropic v and B directions), "
+                "gamma 4/3; previous-step guess = generating rho and h 1% high, speed 1% low")
+
+
+def run_c2p_batch(mb, torch, ranks, guess, reps=3):
+    """Batched primitive recovery: the reference method (Powell hybrid) and
+    Newton from the previous-step, cold and learned guesses, each timed with
+    CUDA events on its stream, iterations and error against the generating
+    state reported."""
+    import ctypes as C
+    from method_b200 import _lib
+    L = _lib.load()
+    n = C2P_CELLS
+    gamma = 4.0 / 3.0
+    dev = torch.device("cuda", ranks.local)
+    F, D = C.POINTER(C.c_float), C.POINTER(C.c_double)
+    feat = torch.empty((n, 8), dtype=torch.float32, device=dev)
+    tgt = torch.empty((n, 2), dtype=torch.float32, device=dev)
+    cons = torch.empty((9, n), dtype=torch.float64, device=dev)
+    truth = torch.empty((8, n), dtype=torch.float64, device=dev)
+    rc = L.mth_mlp_make_pairs(n, 4242 + ranks.rank, gamma, C.cast(feat.data_ptr(), F),
+                              C.cast(tgt.data_ptr(), F), C.cast(cons.data_ptr(), D),
+                              C.cast(truth.data_ptr(), D), ranks.local)
+    if rc != 0:
+        raise RuntimeError(f"mth_mlp_make_pairs: {rc}")
+    del feat, tgt
+    pg0 = truth.clone()
+    pg0[0] *= 1.01
+    pg0[1:4] *= 0.99
+    ag0 = torch.zeros((13, n), dtype=torch.float64, device=dev)
+    ag0[0] = (1.0 + truth[4] / truth[0] * (gamma / (gamma - 1.0))) * 1.01
+    ctx = C.c_void_p()
+    if L.mth_c2p_ctx_create(n, ranks.local, C.byref(ctx)) != 0:
+        raise RuntimeError("mth_c2p_ctx_create failed")
+    if guess:
+        L.mth_c2p_ctx_set_mlp(ctx, guess[0].ctypes.data_as(F), guess[1].ctypes.data_as(F))
+    stream = torch.cuda.Stream(device=dev)
+    prims = torch.empty_like(pg0)
+    aux = torch.empty_like(ag0)
+    out = {}
+    methods = [("hybrd_previous", 0, 0), ("newton_previous", 1, 0), ("newton_cold", 1, 2)]
+    if guess:
+        methods.append(("newton_mlp", 1, 1))
+    for name, method, g in methods:
+        ms = 0.0
+        with torch.cuda.stream(stream):
+            for rep in range(reps + 1):
+                prims.copy_(pg0)
+                aux.copy_(ag0)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                r = L.mth_c2p_ctx_run(ctx, gamma, n, cons.data_ptr(), prims.data_ptr(),
+                                      aux.data_ptr(), method, g, stream.cuda_stream)
+                e1.record(stream)
+                if r != 0:
+                    raise RuntimeError(f"mth_c2p_ctx_run {name}: {r}")
+                st = _lib.C2PBatchStats()
+                L.mth_c2p_ctx_stats(ctx, stream.cuda_stream, C.byref(st))
+                if rep > 0:
+                    ms += e0.elapsed_time(e1)
+            rel = ((prims[0] - truth[0]).abs() / truth[0])
+            torch.cuda.synchronize(dev)
+        ms = ranks.max(ms / reps)
+        out[name] = {"cells_per_s": ranks.world * n / (ms * 1e-3), "ms": round(ms, 3),
+                     "iters_per_cell": st.iterations / max(st.cells, 1),
+                     "unconverged": int(st.unconverged), "fallbacks": int(st.fallbacks),
+                     "median_rel_err_rho": float(rel.nan_to_num(1.0).median()),
+                     "max_rel_err_rho": float(rel.nan_to_num(1.0).max())}
+    L.mth_c2p_ctx_destroy(ctx)
+    res = {"workload": C2P_WORKLOAD, "cells": n, "unit": "cells/s", "methods": out,
+           "iterations": "hybrd: residual evaluations; newton: Newton steps (incl. fallbacks)"}
+    if "newton_mlp" in out:
+        res["mlp_iters_saved_vs_cold"] = (out["newton_cold"]["iters_per_cell"]
+                                          - out["newton_mlp"]["iters_per_cell"])
+    return res
 
 
 def roofline_of(sim, dt, peak, reps=3):
@@ -223,8 +365,10 @@ def main():
     ap.add_argument("--n", type=int, default=N_DEFAULT)
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--forms", default="plain,mixed",
+    ap.add_argument("--forms", default="plain,mixed,mixed_mlp",
                     help="forms to run (profiling runs one at a time)")
+    ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--no-c2p-batch", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
@@ -232,28 +376,11 @@ def main():
     import torch
     import method_b200 as mb
     from method_b200 import initial
+    from method_b200.ranks import Ranks
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-
-    def barrier():
-        if dist:
-            dist.barrier()
-        torch.cuda.synchronize()
-
-    def max_over_ranks(x):
-        if not dist:
-            return x
-        t = torch.tensor([x], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    ranks = Ranks("nccl", timeout_s=120)
+    world, rank, local = ranks.world, ranks.rank, ranks.local
+    barrier, max_over_ranks = ranks.barrier, ranks.max
 
     n = args.n
     dt = steady_dt(n)
@@ -262,11 +389,21 @@ def main():
     K, W = args.steps, args.warmup
     results = {}
     clocks = Clocks(local)
-    forms = [f for f in ("plain", "mixed") if f in args.forms.split(",")]
+    forms = [f for f in ("plain", "mixed", "mixed_mlp") if f in args.forms.split(",")]
+    guess = None
+    train = None
+    if "mixed_mlp" in forms or not args.no_ensemble or not args.no_c2p_batch:
+        t0 = time.perf_counter()
+        P, S, loss = mb.train_guess(device=local)
+        train = {"loss": loss, "seconds": round(time.perf_counter() - t0, 2),
+                 "samples": 1 << 19, "iterations": 4000, "batch": 8192}
+        guess = (P, S)
+    ensemble = None
     with clocks:
         for form in forms:
             prec = "fp64" if form == "plain" else "mixed"
-            sim, stream, ev0, ev1 = run_form(mb, torch, prims0, n, prec, K, W, dt, local)
+            sim, stream, ev0, ev1 = run_form(mb, torch, prims0, n, prec, K, W, dt, local,
+                                             guess if form == "mixed_mlp" else None)
             sim.reset_stats()
             barrier()
             ev0.record(stream)
@@ -280,6 +417,17 @@ def main():
             st = sim.stats()
             c, p, a = sim.state()
             results[form] = dict(sim=sim, ms=ms, stats=st, cons=interior(c), prims=interior(p))
+        if not args.no_ensemble:
+            ke, we = max(1, min(K, 20)), max(W, 3)
+            ensemble = run_ensemble(mb, initial, torch, ranks, ke, we, None)
+            if guess:
+                e_mlp = run_ensemble(mb, initial, torch, ranks, ke, we, guess)
+                ensemble["with_learned_guess"] = {
+                    k: e_mlp[k] for k in ("value", "ms_per_step", "c2p_newton_iters_per_cell",
+                                          "c2p_unconverged", "c2p_fallbacks")}
+        c2p_batch = None
+        if not args.no_c2p_batch:
+            c2p_batch = run_c2p_batch(mb, torch, ranks, guess)
     clk = clocks.summary()
 
     cells = n * n
@@ -302,19 +450,22 @@ def main():
             "kernels": [{"name": k["name"], "launches_per_step": k["launches"] / 3.0,
                          "ms_per_launch": round(k["total_ms"] / k["launches"], 4)} for k in ks],
         }
-    if forms != ["plain", "mixed"]:
+    if not {"plain", "mixed"} <= set(forms):
         if rank == 0:
             print(json.dumps({f: results[f]["summary"] for f in forms}), flush=True)
         for r in results.values():
             r["sim"].close()
+        ranks.close()
         return
     # L1 of the mixed form against the FP64 result (bit-identical to the reference)
     l1 = {}
-    for name in ("cons", "prims"):
-        ref_, mix = results["plain"][name], results["mixed"][name]
-        d = np.abs(mix - ref_)
-        l1[name] = {"l1_abs": float(d.mean()), "l1_rel": float(d.sum() / np.abs(ref_).sum()),
-                    "max_abs": float(d.max())}
+    for form in [f for f in forms if f != "plain"]:
+        for name in ("cons", "prims"):
+            ref_, mix = results["plain"][name], results[form][name]
+            d = np.abs(mix - ref_)
+            key = name if form == "mixed" else f"{form}_{name}"
+            l1[key] = {"l1_abs": float(d.mean()), "l1_rel": float(d.sum() / np.abs(ref_).sum()),
+                       "max_abs": float(d.max())}
 
     # end to end through the reference-facing call on host arrays (mixed form)
     e2e = None
@@ -358,7 +509,11 @@ def main():
             "roofline": results["mixed"]["roof"],
             "plain": {**results["plain"]["summary"], "dtype": "f64"},
             "mixed": results["mixed"]["summary"],
+            "mixed_mlp": results["mixed_mlp"]["summary"] if "mixed_mlp" in results else None,
+            "guess_training": train,
             "l1_mixed_vs_fp64": l1,
+            "ensemble": ensemble,
+            "c2p_batch": c2p_batch,
             "speedup_mixed_vs_plain": results["plain"]["ms"] / results["mixed"]["ms"],
             "cpu_baseline": cpu,
             "e2e": e2e,
@@ -368,9 +523,7 @@ def main():
         print(json.dumps(line), flush=True)
     for r in results.values():
         r["sim"].close()
-    if dist:
-        dist.barrier()
-        dist.destroy_process_group()
+    ranks.close()
 
 
 if __name__ == "__main__":

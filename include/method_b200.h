@@ -180,7 +180,8 @@ mth_status mth_mlp_grad(const float* params, int n, const float* x, const float*
 mth_status mth_mlp_forward(const float* params, int n, const float* x, float* y, int device);
 /* Solver-generated training pairs: features [n][8], targets [n][2] (raw,
  * not standardised), optionally the conserved [9][n] and generating
- * primitive [8][n] states. */
+ * primitive [8][n] states.  Output pointers may be host or device memory
+ * (copies use unified addressing). */
 mth_status mth_mlp_make_pairs(long long n, unsigned long long seed, double gamma, float* feat,
                               float* tgt, double* cons, double* prims, int device);
 /* Installs a trained network in a handle (precision MTH_MIXED, guess MTH_GUESS_MLP). */
@@ -200,6 +201,23 @@ typedef struct {
 mth_status mth_c2p_batch(double gamma, long long n, const double* cons, double* prims,
                          double* aux, int method, int guess, const float* mlp_params,
                          const float* mlp_stats, void* stream, mth_c2p_batch_stats* stats);
+
+/* Reusable workspace for batched primitive recovery: the same solve as
+ * mth_c2p_batch without per-call allocation or synchronisation.  Create it
+ * for up to max_n cells on a device (allocates the guess planes and
+ * counters), install a trained network once if MTH_GUESS_MLP is used, then
+ * enqueue runs on any stream of that device; each run resets the counters,
+ * which mth_c2p_ctx_stats reads back (synchronising the stream; returns
+ * MTH_ERR_C2P if cells stayed unconverged).  Runs that overlap on the GPU
+ * share the workspace and race: order them on one stream.  No counterpart in
+ * the reference (see mth_c2p_batch). */
+typedef struct mth_c2p_ctx mth_c2p_ctx;
+mth_status mth_c2p_ctx_create(long long max_n, int device, mth_c2p_ctx** out);
+mth_status mth_c2p_ctx_destroy(mth_c2p_ctx* c);
+mth_status mth_c2p_ctx_set_mlp(mth_c2p_ctx* c, const float* params, const float* stats);
+mth_status mth_c2p_ctx_run(mth_c2p_ctx* c, double gamma, long long n, const double* cons,
+                           double* prims, double* aux, int method, int guess, void* stream);
+mth_status mth_c2p_ctx_stats(mth_c2p_ctx* c, void* stream, mth_c2p_batch_stats* stats);
 
 /* Largest number of interior cells mth_c2p_srmhd_noalloc accepts per call. */
 #define MTH_NOALLOC_MAX_CELLS (1 << 20)
@@ -269,6 +287,12 @@ mth_status mth_ensemble_set_stream(mth_ensemble* e, void* stream);
 mth_status mth_ensemble_autotune(mth_ensemble* e, int reps, int* ti3);
 /* Enqueues n_steps ensemble steps (asynchronous; see mth_ensemble_sync). */
 mth_status mth_ensemble_step(mth_ensemble* e, int n_steps);
+/* Per-phase timing of `reps` ensemble steps run eagerly (one phase at a time,
+ * CUDA events around each) into up to max_out records (bytes_per_launch 0);
+ * *n_out receives the number of distinct phases.  The steps advance the
+ * members like mth_ensemble_step. */
+mth_status mth_ensemble_profile(mth_ensemble* e, int reps, mth_kernel_time* out, int max_out,
+                                int* n_out);
 /* Waits for the enqueued steps; returns MTH_ERR_C2P / MTH_ERR_IMPLICIT if any
  * member's solve failed (the reference's exceptions). */
 mth_status mth_ensemble_sync(mth_ensemble* e);

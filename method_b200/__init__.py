@@ -25,7 +25,7 @@ INTEGRATORS = {"rk2": 0, "rksplit": 1, "ssp2": 2}
 PRECISIONS = {"fp64": 0, "mixed": 1}
 GUESSES = {"previous": 0, "mlp": 1}
 
-__all__ = ["Simulation", "Ensemble", "MODELS", "BCS", "INTEGRATORS", "pin_host", "unpin_host"]
+__all__ = ["Simulation", "Ensemble", "train_guess", "MODELS", "BCS", "INTEGRATORS", "pin_host", "unpin_host"]
 
 
 def pin_host(arr):
@@ -234,6 +234,25 @@ class Simulation:
         return self.stats()["t"]
 
 
+def train_guess(seed=7, n_samples=1 << 19, iterations=4000, batch=8192, lr=3e-3,
+                gamma=4.0 / 3.0, device=0):
+    """Trains the C2P guess network on the GPU on (conserved -> primitive)
+    pairs the solver generates (mth_mlp_train).  Returns (params, stats,
+    final loss) for Simulation.set_mlp / Ensemble.set_mlp."""
+    L = _lib.load()
+    cfg = _lib.MlpTrainConfig(seed=seed, n_samples=n_samples, iterations=iterations, batch=batch,
+                              lr=lr, gamma=gamma)
+    P = np.zeros(_lib.MLP_NPARAM, dtype=np.float32)
+    S = np.zeros(_lib.MLP_NSTAT, dtype=np.float32)
+    loss = np.zeros(1, dtype=np.float32)
+    F = C.POINTER(C.c_float)
+    rc = L.mth_mlp_train(C.byref(cfg), P.ctypes.data_as(F), S.ctypes.data_as(F),
+                         loss.ctypes.data_as(F), device)
+    if rc != 0:
+        raise RuntimeError(f"mth_mlp_train failed: {_lib.STATUS.get(rc, rc)}")
+    return P, S, float(loss[0])
+
+
 class Ensemble:
     """Independent 2D simulations of uneven sizes advanced together on one GPU.
 
@@ -317,6 +336,15 @@ class Ensemble:
 
     def sync(self):
         self._check(self.L.mth_ensemble_sync(self.e), "step")
+
+    def profile(self, reps=2):
+        """Per-phase timing of `reps` eager steps (they advance the members)."""
+        out = (_lib.KernelTime * 64)()
+        n = C.c_int()
+        self._check(self.L.mth_ensemble_profile(self.e, int(reps), out, 64, C.byref(n)),
+                    "profile")
+        return [dict(name=out[i].name.decode(), launches=out[i].launches,
+                     total_ms=out[i].total_ms) for i in range(min(n.value, 64))]
 
     def set_mlp(self, params, stats):
         """Installs a trained C2P guess network (members created with guess='mlp')."""

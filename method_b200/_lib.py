@@ -22,11 +22,12 @@ SYMBOLS = [
     "mth_flux_F", "mth_source", "mth_flux_vector", "mth_c2p_cells", "mth_step", "mth_update_time", "mth_evolve", "mth_sync",
     "mth_get_stats", "mth_reset_stats", "mth_step_host", "mth_pin_host", "mth_unpin_host",
     "mth_set_stream", "mth_profile_step", "mth_mlp_train", "mth_mlp_grad", "mth_mlp_forward",
-    "mth_mlp_make_pairs", "mth_set_mlp", "mth_c2p_batch", "mth_c2p_srmhd_noalloc",
+    "mth_mlp_make_pairs", "mth_set_mlp", "mth_c2p_batch", "mth_c2p_ctx_create", "mth_c2p_ctx_destroy",
+    "mth_c2p_ctx_set_mlp", "mth_c2p_ctx_run", "mth_c2p_ctx_stats", "mth_c2p_srmhd_noalloc",
     "mth_device_state", "mth_ensemble_create", "mth_ensemble_destroy",
     "mth_ensemble_last_error", "mth_ensemble_set_prims", "mth_ensemble_download",
     "mth_ensemble_set_mlp", "mth_ensemble_set_stream", "mth_ensemble_autotune", "mth_ensemble_step",
-    "mth_ensemble_sync", "mth_ensemble_stats", "mth_ensemble_info",
+    "mth_ensemble_profile", "mth_ensemble_sync", "mth_ensemble_stats", "mth_ensemble_info",
 ]
 
 MLP_NPARAM = 9928
@@ -118,6 +119,12 @@ def load():
     L.mth_set_mlp.argtypes = [H, F, F]
     L.mth_c2p_batch.argtypes = [C.c_double, C.c_longlong, C.c_void_p, C.c_void_p, C.c_void_p,
                                 C.c_int, C.c_int, F, F, C.c_void_p, C.POINTER(C2PBatchStats)]
+    L.mth_c2p_ctx_create.argtypes = [C.c_longlong, C.c_int, C.POINTER(C.c_void_p)]
+    L.mth_c2p_ctx_destroy.argtypes = [C.c_void_p]
+    L.mth_c2p_ctx_set_mlp.argtypes = [C.c_void_p, F, F]
+    L.mth_c2p_ctx_run.argtypes = [C.c_void_p, C.c_double, C.c_longlong, C.c_void_p, C.c_void_p,
+                                  C.c_void_p, C.c_int, C.c_int, C.c_void_p]
+    L.mth_c2p_ctx_stats.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C2PBatchStats)]
     L.mth_c2p_srmhd_noalloc.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
                                          C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                          C.c_void_p, C.c_void_p, C.c_void_p]
@@ -131,6 +138,8 @@ def load():
     L.mth_ensemble_set_stream.argtypes = [E, C.c_void_p]
     L.mth_ensemble_autotune.argtypes = [E, C.c_int, C.POINTER(C.c_int)]
     L.mth_ensemble_step.argtypes = [E, C.c_int]
+    L.mth_ensemble_profile.argtypes = [E, C.c_int, C.POINTER(KernelTime), C.c_int,
+                                       C.POINTER(C.c_int)]
     L.mth_ensemble_sync.argtypes = [E]
     L.mth_ensemble_stats.argtypes = [E, C.c_int, C.POINTER(Stats)]
     L.mth_ensemble_info.argtypes = [E, C.POINTER(C.c_longlong), C.POINTER(C.c_int)]

@@ -723,52 +723,111 @@ mth_status mth_set_mlp(mth_handle* h, const float* params, const float* stats) {
   return MTH_OK;
 }
 
+}  // extern "C"
+
+struct mth_c2p_ctx {
+  int device = 0;
+  long long max_n = 0;
+  float* P = nullptr;       // network parameters (device)
+  float* S = nullptr;       // network statistics (device)
+  double* zg = nullptr;     // guess planes, 2 x max_n
+  long long* cnt = nullptr; // cells, iterations, unconverged, fallbacks
+  bool has_mlp = false;
+};
+
+extern "C" {
+
+mth_status mth_c2p_ctx_create(long long max_n, int device, mth_c2p_ctx** out) {
+  if (max_n <= 0 || !out) return MTH_ERR_INVALID;
+  *out = nullptr;
+  if (cudaSetDevice(device) != cudaSuccess) return MTH_ERR_CUDA;
+  mth_c2p_ctx* c = new mth_c2p_ctx();
+  c->device = device;
+  c->max_n = max_n;
+  if (mlp::configure() != cudaSuccess || cudaMalloc(&c->P, sizeof(float) * MLP_NPARAM) ||
+      cudaMalloc(&c->S, sizeof(float) * MLP_NSTAT) ||
+      cudaMalloc(&c->zg, sizeof(double) * 2 * max_n) ||
+      cudaMalloc(&c->cnt, sizeof(long long) * 4) ||
+      cudaMemset(c->cnt, 0, sizeof(long long) * 4)) {
+    mth_c2p_ctx_destroy(c);
+    return MTH_ERR_CUDA;
+  }
+  *out = c;
+  return MTH_OK;
+}
+
+mth_status mth_c2p_ctx_destroy(mth_c2p_ctx* c) {
+  if (!c) return MTH_OK;
+  cudaSetDevice(c->device);
+  cudaDeviceSynchronize();
+  cudaFree(c->P);
+  cudaFree(c->S);
+  cudaFree(c->zg);
+  cudaFree(c->cnt);
+  delete c;
+  return MTH_OK;
+}
+
+mth_status mth_c2p_ctx_set_mlp(mth_c2p_ctx* c, const float* params, const float* stats) {
+  if (!c || !params || !stats) return MTH_ERR_INVALID;
+  if (cudaSetDevice(c->device) ||
+      cudaMemcpy(c->P, params, sizeof(float) * MLP_NPARAM, cudaMemcpyHostToDevice) ||
+      cudaMemcpy(c->S, stats, sizeof(float) * MLP_NSTAT, cudaMemcpyHostToDevice))
+    return MTH_ERR_CUDA;
+  c->has_mlp = true;
+  return MTH_OK;
+}
+
+mth_status mth_c2p_ctx_run(mth_c2p_ctx* c, double gamma, long long n, const double* cons,
+                           double* prims, double* aux, int method, int guess, void* stream) {
+  if (!c || n <= 0 || n > c->max_n || !cons || !prims || !aux || method < 0 || method > 1 ||
+      guess < 0 || guess > 2 || (guess == MTH_GUESS_MLP && !c->has_mlp))
+    return MTH_ERR_INVALID;
+  if (cudaSetDevice(c->device) != cudaSuccess) return MTH_ERR_CUDA;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (cudaMemsetAsync(c->cnt, 0, sizeof(long long) * 4, st) != cudaSuccess) return MTH_ERR_CUDA;
+  if (guess == MTH_GUESS_MLP) {
+    Grid g{};
+    g.Ntot = n;
+    if (mlp::launch_zguess(g, n, true, cons, c->P, c->S, c->zg, st) != cudaSuccess)
+      return MTH_ERR_CUDA;
+  }
+  if (launch_c2p_batch(n, gamma, method, guess, cons, prims, aux,
+                       guess == MTH_GUESS_MLP ? c->zg : nullptr, c->cnt, st) != cudaSuccess)
+    return MTH_ERR_CUDA;
+  return MTH_OK;
+}
+
+mth_status mth_c2p_ctx_stats(mth_c2p_ctx* c, void* stream, mth_c2p_batch_stats* stats) {
+  if (!c || !stats) return MTH_ERR_INVALID;
+  if (cudaSetDevice(c->device) != cudaSuccess) return MTH_ERR_CUDA;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  long long h[4] = {0, 0, 0, 0};
+  if (cudaMemcpyAsync(h, c->cnt, sizeof h, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return MTH_ERR_CUDA;
+  stats->cells = h[0];
+  stats->iterations = h[1];
+  stats->unconverged = h[2];
+  stats->fallbacks = h[3];
+  return h[2] > 0 ? MTH_ERR_C2P : MTH_OK;
+}
+
 mth_status mth_c2p_batch(double gamma, long long n, const double* cons, double* prims,
                          double* aux, int method, int guess, const float* mlp_params,
                          const float* mlp_stats, void* stream, mth_c2p_batch_stats* stats) {
   if (n <= 0 || !cons || !prims || !aux || method < 0 || method > 1 || guess < 0 || guess > 2 ||
       (guess == MTH_GUESS_MLP && (!mlp_params || !mlp_stats)))
     return MTH_ERR_INVALID;
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
-  float *P = nullptr, *S = nullptr;
-  double* zg = nullptr;
-  long long* cnt = nullptr;
-  mth_status rc = MTH_OK;
-  auto bad = [&](cudaError_t e) { return e != cudaSuccess; };
-  if (bad(cudaMalloc(&cnt, sizeof(long long) * 4)) ||
-      bad(cudaMemsetAsync(cnt, 0, sizeof(long long) * 4, st))) {
-    rc = MTH_ERR_CUDA;
-  } else if (guess == MTH_GUESS_MLP) {
-    Grid g{};
-    g.Ntot = n;
-    if (bad(mlp::configure()) || bad(cudaMalloc(&P, sizeof(float) * MLP_NPARAM)) ||
-        bad(cudaMalloc(&S, sizeof(float) * MLP_NSTAT)) ||
-        bad(cudaMalloc(&zg, sizeof(double) * 2 * n)) ||
-        bad(cudaMemcpyAsync(P, mlp_params, sizeof(float) * MLP_NPARAM, cudaMemcpyHostToDevice,
-                            st)) ||
-        bad(cudaMemcpyAsync(S, mlp_stats, sizeof(float) * MLP_NSTAT, cudaMemcpyHostToDevice,
-                            st)) ||
-        bad(mlp::launch_zguess(g, n, true, cons, P, S, zg, st)))
-      rc = MTH_ERR_CUDA;
-  }
-  if (rc == MTH_OK &&
-      bad(launch_c2p_batch(n, gamma, method, guess, cons, prims, aux, zg, cnt, st)))
-    rc = MTH_ERR_CUDA;
-  long long h[4] = {0, 0, 0, 0};
-  if (rc == MTH_OK && (bad(cudaMemcpyAsync(h, cnt, sizeof h, cudaMemcpyDeviceToHost, st)) ||
-                       bad(cudaStreamSynchronize(st))))
-    rc = MTH_ERR_CUDA;
-  if (stats) {
-    stats->cells = h[0];
-    stats->iterations = h[1];
-    stats->unconverged = h[2];
-    stats->fallbacks = h[3];
-  }
-  cudaFree(P);
-  cudaFree(S);
-  cudaFree(zg);
-  cudaFree(cnt);
-  if (rc == MTH_OK && h[2] > 0) rc = MTH_ERR_C2P;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return MTH_ERR_CUDA;
+  mth_c2p_ctx* c = nullptr;
+  mth_status rc = mth_c2p_ctx_create(n, dev, &c);
+  if (rc == MTH_OK && guess == MTH_GUESS_MLP) rc = mth_c2p_ctx_set_mlp(c, mlp_params, mlp_stats);
+  if (rc == MTH_OK) rc = mth_c2p_ctx_run(c, gamma, n, cons, prims, aux, method, guess, stream);
+  mth_c2p_batch_stats local{};
+  if (rc == MTH_OK) rc = mth_c2p_ctx_stats(c, stream, stats ? stats : &local);
+  mth_c2p_ctx_destroy(c);
   return rc;
 }
 

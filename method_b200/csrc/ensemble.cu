@@ -31,6 +31,17 @@ int size_class(int nx) { return nx <= 96 ? 0 : (nx <= 192 ? 1 : 2); }
 
 }  // namespace
 
+// Per-phase event timing for mth_ensemble_profile (null when not profiling).
+struct PhaseTimer {
+  struct Rec {
+    std::string name;
+    int launches = 0;
+    double ms = 0;
+  };
+  std::vector<Rec> recs;
+  cudaEvent_t a = nullptr, b = nullptr;
+};
+
 struct mth_ensemble {
   int n = 0;
   int precision = MTH_MIXED;
@@ -54,6 +65,9 @@ struct mth_ensemble {
   float* mlp_stats = nullptr;      // device, MLP_NSTAT
   bool has_mlp = false;
   cudaStream_t own = nullptr, st = nullptr;
+  cudaStream_t side = nullptr;  // second branch of the captured step
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  PhaseTimer* timer = nullptr;
   cudaGraphExec_t graph = nullptr;
   std::string err;
 };
@@ -122,74 +136,138 @@ cudaError_t build_flux_items(mth_ensemble* e) {
 
 int flux_grid(const mth_ensemble* e, int n_items) {
   (void)e;
-  return std::max(1, std::min(n_items, 148 * 4));
+  return std::max(1, n_items);  // the launcher caps it at the resident capacity
+}
+
+template <class F>
+cudaError_t phase(mth_ensemble* e, cudaStream_t s, const char* name, F&& f) {
+  PhaseTimer* pt = e->timer;
+  if (!pt) return f();
+  cudaError_t r = cudaEventRecord(pt->a, s);
+  if (r == cudaSuccess) r = f();
+  if (r == cudaSuccess) r = cudaEventRecord(pt->b, s);
+  if (r == cudaSuccess) r = cudaEventSynchronize(pt->b);
+  float ms = 0.f;
+  if (r == cudaSuccess) r = cudaEventElapsedTime(&ms, pt->a, pt->b);
+  if (r != cudaSuccess) return r;
+  for (auto& x : pt->recs)
+    if (x.name == name) {
+      x.launches++;
+      x.ms += ms;
+      return cudaSuccess;
+    }
+  pt->recs.push_back({name, 1, ms});
+  return cudaSuccess;
 }
 
 // One flux phase of every member of a model (all size classes).
-cudaError_t flux_phase(mth_ensemble* e, int md, int ic, int ip, int ia, int iu0, int iout,
-                       int mode) {
+cudaError_t flux_phase(mth_ensemble* e, cudaStream_t s, int md, int ic, int ip, int ia, int iu0,
+                       int iout, int mode) {
   for (int c = 0; c < kClasses; ++c) {
     const int n = e->n_flux[md][c];
     if (!n) continue;
-    cudaError_t r = (e->precision == MTH_MIXED)
-                        ? ens_fvs_fp32(e->d_mem, e->d_flux[md][c], n, md, e->order, e->ti[c], ic,
-                                       ip, ia, iu0, iout, mode, flux_grid(e, n), e->st)
-                        : ens_fvs_fp64(e->d_mem, e->d_flux[md][c], n, md, e->order, e->ti[c], ic,
-                                       ip, ia, iu0, iout, mode, flux_grid(e, n), e->st);
+    static const char* names[2][2][kClasses] = {
+        {{"fvs_fp64_srmhd_c0", "fvs_fp64_srmhd_c1", "fvs_fp64_srmhd_c2"},
+         {"fvs_fp64_srrmhd_c0", "fvs_fp64_srrmhd_c1", "fvs_fp64_srrmhd_c2"}},
+        {{"fvs_fp32_srmhd_c0", "fvs_fp32_srmhd_c1", "fvs_fp32_srmhd_c2"},
+         {"fvs_fp32_srrmhd_c0", "fvs_fp32_srrmhd_c1", "fvs_fp32_srrmhd_c2"}}};
+    const bool mixed = e->precision == MTH_MIXED;
+    cudaError_t r = phase(e, s, names[mixed][md][c], [&] {
+      return mixed ? ens_fvs_fp32(e->d_mem, e->d_flux[md][c], n, md, e->order, e->ti[c], ic, ip,
+                                  ia, iu0, iout, mode, flux_grid(e, n), s)
+                   : ens_fvs_fp64(e->d_mem, e->d_flux[md][c], n, md, e->order, e->ti[c], ic, ip,
+                                  ia, iu0, iout, mode, flux_grid(e, n), s);
+    });
     if (r != cudaSuccess) return r;
   }
   return cudaSuccess;
 }
 
-cudaError_t c2p_phase(mth_ensemble* e, int md, int ic, int ipg, int iag, int ip, int ia) {
+cudaError_t c2p_phase(mth_ensemble* e, cudaStream_t s, int md, int ic, int ipg, int iag, int ip,
+                      int ia) {
   const int n = e->n_cells[md];
   if (!n) return cudaSuccess;
   const int grid = std::max(1, std::min(n, e->grid_cells));
   if (e->precision == MTH_MIXED) {
     const int gm = (md == MODEL_SRMHD && e->guess == MTH_GUESS_MLP && e->has_mlp) ? 1 : 0;
     if (gm) {
-      cudaError_t r = ens_mlp_zguess(e->d_mem, e->d_cells[md], n, ic, e->mlp_params,
-                                     e->mlp_stats, e->grid_mlp, e->st);
+      cudaError_t r = phase(e, s, "mlp_zguess", [&] {
+        return ens_mlp_zguess(e->d_mem, e->d_cells[md], n, ic, e->mlp_params, e->mlp_stats,
+                              e->grid_mlp, s);
+      });
       if (r != cudaSuccess) return r;
     }
-    return ens_c2p_newton(e->d_mem, e->d_cells[md], n, md, gm, ic, ipg, iag, ip, ia, grid, e->st);
+    return phase(e, s, md == MODEL_SRMHD ? "c2p_newton_srmhd" : "c2p_newton_srrmhd", [&] {
+      return ens_c2p_newton(e->d_mem, e->d_cells[md], n, md, gm, ic, ipg, iag, ip, ia, grid, s);
+    });
   }
-  cudaError_t r = ens_c2p_srmhd_hybrd(e->d_mem, e->d_cells[md], n, ic, ipg, iag, ip, ia, grid,
-                                      e->st);
+  cudaError_t r = phase(e, s, "c2p_hybrd_srmhd", [&] {
+    return ens_c2p_srmhd_hybrd(e->d_mem, e->d_cells[md], n, ic, ipg, iag, ip, ia, grid, s);
+  });
   if (r != cudaSuccess) return r;
-  return ens_c2p_retry(e->d_mem, e->n, ic, ip, ia, e->st);
+  return phase(e, s, "c2p_retry", [&] { return ens_c2p_retry(e->d_mem, e->n, ic, ip, ia, s); });
 }
 
-// One time step of every member (updateTime semantics per member).
-cudaError_t enqueue_ens_step(mth_ensemble* e) {
-  cudaError_t r = ens_dt(e->d_mem, e->n, e->st);
+// RK2 (RK2.cc:93-100) of every SRMHD member.
+cudaError_t srmhd_rk2(mth_ensemble* e, cudaStream_t s) {
+  const int md = MODEL_SRMHD;
+  cudaError_t r;
+  if ((r = flux_phase(e, s, md, EA_CONS, EA_PRIMS, EA_AUX, -1, EA_P1C, STAGE_EULER))) return r;
+  if ((r = c2p_phase(e, s, md, EA_P1C, EA_PRIMS, EA_AUX, EA_P1P, EA_P1A))) return r;
+  if ((r = flux_phase(e, s, md, EA_P1C, EA_P1P, EA_P1A, EA_CONS, EA_CONS, STAGE_RK2_CORR)))
+    return r;
+  return c2p_phase(e, s, md, EA_CONS, EA_PRIMS, EA_AUX, EA_PRIMS, EA_AUX);
+}
+
+// SSP2 (SSP2.cc:53-173), mixed form, of every SRRMHD member.
+cudaError_t srrmhd_ssp2(mth_ensemble* e, cudaStream_t s) {
+  const int md = MODEL_SRRMHD;
+  const int n = e->n_cells[md];
+  const int grid = std::max(1, std::min(n, e->grid_cells));
+  Item* it = e->d_cells[md];
+  cudaError_t r;
+  for (int stage = 1; stage <= 2; ++stage) {
+    const int u = stage == 1 ? EA_U1 : EA_U2, src = stage == 1 ? EA_S1 : EA_S2,
+              fl = stage == 1 ? EA_F1 : EA_F2;
+    if ((r = phase(e, s, "imex_newton", [&] {
+           return ens_imex_fast(e->d_mem, it, n, stage, grid, s);
+         })))
+      return r;
+    if ((r = phase(e, s, "imex_queued", [&] { return ens_imex_queued(e->d_mem, e->n, stage, s); })))
+      return r;
+    if ((r = c2p_phase(e, s, md, u, EA_PRIMS, EA_AUX, EA_PRIMS, EA_AUX))) return r;
+    if ((r = phase(e, s, "source", [&] {
+           return ens_source(e->d_mem, it, n, u, EA_AUX, src, grid, s);
+         })))
+      return r;
+    if ((r = flux_phase(e, s, md, u, EA_PRIMS, EA_AUX, -1, fl, STAGE_FNET))) return r;
+  }
+  if ((r = phase(e, s, "ssp2_combine", [&] { return ens_combine(e->d_mem, it, n, grid, s); })))
+    return r;
+  return c2p_phase(e, s, md, EA_CONS, EA_PRIMS, EA_AUX, EA_PRIMS, EA_AUX);
+}
+
+// One time step of every member (updateTime semantics per member).  The two
+// models' members are independent, so while capturing (fork = true) the
+// SRRMHD branch runs on a second stream beside the SRMHD one and each
+// branch's persistent launches fill the other's tails.
+cudaError_t enqueue_ens_step(mth_ensemble* e, bool fork) {
+  cudaStream_t s = e->st;
+  cudaError_t r = phase(e, s, "dt", [&] { return ens_dt(e->d_mem, e->n, s); });
   if (r != cudaSuccess) return r;
-  if (e->has_model[MODEL_SRMHD]) {  // RK2 (RK2.cc:93-100)
-    const int md = MODEL_SRMHD;
-    if ((r = flux_phase(e, md, EA_CONS, EA_PRIMS, EA_AUX, -1, EA_P1C, STAGE_EULER))) return r;
-    if ((r = c2p_phase(e, md, EA_P1C, EA_PRIMS, EA_AUX, EA_P1P, EA_P1A))) return r;
-    if ((r = flux_phase(e, md, EA_P1C, EA_P1P, EA_P1A, EA_CONS, EA_CONS, STAGE_RK2_CORR))) return r;
-    if ((r = c2p_phase(e, md, EA_CONS, EA_PRIMS, EA_AUX, EA_PRIMS, EA_AUX))) return r;
+  const bool both = e->has_model[MODEL_SRMHD] && e->has_model[MODEL_SRRMHD];
+  if (fork && both) {
+    if ((r = cudaEventRecord(e->ev_fork, s))) return r;
+    if ((r = cudaStreamWaitEvent(e->side, e->ev_fork, 0))) return r;
+    if ((r = srrmhd_ssp2(e, e->side))) return r;
+    if ((r = cudaEventRecord(e->ev_join, e->side))) return r;
+    if ((r = srmhd_rk2(e, s))) return r;
+    if ((r = cudaStreamWaitEvent(s, e->ev_join, 0))) return r;
+  } else {
+    if (e->has_model[MODEL_SRMHD] && (r = srmhd_rk2(e, s))) return r;
+    if (e->has_model[MODEL_SRRMHD] && (r = srrmhd_ssp2(e, s))) return r;
   }
-  if (e->has_model[MODEL_SRRMHD]) {  // SSP2 (SSP2.cc:53-173), mixed form
-    const int md = MODEL_SRRMHD;
-    const int n = e->n_cells[md];
-    const int grid = std::max(1, std::min(n, e->grid_cells));
-    Item* it = e->d_cells[md];
-    if ((r = ens_imex_fast(e->d_mem, it, n, 1, grid, e->st))) return r;
-    if ((r = ens_imex_queued(e->d_mem, e->n, 1, e->st))) return r;
-    if ((r = c2p_phase(e, md, EA_U1, EA_PRIMS, EA_AUX, EA_PRIMS, EA_AUX))) return r;
-    if ((r = ens_source(e->d_mem, it, n, EA_U1, EA_AUX, EA_S1, grid, e->st))) return r;
-    if ((r = flux_phase(e, md, EA_U1, EA_PRIMS, EA_AUX, -1, EA_F1, STAGE_FNET))) return r;
-    if ((r = ens_imex_fast(e->d_mem, it, n, 2, grid, e->st))) return r;
-    if ((r = ens_imex_queued(e->d_mem, e->n, 2, e->st))) return r;
-    if ((r = c2p_phase(e, md, EA_U2, EA_PRIMS, EA_AUX, EA_PRIMS, EA_AUX))) return r;
-    if ((r = ens_source(e->d_mem, it, n, EA_U2, EA_AUX, EA_S2, grid, e->st))) return r;
-    if ((r = flux_phase(e, md, EA_U2, EA_PRIMS, EA_AUX, -1, EA_F2, STAGE_FNET))) return r;
-    if ((r = ens_combine(e->d_mem, it, n, grid, e->st))) return r;
-    if ((r = c2p_phase(e, md, EA_CONS, EA_PRIMS, EA_AUX, EA_PRIMS, EA_AUX))) return r;
-  }
-  return ens_advance(e->d_mem, e->n, e->st);
+  return phase(e, s, "advance", [&] { return ens_advance(e->d_mem, e->n, s); });
 }
 
 mth_status capture(mth_ensemble* e) {
@@ -199,7 +277,7 @@ mth_status capture(mth_ensemble* e) {
   e->st = e->own;
   cudaGraph_t g;
   ECU(e, cudaStreamBeginCapture(e->st, cudaStreamCaptureModeThreadLocal));
-  cudaError_t r = enqueue_ens_step(e);
+  cudaError_t r = enqueue_ens_step(e, true);
   cudaError_t r2 = cudaStreamEndCapture(e->st, &g);
   e->st = work;
   if (r != cudaSuccess || r2 != cudaSuccess)
@@ -255,6 +333,9 @@ mth_status mth_ensemble_create(const mth_config* cfgs, int n, mth_ensemble** out
   cudaError_t r;
   if ((r = cudaSetDevice(e->device))) { delete e; return MTH_ERR_CUDA; }
   if ((r = cudaStreamCreateWithFlags(&e->own, cudaStreamNonBlocking))) return bail(r);
+  if ((r = cudaStreamCreateWithFlags(&e->side, cudaStreamNonBlocking))) return bail(r);
+  if ((r = cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming))) return bail(r);
+  if ((r = cudaEventCreateWithFlags(&e->ev_join, cudaEventDisableTiming))) return bail(r);
   e->st = e->own;
   for (int m = 0; m < n; ++m) {
     Member& d = e->mem[m];
@@ -321,6 +402,9 @@ mth_status mth_ensemble_destroy(mth_ensemble* e) {
     if (e->d_cells[md]) cudaFree(e->d_cells[md]);
   }
   if (e->own) cudaStreamDestroy(e->own);
+  if (e->side) cudaStreamDestroy(e->side);
+  if (e->ev_fork) cudaEventDestroy(e->ev_fork);
+  if (e->ev_join) cudaEventDestroy(e->ev_join);
   delete e;
   return MTH_OK;
 }
@@ -455,6 +539,34 @@ mth_status mth_ensemble_step(mth_ensemble* e, int n_steps) {
   }
   for (int s = 0; s < n_steps; ++s) ECU(e, cudaGraphLaunch(e->graph, e->st));
   return MTH_OK;
+}
+
+mth_status mth_ensemble_profile(mth_ensemble* e, int reps, mth_kernel_time* out, int max_out,
+                                int* n_out) {
+  if (!e || reps <= 0 || (!out && max_out > 0)) return MTH_ERR_INVALID;
+  ECU(e, cudaSetDevice(e->device));
+  PhaseTimer pt;
+  ECU(e, cudaEventCreate(&pt.a));
+  ECU(e, cudaEventCreate(&pt.b));
+  e->timer = &pt;
+  cudaError_t r = cudaSuccess;
+  for (int i = 0; i < reps && r == cudaSuccess; ++i) r = enqueue_ens_step(e, false);
+  e->timer = nullptr;
+  cudaEventDestroy(pt.a);
+  cudaEventDestroy(pt.b);
+  ECU(e, r);
+  int n = 0;
+  for (const auto& x : pt.recs) {
+    if (n < max_out) {
+      std::snprintf(out[n].name, sizeof out[n].name, "%s", x.name.c_str());
+      out[n].launches = x.launches;
+      out[n].total_ms = x.ms;
+      out[n].bytes_per_launch = 0;
+    }
+    ++n;
+  }
+  if (n_out) *n_out = n;
+  return mth_ensemble_sync(e);
 }
 
 mth_status mth_ensemble_sync(mth_ensemble* e) {

@@ -14,6 +14,8 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "common.cuh"
 #include "ensemble.h"
 #include "fvs2d.cuh"
@@ -565,9 +567,18 @@ cudaError_t ens_fvs_fp32_instance(const Member* mem, const Item* items, int n, i
                                   cudaStream_t st) {
   using S = Fvs2dSmem<M, float, ORDER, TI>;
   auto kern = k_ens_fvs_fp32<M, ORDER, TI>;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)S::bytes);
-  if (e != cudaSuccess) return e;
+  static int cap = 0;  // resident CTAs of this instance on the device
+  if (!cap) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)S::bytes);
+    if (e != cudaSuccess) return e;
+    int dev = 0, sms = 0, occ = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, 32 * TI, S::bytes);
+    cap = std::max(1, occ) * std::max(1, sms);
+  }
+  grid = std::min(grid, cap);
   kern<<<grid, dim3(32, TI), S::bytes, st>>>(mem, items, n, ic, ip, ia, iu0, iout, mode);
   return cudaGetLastError();
 }

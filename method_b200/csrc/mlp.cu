@@ -4,6 +4,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <vector>
@@ -207,27 +208,170 @@ __global__ void __launch_bounds__(256) k_mlp_train(const float* __restrict__ P, 
   bias_grad(s.dZa, H, H, grad + OFF_B1);
 }
 
+// ------------------------------------------------------------- inference
+// Activations stay in registers: the m16n8k16 accumulator fragment of one
+// layer (rows g, g+8; columns 2t, 2t+1 of each 8-column tile) is, after
+// bias, ReLU and rounding to BF16, exactly the A fragment of the next layer
+// (k = 16 kc + 2t, 2t+1 from tile 2 kc; k + 8 from tile 2 kc + 1).  Weights
+// sit in shared memory in fragment order: fragment (kc, nt) of a lane is one
+// 8-byte word, B(16 kc + 2t .. +1, 8 nt + g) and B(16 kc + 2t + 8 .. +9,
+// 8 nt + g), at index (kc * NT + nt) * 32 + lane.  The arithmetic (operand
+// rounding, bias-initialised accumulators, k order) is that of forward(), so
+// both give the same outputs.  One warp owns 32 rows (two m-tiles); CTAs
+// are persistent and load the weights once.
+constexpr int KC1 = INP / 16, KCH = H / 16, NTH = H / 8, NT4 = OUTP / 8;
+
+struct InferSmem {
+  uint2 w1[KC1 * NTH * 32];
+  uint2 w2[KCH * NTH * 32];
+  uint2 w3[KCH * NTH * 32];
+  uint2 w4[KCH * NT4 * 32];
+  float b1[H], b2[H], b3[H], b4[OUTP];
+  float stats[NSTAT];
+  float x[WARPS][32][IN];   // per-warp standardised features
+  float y[WARPS][32][OUT];  // per-warp outputs (standardised)
+};
+
+__device__ void load_infer_weights(InferSmem& s, const float* __restrict__ P,
+                                   const float* __restrict__ st) {
+  auto frag = [&](uint2* dst, int off, int N, int i) {
+    const int lane = i & 31, f = i >> 5, NT = N / 8;
+    const int kc = f / NT, nt = f % NT, g = lane >> 2, t = lane & 3;
+    const int k0 = kc * 16 + 2 * t, n = nt * 8 + g;
+    auto w = [&](int k) { return __float2bfloat16(P[off + k * N + n]); };
+    dst[i] = make_uint2(pack_bf16(w(k0), w(k0 + 1)), pack_bf16(w(k0 + 8), w(k0 + 9)));
+  };
+  for (int i = threadIdx.x; i < KC1 * NTH * 32; i += blockDim.x) frag(s.w1, OFF_W1, H, i);
+  for (int i = threadIdx.x; i < KCH * NTH * 32; i += blockDim.x) {
+    frag(s.w2, OFF_W2, H, i);
+    frag(s.w3, OFF_W3, H, i);
+  }
+  for (int i = threadIdx.x; i < KCH * NT4 * 32; i += blockDim.x) frag(s.w4, OFF_W4, OUTP, i);
+  for (int i = threadIdx.x; i < H; i += blockDim.x) {
+    s.b1[i] = P[OFF_B1 + i];
+    s.b2[i] = P[OFF_B2 + i];
+    s.b3[i] = P[OFF_B3 + i];
+  }
+  for (int i = threadIdx.x; i < OUTP; i += blockDim.x) s.b4[i] = P[OFF_B4 + i];
+  for (int i = threadIdx.x; i < NSTAT; i += blockDim.x) s.stats[i] = st ? st[i] : 0.f;
+}
+
+template <int KC, int NT>
+__device__ __forceinline__ void dense_regs(const uint32_t (&a)[KC][4], const uint2* __restrict__ w,
+                                           const float* __restrict__ b, float (&c)[NT][4]) {
+  const int lane = threadIdx.x & 31, t = lane & 3;
+#pragma unroll
+  for (int nt = 0; nt < NT; ++nt) {
+    const float b0 = b[nt * 8 + 2 * t], b1 = b[nt * 8 + 2 * t + 1];
+    c[nt][0] = b0;
+    c[nt][1] = b1;
+    c[nt][2] = b0;
+    c[nt][3] = b1;
+#pragma unroll
+    for (int kc = 0; kc < KC; ++kc) {
+      const uint2 bw = w[(kc * NT + nt) * 32 + lane];
+      const uint32_t bf[2] = {bw.x, bw.y};
+      mma_bf16(c[nt], a[kc], bf);
+    }
+  }
+}
+
+template <int NT>
+__device__ __forceinline__ void relu_pack(const float (&c)[NT][4], uint32_t (&a)[NT / 2][4]) {
+  auto r = [](float v) { return __float2bfloat16(fmaxf(v, 0.f)); };
+#pragma unroll
+  for (int kc = 0; kc < NT / 2; ++kc) {
+    a[kc][0] = pack_bf16(r(c[2 * kc][0]), r(c[2 * kc][1]));
+    a[kc][1] = pack_bf16(r(c[2 * kc][2]), r(c[2 * kc][3]));
+    a[kc][2] = pack_bf16(r(c[2 * kc + 1][0]), r(c[2 * kc + 1][1]));
+    a[kc][3] = pack_bf16(r(c[2 * kc + 1][2]), r(c[2 * kc + 1][3]));
+  }
+}
+
+// The 32 rows of this warp: x (standardised features) -> y (outputs).
+// Whole warp, converged.
+__device__ __forceinline__ void warp_infer(const InferSmem& s, const float (*x)[IN],
+                                           float (*y)[OUT]) {
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+#pragma unroll
+  for (int mt = 0; mt < 2; ++mt) {
+    const int r = mt * 16 + g;
+    uint32_t a1[KC1][4];
+    a1[0][0] = pack_bf16(__float2bfloat16(x[r][2 * t]), __float2bfloat16(x[r][2 * t + 1]));
+    a1[0][1] = pack_bf16(__float2bfloat16(x[r + 8][2 * t]), __float2bfloat16(x[r + 8][2 * t + 1]));
+    a1[0][2] = 0u;  // input columns 8..15 are padding
+    a1[0][3] = 0u;
+    float c[NTH][4];
+    uint32_t a[KCH][4];
+    dense_regs<KC1, NTH>(a1, s.w1, s.b1, c);
+    relu_pack<NTH>(c, a);
+    dense_regs<KCH, NTH>(a, s.w2, s.b2, c);
+    relu_pack<NTH>(c, a);
+    dense_regs<KCH, NTH>(a, s.w3, s.b3, c);
+    relu_pack<NTH>(c, a);
+    float c4[NT4][4];
+    dense_regs<KCH, NT4>(a, s.w4, s.b4, c4);
+    if (t == 0) {
+      y[r][0] = c4[0][0];
+      y[r][1] = c4[0][1];
+      y[r + 8][0] = c4[0][2];
+      y[r + 8][1] = c4[0][3];
+    }
+  }
+}
+
 // Forward only: y[n][2] (standardised outputs) from standardised features.
-__global__ void __launch_bounds__(256) k_mlp_forward(const float* __restrict__ P, int n,
+__global__ void __launch_bounds__(256) k_mlp_forward(const float* __restrict__ P, long long n,
                                                       const float* __restrict__ x,
                                                       float* __restrict__ y) {
   extern __shared__ __align__(16) unsigned char raw[];
-  Smem& s = *reinterpret_cast<Smem*>(raw);
-  load_weights(s, P, nullptr);
-  const long long base = (long long)blockIdx.x * ROWS;
-  for (int i = threadIdx.x; i < ROWS * INP; i += blockDim.x) {
-    const int r = i / INP, k = i % INP;
-    const long long q = base + r;
-    s.X[i] = __float2bfloat16((k < IN && q < n) ? x[q * IN + k] : 0.f);
-  }
+  InferSmem& s = *reinterpret_cast<InferSmem*>(raw);
+  load_infer_weights(s, P, nullptr);
   __syncthreads();
-  forward(s);
-  __syncthreads();
-  for (int i = threadIdx.x; i < ROWS * OUT; i += blockDim.x) {
-    const int r = i / OUT, j = i % OUT;
-    const long long q = base + r;
-    if (q < n) y[q * OUT + j] = s.Y[r * OUTP + j];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (long long c0 = ((long long)blockIdx.x * WARPS + warp) * 32; c0 < n;
+       c0 += (long long)gridDim.x * WARPS * 32) {
+    const long long q = c0 + lane;
+#pragma unroll
+    for (int k = 0; k < IN; ++k) s.x[warp][lane][k] = q < n ? x[q * IN + k] : 0.f;
+    __syncwarp();
+    warp_infer(s, s.x[warp], s.y[warp]);
+    __syncwarp();
+    if (q < n) {
+      y[q * OUT] = s.y[warp][lane][0];
+      y[q * OUT + 1] = s.y[warp][lane][1];
+    }
+    __syncwarp();
   }
+}
+
+// One lane's cell: standardised features into the warp's x row; returns D.
+__device__ __forceinline__ double stage_features(InferSmem& s, int warp, int lane,
+                                                 const double* __restrict__ cons, long long N,
+                                                 long long cell) {
+  float f[IN] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  double D = 1.0;
+  if (cell >= 0) {
+    double c[9];
+#pragma unroll
+    for (int v = 0; v < 9; ++v) c[v] = cons[v * N + cell];
+    D = c[0];
+    features_srmhd(c, f);
+  }
+#pragma unroll
+  for (int k = 0; k < IN; ++k) s.x[warp][lane][k] = (f[k] - s.stats[k]) * s.stats[IN + k];
+  return D;
+}
+
+// The guess (Z, v^2) of one lane's cell from the warp's y row.
+__device__ __forceinline__ void write_guess(const InferSmem& s, int warp, int lane, double D,
+                                            long long cell, long long N,
+                                            double* __restrict__ zguess) {
+  if (cell < 0) return;
+  const float y0 = s.y[warp][lane][0] * s.stats[2 * IN + 2] + s.stats[2 * IN];
+  const float y1 = s.y[warp][lane][1] * s.stats[2 * IN + 3] + s.stats[2 * IN + 1];
+  zguess[cell] = D * (double)exp10f(y0);
+  zguess[N + cell] = fmin(fmax((double)y1, 0.0), 0.999999);
 }
 
 // Guess of Z = rho h W^2 and v^2 for every interior cell of a grid, or for
@@ -239,50 +383,80 @@ __global__ void __launch_bounds__(256) k_mlp_zguess(Grid g, long long n_cells, i
                                                      const float* __restrict__ st,
                                                      double* __restrict__ zguess) {
   extern __shared__ __align__(16) unsigned char raw[];
-  Smem& s = *reinterpret_cast<Smem*>(raw);
-  load_weights(s, P, st);
-  __shared__ double Dcell[ROWS];
-  __shared__ long long cellid[ROWS];
-  const long long base = (long long)blockIdx.x * ROWS;
-  if (threadIdx.x < ROWS) {
-    const long long t = base + threadIdx.x;
-    float f[IN] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  InferSmem& s = *reinterpret_cast<InferSmem*>(raw);
+  load_infer_weights(s, P, st);
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const long long N = batch ? n_cells : g.Ntot;
+  for (long long c0 = ((long long)blockIdx.x * WARPS + warp) * 32; c0 < n_cells;
+       c0 += (long long)gridDim.x * WARPS * 32) {
+    const long long t = c0 + lane;
     long long cell = -1;
-    double D = 1.0;
     if (t < n_cells) {
       if (batch) {
         cell = t;
       } else {
-        const int nk = g.ke - g.ks, nj = g.je - g.js;
-        const int k = g.ks + (int)(t % nk);
-        const int j = g.js + (int)((t / nk) % nj);
-        const int i = g.is + (int)(t / ((long long)nk * nj));
+        int i, j, k;
+        interior_ijk(g, t, i, j, k);
         cell = cell_id(g, i, j, k);
       }
-      const long long N = batch ? n_cells : g.Ntot;
-      double c[9];
-#pragma unroll
-      for (int v = 0; v < 9; ++v) c[v] = cons[v * N + cell];
-      D = c[0];
-      features_srmhd(c, f);
     }
-    cellid[threadIdx.x] = cell;
-    Dcell[threadIdx.x] = D;
-#pragma unroll
-    for (int k = 0; k < INP; ++k)
-      s.X[threadIdx.x * INP + k] =
-          __float2bfloat16(k < IN ? (f[k] - s.stats[k]) * s.stats[IN + k] : 0.f);
+    const double D = stage_features(s, warp, lane, cons, N, cell);
+    __syncwarp();
+    warp_infer(s, s.x[warp], s.y[warp]);
+    __syncwarp();
+    write_guess(s, warp, lane, D, cell, N, zguess);
+    __syncwarp();
   }
+}
+
+// Ensembles: the guess for the cells of every SRMHD member into the member's
+// EA_ZG planes.  A 128-cell work item is four 32-row warp chunks.
+__global__ void __launch_bounds__(256) k_ens_mlp_zguess(const Member* __restrict__ mem,
+                                                        const Item* __restrict__ items,
+                                                        int n_items, int ic,
+                                                        const float* __restrict__ P,
+                                                        const float* __restrict__ st) {
+  extern __shared__ __align__(16) unsigned char raw[];
+  InferSmem& s = *reinterpret_cast<InferSmem*>(raw);
+  load_infer_weights(s, P, st);
   __syncthreads();
-  forward(s);
-  __syncthreads();
-  if (threadIdx.x < ROWS && cellid[threadIdx.x] >= 0) {
-    const float y0 = s.Y[threadIdx.x * OUTP] * s.stats[2 * IN + 2] + s.stats[2 * IN];
-    const float y1 = s.Y[threadIdx.x * OUTP + 1] * s.stats[2 * IN + 3] + s.stats[2 * IN + 1];
-    const long long stride = batch ? n_cells : g.Ntot;
-    zguess[cellid[threadIdx.x]] = Dcell[threadIdx.x] * exp10((double)y0);
-    zguess[stride + cellid[threadIdx.x]] = fmin(fmax((double)y1, 0.0), 0.999999);
+  constexpr int PER_ITEM = ENS_CHUNK / 32;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const long long n_chunks = (long long)n_items * PER_ITEM;
+  for (long long w = (long long)blockIdx.x * WARPS + warp; w < n_chunks;
+       w += (long long)gridDim.x * WARPS) {
+    const Item it = items[w / PER_ITEM];
+    const Member& d = mem[it.m];
+    const Grid g = d.g;
+    const long long t = it.a + (w % PER_ITEM) * 32 + lane;
+    long long cell = -1;
+    if (t < n_interior(g)) {
+      int i, j, k;
+      interior_ijk(g, t, i, j, k);
+      cell = cell_id(g, i, j, k);
+    }
+    const double D = stage_features(s, warp, lane, d.a[ic], g.Ntot, cell);
+    __syncwarp();
+    warp_infer(s, s.x[warp], s.y[warp]);
+    __syncwarp();
+    write_guess(s, warp, lane, D, cell, g.Ntot, d.a[EA_ZG]);
+    __syncwarp();
   }
+}
+
+int infer_grid(const void* kern, long long rows) {
+  static int sms = 0, per_sm = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, sizeof(InferSmem));
+    if (sms < 1) sms = 148;
+    if (per_sm < 1) per_sm = 1;
+  }
+  const long long need = (rows + WARPS * 32 - 1) / (WARPS * 32);
+  return (int)std::max(1LL, std::min(need, (long long)sms * per_sm));
 }
 
 // Adam on the FP32 master parameters.
@@ -358,61 +532,6 @@ __global__ void k_standardise(long long n, float* __restrict__ feat, float* __re
 
 }  // namespace
 
-// Ensembles: the guess for the cells of every SRMHD member.  Persistent
-// CTAs load the weights once and stride over the 128-cell work items (one
-// item = one ROWS-sample tile); outputs go to the member's EA_ZG planes
-// (Z, v^2) exactly as k_mlp_zguess writes a single grid's.
-__global__ void __launch_bounds__(256) k_ens_mlp_zguess(const Member* __restrict__ mem,
-                                                        const Item* __restrict__ items,
-                                                        int n_items, int ic,
-                                                        const float* __restrict__ P,
-                                                        const float* __restrict__ st) {
-  extern __shared__ __align__(16) unsigned char raw[];
-  Smem& s = *reinterpret_cast<Smem*>(raw);
-  load_weights(s, P, st);
-  __shared__ double Dcell[ROWS];
-  __shared__ long long cellid[ROWS];
-  for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
-    const Item w = items[it];
-    const Member& d = mem[w.m];
-    const Grid g = d.g;
-    __syncthreads();  // weights loaded / previous item's outputs consumed
-    if (threadIdx.x < ROWS) {
-      const long long t = w.a + threadIdx.x;
-      float f[IN] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-      long long cell = -1;
-      double D = 1.0;
-      if (t < n_interior(g)) {
-        int i, j, k;
-        interior_ijk(g, t, i, j, k);
-        cell = cell_id(g, i, j, k);
-        const double* cons = d.a[ic];
-        double c[9];
-#pragma unroll
-        for (int v = 0; v < 9; ++v) c[v] = cons[v * g.Ntot + cell];
-        D = c[0];
-        features_srmhd(c, f);
-      }
-      cellid[threadIdx.x] = cell;
-      Dcell[threadIdx.x] = D;
-#pragma unroll
-      for (int k = 0; k < INP; ++k)
-        s.X[threadIdx.x * INP + k] =
-            __float2bfloat16(k < IN ? (f[k] - s.stats[k]) * s.stats[IN + k] : 0.f);
-    }
-    __syncthreads();
-    forward(s);
-    __syncthreads();
-    if (threadIdx.x < ROWS && cellid[threadIdx.x] >= 0) {
-      const float y0 = s.Y[threadIdx.x * OUTP] * s.stats[2 * IN + 2] + s.stats[2 * IN];
-      const float y1 = s.Y[threadIdx.x * OUTP + 1] * s.stats[2 * IN + 3] + s.stats[2 * IN + 1];
-      double* zg = d.a[EA_ZG];
-      zg[cellid[threadIdx.x]] = Dcell[threadIdx.x] * exp10((double)y0);
-      zg[g.Ntot + cellid[threadIdx.x]] = fmin(fmax((double)y1, 0.0), 0.999999);
-    }
-  }
-}
-
 static_assert(NPARAM == MLP_NPARAM, "parameter layout");
 static_assert(NSTAT == MLP_NSTAT, "statistics layout");
 
@@ -421,12 +540,13 @@ size_t smem_bytes() { return sizeof(Smem) + 16; }
 cudaError_t configure() {
   const int b = (int)sizeof(Smem);
   cudaError_t e = cudaFuncSetAttribute(k_mlp_train, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+  const int bi = (int)sizeof(InferSmem);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    e = cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, bi);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_mlp_zguess, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    e = cudaFuncSetAttribute(k_mlp_zguess, cudaFuncAttributeMaxDynamicSharedMemorySize, bi);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_ens_mlp_zguess, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    e = cudaFuncSetAttribute(k_ens_mlp_zguess, cudaFuncAttributeMaxDynamicSharedMemorySize, bi);
   return e;
 }
 
@@ -437,14 +557,15 @@ cudaError_t launch_train(const float* P, int n, const float* x, const float* t, 
 }
 
 cudaError_t launch_forward(const float* P, int n, const float* x, float* y, cudaStream_t st) {
-  k_mlp_forward<<<(n + ROWS - 1) / ROWS, 256, sizeof(Smem), st>>>(P, n, x, y);
+  k_mlp_forward<<<infer_grid((const void*)k_mlp_forward, n), 256, sizeof(InferSmem), st>>>(
+      P, n, x, y);
   return cudaGetLastError();
 }
 
 cudaError_t launch_zguess(const Grid& g, long long n_cells, bool batch, const double* cons,
                           const float* P, const float* st, double* zguess, cudaStream_t s) {
-  const int blocks = (int)((n_cells + ROWS - 1) / ROWS);
-  k_mlp_zguess<<<blocks, 256, sizeof(Smem), s>>>(g, n_cells, batch ? 1 : 0, cons, P, st, zguess);
+  k_mlp_zguess<<<infer_grid((const void*)k_mlp_zguess, n_cells), 256, sizeof(InferSmem), s>>>(
+      g, n_cells, batch ? 1 : 0, cons, P, st, zguess);
   return cudaGetLastError();
 }
 
@@ -452,8 +573,11 @@ cudaError_t launch_zguess(const Grid& g, long long n_cells, bool batch, const do
 
 cudaError_t ens_mlp_zguess(const Member* mem, const Item* items, int n_items, int ic,
                            const float* params, const float* stats, int grid, cudaStream_t st) {
-  mlp::k_ens_mlp_zguess<<<grid, 256, sizeof(mlp::Smem), st>>>(mem, items, n_items, ic, params,
-                                                              stats);
+  (void)grid;
+  const int blocks = mlp::infer_grid((const void*)mlp::k_ens_mlp_zguess,
+                                     (long long)n_items * ENS_CHUNK);
+  mlp::k_ens_mlp_zguess<<<blocks, 256, sizeof(mlp::InferSmem), st>>>(mem, items, n_items, ic,
+                                                                     params, stats);
   return cudaGetLastError();
 }
 
@@ -659,9 +783,9 @@ extern "C" mth_status mth_mlp_make_pairs(long long n, unsigned long long seed, d
   if (prims) MLP_CU(cudaMalloc(&dp.p, sizeof(double) * n * 8));
   MLP_CU(mlp::launch_make_pairs(n, seed, gamma, df.as<float>(), dt.as<float>(), dc.as<double>(),
                                 dp.as<double>(), 0));
-  MLP_CU(cudaMemcpy(feat, df.p, sizeof(float) * n * mlp::IN, cudaMemcpyDeviceToHost));
-  MLP_CU(cudaMemcpy(tgt, dt.p, sizeof(float) * n * mlp::OUT, cudaMemcpyDeviceToHost));
-  if (cons) MLP_CU(cudaMemcpy(cons, dc.p, sizeof(double) * n * 9, cudaMemcpyDeviceToHost));
-  if (prims) MLP_CU(cudaMemcpy(prims, dp.p, sizeof(double) * n * 8, cudaMemcpyDeviceToHost));
+  MLP_CU(cudaMemcpy(feat, df.p, sizeof(float) * n * mlp::IN, cudaMemcpyDefault));
+  MLP_CU(cudaMemcpy(tgt, dt.p, sizeof(float) * n * mlp::OUT, cudaMemcpyDefault));
+  if (cons) MLP_CU(cudaMemcpy(cons, dc.p, sizeof(double) * n * 9, cudaMemcpyDefault));
+  if (prims) MLP_CU(cudaMemcpy(prims, dp.p, sizeof(double) * n * 8, cudaMemcpyDefault));
   return MTH_OK;
 }

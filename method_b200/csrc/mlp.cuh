@@ -47,14 +47,15 @@ __device__ __forceinline__ void features_srmhd(const double* c, float* f) {
   const double B2 = c[5] * c[5] + c[6] * c[6] + c[7] * c[7];
   const double BS = c[5] * c[1] + c[6] * c[2] + c[7] * c[3];
   const double E = tau + D;
-  f[0] = (float)log10(fmax(tau / D, 1e-30));
-  f[1] = (float)log10(S2 / (D * D) + 1e-30);
-  f[2] = (float)log10(B2 / D + 1e-30);
+  // sums and ratios in FP64, logarithms in FP32 (the network's precision)
+  f[0] = log10f(fmaxf((float)(tau / D), 1e-30f));
+  f[1] = log10f((float)(S2 / (D * D)) + 1e-30f);
+  f[2] = log10f((float)(B2 / D) + 1e-30f);
   f[3] = (float)(BS * BS / (B2 * S2 + 1e-300));
-  f[4] = (float)log10(1.0 + fmax(tau / D, 0.0));
+  f[4] = log10f(1.f + fmaxf((float)(tau / D), 0.f));
   f[5] = (float)(sqrt(S2) / E);
   f[6] = (float)(B2 / E);
-  f[7] = (float)log10(S2 / (E * E) + 1e-30);
+  f[7] = log10f((float)(S2 / (E * E)) + 1e-30f);
 }
 
 __device__ __forceinline__ uint32_t pack_bf16(__nv_bfloat16 lo, __nv_bfloat16 hi) {

@@ -174,3 +174,50 @@ def test_ensemble_with_network_guess(trained):
         assert est["c2p_evals"] == s.stats()["c2p_evals"]
         for a, b in zip(got, want):
             assert np.array_equal(a, b)
+
+
+def test_c2p_ctx_matches_one_shot_batch(trained):
+    """The reusable workspace gives the one-shot batch call's results, run
+    after run, for every guess."""
+    import torch
+
+    from method_b200 import _lib
+    L = _lib.load()
+    P, S, _ = trained
+    n = 5000
+    gamma = 4.0 / 3.0
+    feat = np.zeros((n, 8), dtype=np.float32)
+    tgt = np.zeros((n, 2), dtype=np.float32)
+    cons = np.zeros((9, n))
+    prims = np.zeros((8, n))
+    D = C.POINTER(C.c_double)
+    assert L.mth_mlp_make_pairs(n, 99, gamma, fptr(feat), fptr(tgt), cons.ctypes.data_as(D),
+                                prims.ctypes.data_as(D), 0) == 0
+    pg = prims.copy()
+    pg[0] *= 1.01
+    ag = np.zeros((13, n))
+    ag[0] = (1 + prims[4] / prims[0] * 4.0) * 1.01
+    dc = torch.from_numpy(cons).cuda()
+    ctx = C.c_void_p()
+    assert L.mth_c2p_ctx_create(n, 0, C.byref(ctx)) == 0
+    assert L.mth_c2p_ctx_set_mlp(ctx, fptr(P), fptr(S)) == 0
+    try:
+        for method, guess in ((0, 0), (1, 0), (1, 1), (1, 2)):
+            outs = []
+            for one_shot in (True, False, False):
+                dp = torch.from_numpy(pg.copy()).cuda()
+                da = torch.from_numpy(ag.copy()).cuda()
+                st = _lib.C2PBatchStats()
+                if one_shot:
+                    L.mth_c2p_batch(gamma, n, dc.data_ptr(), dp.data_ptr(), da.data_ptr(), method,
+                                    guess, fptr(P), fptr(S), None, C.byref(st))
+                else:
+                    assert L.mth_c2p_ctx_run(ctx, gamma, n, dc.data_ptr(), dp.data_ptr(),
+                                             da.data_ptr(), method, guess, None) == 0
+                    L.mth_c2p_ctx_stats(ctx, None, C.byref(st))
+                outs.append((dp.cpu().numpy(), st.iterations, st.cells))
+            for o in outs[1:]:
+                assert np.array_equal(o[0], outs[0][0], equal_nan=True), (method, guess)
+                assert o[1:] == outs[0][1:], (method, guess)
+    finally:
+        L.mth_c2p_ctx_destroy(ctx)
