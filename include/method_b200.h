@@ -29,7 +29,8 @@ typedef enum {
 
 enum { MTH_SRMHD = 0, MTH_SRRMHD = 1 };                       /* Model subclasses */
 enum { MTH_OUTFLOW = 0, MTH_PERIODIC = 1, MTH_FLOW = 2 };     /* Bcs subclasses */
-enum { MTH_RK2 = 0, MTH_RKSPLIT = 1, MTH_SSP2 = 2 };          /* TimeIntegrator subclasses */
+enum { MTH_RK2 = 0, MTH_RKSPLIT = 1, MTH_SSP2 = 2,             /* TimeIntegrator subclasses */
+       MTH_SSP3 = 3, MTH_SSP2322 = 4 };                         /* (IMEX: SRRMHD only) */
 enum { MTH_PLAIN_FP64 = 0, MTH_MIXED = 1 };                   /* precision of the flux path */
 enum { MTH_GUESS_PREVIOUS = 0, MTH_GUESS_MLP = 1, MTH_GUESS_COLD = 2 }; /* C2P initial guess */
 enum { MTH_C2P_HYBRD = 0, MTH_C2P_NEWTON = 1 };               /* C2P solver */
@@ -45,7 +46,8 @@ typedef struct {
   double gamma, sigma, cp;
   int weno_order;            /* 3 or 5 (Weno3 / Weno5) */
   int bcs;                   /* MTH_OUTFLOW / MTH_PERIODIC / MTH_FLOW */
-  int integrator;            /* MTH_RK2 / MTH_RKSPLIT / MTH_SSP2 */
+  int integrator;            /* MTH_RK2 / MTH_RKSPLIT / MTH_SSP2 / MTH_SSP3 / MTH_SSP2322;
+                                SSP3 and SSP2322 run the plain FP64 form only */
   int precision;             /* MTH_PLAIN_FP64 / MTH_MIXED */
   int guess;                 /* MTH_GUESS_PREVIOUS / MTH_GUESS_MLP */
   int device;                /* CUDA device ordinal */

@@ -4,7 +4,7 @@
 // Class names, constructor arguments and method signatures follow the
 // reference (Project/CPU/Include/{simData,platformEnv,serialEnv,model,srmhd,
 // srrmhd,flux,fluxVectorSplitting,weno,boundaryConds,timeInt,RK2,rkSplit,
-// SSP2,initFunc,simulation}.h), so a reference driver such as
+// SSP2,SSP3,SSP2322,initFunc,simulation}.h), so a reference driver such as
 // Examples/KelvinHelmholtz/SingleFluidIdealSerial/main.cc compiles against
 // these headers and links against libmethod_b200.so.  The per-name headers
 // in this directory (simData.h, simulation.h, ...) all include this file.
@@ -256,6 +256,20 @@ class SSP2 : public TimeIntegrator {
   SSP2(Data* data, Model* model, Bcs* bcs, FluxMethod* fluxMethod)
       : TimeIntegrator(data, model, bcs, fluxMethod) {}
   int integratorId() const override { return MTH_SSP2; }
+};
+// IMEX SSP3(332) (SSP3.h:34) and SSP2(322) (SSP2322.h:34), both derived from
+// SSP2 as in the reference.
+class SSP3 : public SSP2 {
+ public:
+  SSP3(Data* data, Model* model, Bcs* bcs, FluxMethod* fluxMethod)
+      : SSP2(data, model, bcs, fluxMethod) {}
+  int integratorId() const override { return MTH_SSP3; }
+};
+class SSP2322 : public SSP2 {
+ public:
+  SSP2322(Data* data, Model* model, Bcs* bcs, FluxMethod* fluxMethod)
+      : SSP2(data, model, bcs, fluxMethod) {}
+  int integratorId() const override { return MTH_SSP2322; }
 };
 
 // ------------------------------------------------------------ initial data

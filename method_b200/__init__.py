@@ -21,7 +21,7 @@ from . import _lib
 
 MODELS = {"srmhd": 0, "srrmhd": 1}
 BCS = {"outflow": 0, "periodic": 1, "flow": 2}
-INTEGRATORS = {"rk2": 0, "rksplit": 1, "ssp2": 2}
+INTEGRATORS = {"rk2": 0, "rksplit": 1, "ssp2": 2, "ssp3": 3, "ssp2322": 4}
 PRECISIONS = {"fp64": 0, "mixed": 1}
 GUESSES = {"previous": 0, "mlp": 1}
 

@@ -33,6 +33,8 @@ struct mth_handle {
   double* solution = nullptr;
   double *u1 = nullptr, *u2 = nullptr, *flux1 = nullptr, *flux2 = nullptr;
   double *src1 = nullptr, *src2 = nullptr;
+  double *u3 = nullptr, *flux3 = nullptr, *src3 = nullptr;  // SSP3 / SSP2322
+  double *tprims = nullptr, *taux = nullptr;                // their tempprims / tempaux
   double *fnet = nullptr, *fplus = nullptr, *fminus = nullptr, *frecon = nullptr;
   int* fail_list = nullptr;
   int* fail_count = nullptr;
@@ -160,6 +162,53 @@ cudaError_t flux_stage(mth_handle* h, double* c, double* p, double* a, const dou
   return timed(h, name, dpc, [&] { return flux_stage_raw(h, c, p, a, u0, out, dt, mode); });
 }
 
+// SSP3::step (SSP3.cc:43-216) and SSP2322::step (SSP2322.cc:68-249): three
+// implicit stages, each followed by the recovery (seeded by the stage's last
+// Z), the source and FVS::F of the stage value, then the combination and the
+// final recovery.  SSP2322 never uses F(U1) (its residuals and combination
+// read F2 and F3 only), so that flux is not computed.
+cudaError_t enqueue_ssp3(mth_handle* h, double dt) {
+  const bool s3 = h->cfg.integrator == MTH_SSP3;
+  const int f0 = s3 ? 0 : 3;
+  cudaError_t e;
+  double* U[3] = {h->u1, h->u2, h->u3};
+  double* F[3] = {h->flux1, h->flux2, h->flux3};
+  double* S[3] = {h->src1, h->src2, h->src3};
+  static const char* names[2][3] = {{"imex_ssp2322_stage1", "imex_ssp2322_stage2",
+                                     "imex_ssp2322_stage3"},
+                                    {"imex_ssp3_stage1", "imex_ssp3_stage2", "imex_ssp3_stage3"}};
+  for (int k = 0; k < 3; ++k) {
+    // Z seeds: SSP3 stage 2 starts from the recovered stage-1 state, every
+    // other stage from the step's own aux (SSP3.cc:103-107, 146-159;
+    // SSP2322.cc:86-89, 127-130, 166-186)
+    const double* zaux = (s3 && k == 1) ? h->taux : h->aux;
+    if ((e = timed(h, names[s3][k], 29 + 14 * k, [&] {
+           return launch_imex_sweep(h->g, f0 + k + 1, h->cons, zaux, h->u1, h->u2, h->flux1,
+                                    h->flux2, h->src1, h->src2, U[k], h->taux, dt, imex_work(h),
+                                    h->st);
+         })))
+      return e;
+    if ((e = c2p(h, U[k], h->tprims, h->taux, h->tprims, h->taux))) return e;
+    if ((e = timed(h, "source", 31, [&] {
+           return launch_source(h->g, h->cfg.model, U[k], h->taux, S[k], h->st);
+         })))
+      return e;
+    if (!s3 && k == 0) continue;
+    if ((e = flux_stage(h, U[k], h->tprims, h->taux, nullptr, F[k], dt, STAGE_FNET))) return e;
+  }
+  if ((e = timed(h, s3 ? "ssp3_combine" : "ssp2322_combine", s3 ? 98 : 70, [&] {
+         return s3 ? launch_ssp3_combine(h->g, h->cons, h->flux1, h->flux2, h->flux3, h->src1,
+                                         h->src2, h->src3, dt, h->st)
+                   : launch_ssp2322_combine(h->g, h->cons, h->flux2, h->flux3, h->src2, h->src3,
+                                            dt, h->st);
+       })))
+    return e;
+  // SSP3 recovers from the step's own aux; SSP2322 first copies U3's
+  // recovered prims / aux over them (SSP2322.cc:236-245), of which only
+  // aux[10] seeds the recovery
+  return c2p(h, h->cons, h->prims, s3 ? h->aux : h->taux, h->prims, h->aux);
+}
+
 // One TimeIntegrator::step, enqueued on the handle's stream.
 cudaError_t enqueue_step(mth_handle* h, double dt) {
   cudaError_t e;
@@ -184,6 +233,7 @@ cudaError_t enqueue_step(mth_handle* h, double dt) {
     }
     return cudaSuccess;
   }
+  if (integ == MTH_SSP3 || integ == MTH_SSP2322) return enqueue_ssp3(h, dt);
   // SSP2::step (SSP2.cc:53-173).
   const bool fast = h->cfg.precision == MTH_MIXED;
   if ((e = timed(h, fast ? "imex_newton_stage1" : "imex_hybrd_stage1", 29, [&] {
@@ -354,7 +404,8 @@ mth_status mth_create(const mth_config* cfg, mth_handle** out) {
   if (c.sigma < 0.0 || (c.weno_order != 3 && c.weno_order != 5) ||
       c.Ng < (c.weno_order + 1) / 2 + 1 || c.nx <= 0 || c.ny < 0 || c.nz < 0 ||
       (c.ny == 0 && c.nz != 0) || c.bcs < 0 || c.bcs > 2 || c.integrator < 0 ||
-      c.integrator > 2 || (c.integrator == MTH_SSP2 && c.model != MTH_SRRMHD) ||
+      c.integrator > 4 || (c.integrator >= MTH_SSP2 && c.model != MTH_SRRMHD) ||
+      (c.integrator >= MTH_SSP3 && (c.precision != MTH_PLAIN_FP64 || c.guess != 0)) ||
       c.precision < 0 || c.precision > 1 || c.guess < 0 || c.guess > 1) {
     delete h;
     return MTH_ERR_INVALID;
@@ -383,13 +434,19 @@ mth_status mth_create(const mth_config* cfg, mth_handle** out) {
   if ((e = alloc0(&h->cons, bytes(h, h->NC), h->st))) return bail("cons", e);
   if ((e = alloc0(&h->prims, bytes(h, h->NP), h->st))) return bail("prims", e);
   if ((e = alloc0(&h->aux, bytes(h, h->NA), h->st))) return bail("aux", e);
-  if (c.integrator != MTH_SSP2) {
+  if (c.integrator == MTH_RK2 || c.integrator == MTH_RKSPLIT) {
     if ((e = alloc0(&h->p1cons, bytes(h, h->NC), h->st))) return bail("p1cons", e);
     if ((e = alloc0(&h->p1prims, bytes(h, h->NP), h->st))) return bail("p1prims", e);
     if ((e = alloc0(&h->p1aux, bytes(h, h->NA), h->st))) return bail("p1aux", e);
   } else {
     for (double** p : {&h->u1, &h->u2, &h->flux1, &h->flux2, &h->src1, &h->src2})
-      if ((e = alloc0(p, bytes(h, h->NC), h->st))) return bail("ssp2", e);
+      if ((e = alloc0(p, bytes(h, h->NC), h->st))) return bail("imex", e);
+    if (c.integrator != MTH_SSP2) {
+      for (double** p : {&h->u3, &h->flux3, &h->src3})
+        if ((e = alloc0(p, bytes(h, h->NC), h->st))) return bail("imex3", e);
+      if ((e = alloc0(&h->tprims, bytes(h, h->NP), h->st))) return bail("tempprims", e);
+      if ((e = alloc0(&h->taux, bytes(h, h->NA), h->st))) return bail("tempaux", e);
+    }
   }
   if (c.model == MTH_SRMHD && (e = alloc0(&h->solution, bytes(h, 2), h->st)))
     return bail("solution", e);
@@ -418,7 +475,7 @@ mth_status mth_destroy(mth_handle* h) {
   for (auto& kv : h->graphs) cudaGraphExecDestroy(kv.second);
   for (double* p : {h->cons, h->prims, h->aux, h->p1cons, h->p1prims, h->p1aux, h->solution,
                     h->u1, h->u2, h->flux1, h->flux2, h->src1, h->src2, h->fnet, h->fplus,
-                    h->fminus, h->frecon})
+                    h->fminus, h->frecon, h->u3, h->flux3, h->src3, h->tprims, h->taux})
     if (p) cudaFree(p);
   if (h->fail_list) cudaFree(h->fail_list);
   if (h->fail_count) cudaFree(h->fail_count);

@@ -53,6 +53,10 @@ __device__ __forceinline__ long long n_interior(const Grid& g) {
   return (long long)(g.ie - g.is) * (g.je - g.js) * (g.ke - g.ks);
 }
 
+inline long long n_interior_host(const Grid& g) {
+  return (long long)(g.ie - g.is) * (g.je - g.js) * (g.ke - g.ks);
+}
+
 // Maps an index of one direction onto the interior cell whose value the
 // reference's boundary pass would have copied there.
 __host__ __device__ inline int map_dim(int i, int n, int Ng, int kind) {

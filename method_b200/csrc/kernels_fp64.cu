@@ -480,6 +480,9 @@ __device__ __forceinline__ long long imex_cell(const Grid& g, long long cell,
   R.u = u;
   R.flux1 = f1;
   R.source1 = s1;
+  R.flux2 = nullptr;
+  R.source2 = nullptr;
+  R.hmgam = 0.0;
   R.dt = dt;
   R.gam = kImexGam;
   R.om2gam = kImexOm2Gam;
@@ -538,6 +541,110 @@ __global__ void __launch_bounds__(64)
 }
 
 __global__ void k_reset_count(int* c) { *c = 0; }
+
+// SSP3(332) / SSP2(322) implicit stages.  FORM is the residual form of
+// srrmhd::ImexResidual (1, 2, 3: SSP3 stages; 4, 5, 6: SSP2322 stages);
+// XFORM the initial guess: 0 U^n, 1 U1 (SSP3.cc:114), 2 U2 + dt (F1 + F2) / 4
+// (SSP3.cc:149-150), 3 (U^n + U2 - dt F2) / 2 (SSP2322.cc:169-171).  The Z
+// guess comes from zaux[10]; as the reference copies args.aux back into
+// tempaux after each cell's solve, the last evaluation's Z goes to zout[10],
+// which then seeds that stage's recovery.
+constexpr double kSsp3Tol = 0.0000000149011612;
+constexpr double kSsp2322Tol = 1.48e-8;
+constexpr double kImexHmGam = 0.2071067811865475;
+
+template <int FORM, int XFORM>
+__global__ void __launch_bounds__(64)
+    k_imex_sweep(Grid g, const double* __restrict__ cons, const double* zaux,
+                 const double* __restrict__ u1, const double* __restrict__ u2,
+                 const double* __restrict__ flux1, const double* __restrict__ flux2,
+                 const double* __restrict__ source1, const double* __restrict__ source2,
+                 double* __restrict__ out, double* zout, double dt, C2PWork w) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  long long evals = 0;
+  if (t < n_interior(g)) {
+    int i, j, k;
+    interior_ijk(g, t, i, j, k);
+    const long long N = g.Ntot, cell = cell_id(g, i, j, k);
+    double u[14], f1[14], f2[14], s1[14], s2[14], x[14], fv[14];
+#pragma unroll
+    for (int v = 0; v < 14; ++v) {
+      const long long o = v * N + cell;
+      u[v] = cons[o];
+      f1[v] = (FORM == 2 || FORM == 3) ? flux1[o] : 0.0;
+      s1[v] = (FORM == 2 || FORM == 3 || FORM == 5) ? source1[o] : 0.0;
+      f2[v] = (FORM == 3 || FORM == 6) ? flux2[o] : 0.0;
+      s2[v] = (FORM == 6) ? source2[o] : 0.0;
+      if (XFORM == 0) x[v] = u[v];
+      else if (XFORM == 1) x[v] = u1[o];
+      else if (XFORM == 2) x[v] = u2[o] + dt * (f1[v] + f2[v]) / 4.0;
+      else x[v] = 0.5 * (u[v] + u2[o] - dt * f2[v]);
+    }
+    srrmhd::ImexResidual R;
+    R.u = u;
+    R.flux1 = f1;
+    R.source1 = s1;
+    R.flux2 = f2;
+    R.source2 = s2;
+    R.dt = dt;
+    R.gam = kImexGam;
+    R.om2gam = kImexOm2Gam;
+    R.hmgam = kImexHmGam;
+    R.g = g.gamma;
+    R.sigma = g.sigma;
+    R.cp = g.cp;
+    R.Z = zaux[10 * N + cell];
+    R.stage = FORM;
+    R.evals = 0;
+    HybrdResult res = Hybrd<14>::solve(R, x, fv, FORM <= 3 ? kSsp3Tol : kSsp2322Tol);
+#pragma unroll
+    for (int v = 0; v < 14; ++v) out[v * N + cell] = x[v];
+    zout[10 * N + cell] = R.Z;
+    evals = res.nfev;
+    if (res.info != 1) {
+      atomicAdd((unsigned long long*)&w.counters[2], 1ull);
+      atomicOr((unsigned long long*)&w.counters[3], (unsigned long long)ERR_IMPLICIT);
+    }
+  }
+  const unsigned mask = __ballot_sync(0xffffffffu, t < n_interior(g));
+  for (int o = 16; o > 0; o >>= 1) evals += __shfl_down_sync(0xffffffffu, evals, o);
+  if ((threadIdx.x & 31) == 0 && mask) {
+    atomicAdd((unsigned long long*)&w.counters[0], (unsigned long long)__popc(mask));
+    atomicAdd((unsigned long long*)&w.counters[1], (unsigned long long)evals);
+  }
+}
+
+// SSP3(332) combination (SSP3.cc:204-214).
+__global__ void k_ssp3_combine(Grid g, double* cons, const double* __restrict__ f1,
+                               const double* __restrict__ f2, const double* __restrict__ f3,
+                               const double* __restrict__ s1, const double* __restrict__ s2,
+                               const double* __restrict__ s3, double dt) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= n_interior(g)) return;
+  int i, j, k;
+  interior_ijk(g, t, i, j, k);
+  const long long cell = cell_id(g, i, j, k);
+  for (int v = 0; v < 14; ++v) {
+    const long long o = v * g.Ntot + cell;
+    cons[o] = cons[o] - dt * (f1[o] + f2[o] + 4 * f3[o]) / 6.0 +
+              dt * (s1[o] + s2[o] + 4 * s3[o]) / 6.0;
+  }
+}
+
+// SSP2(322) combination (SSP2322.cc:224-234).
+__global__ void k_ssp2322_combine(Grid g, double* cons, const double* __restrict__ f2,
+                                  const double* __restrict__ f3, const double* __restrict__ s2,
+                                  const double* __restrict__ s3, double dt) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= n_interior(g)) return;
+  int i, j, k;
+  interior_ijk(g, t, i, j, k);
+  const long long cell = cell_id(g, i, j, k);
+  for (int v = 0; v < 14; ++v) {
+    const long long o = v * g.Ntot + cell;
+    cons[o] = cons[o] - dt * 0.5 * (f2[o] + f3[o] - s2[o] - s3[o]);
+  }
+}
 
 // SSP2 combination U += -0.5 dt (flux1 + flux2 - source1 - source2)
 // (SSP2.cc:155-166).
@@ -952,6 +1059,44 @@ cudaError_t launch_imex_stage_queued(const Grid& g, int stage, const double* con
   else
     k_imex_stage_queued<2><<<148, 64, 0, st>>>(g, cons, aux_guess, u1, flux1, source1, out, dt, w);
   k_reset_count<<<1, 1, 0, st>>>(w.fail_count);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_imex_sweep(const Grid& g, int form, const double* cons, const double* zaux,
+                              const double* u1, const double* u2, const double* flux1,
+                              const double* flux2, const double* source1, const double* source2,
+                              double* out, double* zout, double dt, C2PWork w, cudaStream_t st) {
+  const long long nI = n_interior_host(g);
+  const int b = blocks_for(nI, 64);
+#define SWEEP(F, X)                                                                        \
+  k_imex_sweep<F, X><<<b, 64, 0, st>>>(g, cons, zaux, u1, u2, flux1, flux2, source1, source2, \
+                                       out, zout, dt, w)
+  switch (form) {
+    case 1: SWEEP(1, 0); break;  // SSP3 stage 1
+    case 2: SWEEP(2, 1); break;  // SSP3 stage 2
+    case 3: SWEEP(3, 2); break;  // SSP3 stage 3
+    case 4: SWEEP(4, 0); break;  // SSP2322 stage 1
+    case 5: SWEEP(5, 0); break;  // SSP2322 stage 2
+    case 6: SWEEP(6, 3); break;  // SSP2322 stage 3
+    default: return cudaErrorInvalidValue;
+  }
+#undef SWEEP
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ssp3_combine(const Grid& g, double* cons, const double* f1, const double* f2,
+                                const double* f3, const double* s1, const double* s2,
+                                const double* s3, double dt, cudaStream_t st) {
+  k_ssp3_combine<<<blocks_for(n_interior_host(g)), kThreads, 0, st>>>(g, cons, f1, f2, f3, s1, s2,
+                                                                      s3, dt);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ssp2322_combine(const Grid& g, double* cons, const double* f2,
+                                   const double* f3, const double* s2, const double* s3,
+                                   double dt, cudaStream_t st) {
+  k_ssp2322_combine<<<blocks_for(n_interior_host(g)), kThreads, 0, st>>>(g, cons, f2, f3, s2, s3,
+                                                                         dt);
   return cudaGetLastError();
 }
 

@@ -64,6 +64,19 @@ cudaError_t launch_imex_stage_queued(const Grid& g, int stage, const double* con
                                      const double* aux_guess, const double* u1,
                                      const double* flux1, const double* source1, double* out,
                                      double dt, C2PWork w, cudaStream_t st);
+// SSP3(332) / SSP2(322) implicit stage `form` (1-3 SSP3, 4-6 SSP2322) over the
+// interior: hybrd1 on 14 unknowns per cell, U_k into `out`, the last
+// residual evaluation's Z into zout[10].
+cudaError_t launch_imex_sweep(const Grid& g, int form, const double* cons, const double* zaux,
+                              const double* u1, const double* u2, const double* flux1,
+                              const double* flux2, const double* source1, const double* source2,
+                              double* out, double* zout, double dt, C2PWork w, cudaStream_t st);
+cudaError_t launch_ssp3_combine(const Grid& g, double* cons, const double* f1, const double* f2,
+                                const double* f3, const double* s1, const double* s2,
+                                const double* s3, double dt, cudaStream_t st);
+cudaError_t launch_ssp2322_combine(const Grid& g, double* cons, const double* f2,
+                                   const double* f3, const double* s2, const double* s3,
+                                   double dt, cudaStream_t st);
 cudaError_t launch_ssp2_combine(const Grid& g, int nc, double* cons, const double* flux1,
                                 const double* flux2, const double* source1,
                                 const double* source2, double dt, cudaStream_t st);

@@ -105,8 +105,8 @@ mth_handle* Data::gpu() {
   c.weno_order = weno_ ? weno_->order : 3;
   c.bcs = bcs_ ? bcs_->bcId() : MTH_OUTFLOW;
   c.integrator = timeInt_ ? timeInt_->integratorId() : MTH_RK2;
-  if (c.integrator == MTH_SSP2 && c.model != MTH_SRRMHD)
-    throw std::invalid_argument("SSP2 is provided for the SRRMHD model");
+  if (c.integrator >= MTH_SSP2 && c.model != MTH_SRRMHD)
+    throw std::invalid_argument("the IMEX integrators are provided for the SRRMHD model");
   c.precision = precision;
   c.guess = guess;
   c.device = device;

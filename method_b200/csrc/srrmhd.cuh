@@ -194,11 +194,17 @@ __device__ __forceinline__ void prims_to_all(const double* p, double g, double s
 // Residuals of the two implicit SSP2(222) stages (SSP2.cc:194-264).  The
 // secant guess `Z` persists across evaluations exactly like the reference's
 // args.aux[10], so the chain of guesses follows hybrd's evaluation order.
+// Residual of one implicit IMEX stage for one cell.  `stage` selects the
+// form: 1, 2 = SSP2(222) stages 1, 2 (SSP2.cc:194-264; SSP3(332) stages 1, 2
+// use the same expressions, SSP3.cc:237-314); 3 = SSP3(332) stage 3
+// (SSP3.cc:335-355); 4, 5, 6 = SSP2(322) stages 1-3 (SSP2322.cc:262-383).
 struct ImexResidual {
   const double* u;        // U^n of the cell (14)
-  const double* flux1;    // stage 2 only
-  const double* source1;  // stage 2 only
-  double dt, gam, om2gam, g, sigma, cp;
+  const double* flux1;    // forms 2, 3
+  const double* source1;  // forms 2, 3, 5
+  const double* flux2;    // forms 3, 6
+  const double* source2;  // form 6
+  double dt, gam, om2gam, hmgam, g, sigma, cp;
   double Z;
   int stage;
   int evals;
@@ -216,10 +222,25 @@ struct ImexResidual {
     if (stage == 1) {
 #pragma unroll
       for (int i = 0; i < NC; ++i) fv[i] = x[i] - u[i] - dt * gam * s[i];
-    } else {
+    } else if (stage == 2) {
 #pragma unroll
       for (int i = 0; i < NC; ++i)
         fv[i] = x[i] - u[i] + dt * (flux1[i] - om2gam * source1[i] - gam * s[i]);
+    } else if (stage == 3) {
+#pragma unroll
+      for (int i = 0; i < NC; ++i)
+        fv[i] = x[i] - u[i] + dt * (flux1[i] + flux2[i]) / 4.0 -
+                dt * (hmgam * source1[i] + gam * s[i]);
+    } else if (stage == 4) {
+#pragma unroll
+      for (int i = 0; i < NC; ++i) fv[i] = x[i] - u[i] - dt * 0.5 * s[i];
+    } else if (stage == 5) {
+#pragma unroll
+      for (int i = 0; i < NC; ++i) fv[i] = x[i] - u[i] + dt * 0.5 * (source1[i] - s[i]);
+    } else {
+#pragma unroll
+      for (int i = 0; i < NC; ++i)
+        fv[i] = x[i] - u[i] + dt * (flux2[i] - 0.5 * source2[i] - 0.5 * s[i]);
     }
   }
 };

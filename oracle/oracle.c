@@ -14,6 +14,7 @@
  *   SRRMHD model ............. Project/CPU/Src/srrmhd.cc:65-581
  *   Boundary conditions ...... Project/CPU/Src/boundaryConds.cc:5-145, 449-733
  *   RK2 / RKSplit / SSP2 ..... Project/CPU/Src/RK2.cc, rkSplit.cc, SSP2.cc, IMEX2Args.cc
+ *   SSP3 / SSP2322 ........... Project/CPU/Src/SSP3.cc, SSP2322.cc, IMEX3Args.cc
  *   Simulation::updateTime ... Project/CPU/Src/simulation.cc:104-133
  *   Powell hybrid (hybrd1) ... Project/CPU/CminpackLibrary/Src/{hybrd1,hybrd,fdjac1,
  *                              qrfac,qform,dogleg,r1updt,r1mpyq,enorm}.cc
@@ -38,7 +39,7 @@ typedef struct {
   double gamma, sigma, cp;
   int weno;       /* 3 or 5 */
   int bcs;        /* 0 outflow, 1 periodic, 2 flow */
-  int integrator; /* 0 RK2, 1 RKSplit, 2 SSP2 */
+  int integrator; /* 0 RK2, 1 RKSplit, 2 SSP2, 3 SSP3, 4 SSP2322 */
 } orc_config;
 
 typedef struct {
@@ -50,6 +51,7 @@ typedef struct {
   double *cons, *prims, *aux, *f;
   double *p1cons, *p1prims, *p1aux, *args1, *args2; /* RK2 */
   double *U1, *U2, *flux1, *flux2, *source1, *source2; /* SSP2 */
+  double *U3, *flux3, *source3, *tprims, *taux;      /* SSP3 / SSP2322 */
   double *solution;                                   /* SRMHD C2P */
   double *fplus, *fminus, *fprec, *fmrec, *fx, *fy, *fz, *source;
   int failed; /* 1 C2P, 2 implicit */
@@ -949,9 +951,12 @@ static int rksplit_step(orc_sim* s, double dt) {
   return finalise(s, s->cons, s->prims, s->aux);
 }
 
-/* IMEX SSP2(222) residuals (SSP2.cc:194-264) */
+/* IMEX residuals.  kind 1, 2: SSP2(222) stages 1, 2 (SSP2.cc:194-264), also
+ * SSP3(332) stages 1, 2 (SSP3.cc:237-314, the same expressions); kind 3:
+ * SSP3(332) stage 3 (SSP3.cc:335-355); kinds 4, 5, 6: SSP2(322) stages 1-3
+ * (SSP2322.cc:262-383). */
 typedef struct {
-  double cons[14], aux10, flux1[14], source1[14], dt, g, sigma, cp;
+  double cons[14], aux10, flux1[14], source1[14], flux2[14], source2[14], dt, g, sigma, cp;
   int stage;
 } imex_ctx;
 
@@ -967,11 +972,130 @@ static void imex_residual(void* ctx, int n, const double* x, double* fvec) {
   a->aux10 = ax[10];
   if (!ok) { for (int i = 0; i < n; i++) fvec[i] = 1.0e6; return; }
   srrmhd_source_cell(x, ax, a->cp, src);
-  if (a->stage == 1)
-    for (int i = 0; i < n; i++) fvec[i] = x[i] - a->cons[i] - a->dt * gam * src[i];
-  else
-    for (int i = 0; i < n; i++)
-      fvec[i] = x[i] - a->cons[i] + a->dt * (a->flux1[i] - om2gam * a->source1[i] - gam * src[i]);
+  /* IMEX3Arguments (IMEX3Args.h:28-29) adds hmgam; SSP3's assignment from
+   * IMEX3Arguments(data) keeps the default-constructed constants as well. */
+  const double hmgam = 0.2071067811865475;
+  switch (a->stage) {
+    case 1:
+      for (int i = 0; i < n; i++) fvec[i] = x[i] - a->cons[i] - a->dt * gam * src[i];
+      break;
+    case 2:
+      for (int i = 0; i < n; i++)
+        fvec[i] = x[i] - a->cons[i] + a->dt * (a->flux1[i] - om2gam * a->source1[i] - gam * src[i]);
+      break;
+    case 3:
+      for (int i = 0; i < n; i++)
+        fvec[i] = x[i] - a->cons[i] + a->dt * (a->flux1[i] + a->flux2[i]) / 4.0 -
+                  a->dt * (hmgam * a->source1[i] + gam * src[i]);
+      break;
+    case 4:
+      for (int i = 0; i < n; i++) fvec[i] = x[i] - a->cons[i] - a->dt * 0.5 * src[i];
+      break;
+    case 5:
+      for (int i = 0; i < n; i++)
+        fvec[i] = x[i] - a->cons[i] + a->dt * 0.5 * (a->source1[i] - src[i]);
+      break;
+    default:
+      for (int i = 0; i < n; i++)
+        fvec[i] = x[i] - a->cons[i] + a->dt * (a->flux2[i] - 0.5 * a->source2[i] - 0.5 * src[i]);
+      break;
+  }
+}
+
+/* One implicit stage of SSP3 / SSP2322 over the interior: initial guess x0
+ * (xform 0: U^n; 1: U1; 2: U2 + dt (F1 + F2) / 4; 3: (U^n + U2 - dt F2) / 2),
+ * Z guess from zaux[10]; writes U_k and, as the reference copies args.aux
+ * back to tempaux, the last evaluation's Z into taux[10]. */
+static int imex_stage_sweep(orc_sim* s, int kind, int xform, double dt, double tol,
+                            const double* zaux, double* out) {
+  imex_ctx ctx;
+  double x[14], fvec[14];
+  ctx.dt = dt; ctx.g = s->c.gamma; ctx.sigma = s->c.sigma; ctx.cp = s->c.cp;
+  ctx.stage = kind;
+  for (int i = s->is; i < s->ie; i++)
+    for (int j = s->js; j < s->je; j++)
+      for (int k = s->ks; k < s->ke; k++) {
+        for (int v = 0; v < 14; v++) {
+          size_t o = IDX(s, v, i, j, k);
+          ctx.cons[v] = s->cons[o];
+          ctx.flux1[v] = s->flux1[o];
+          ctx.source1[v] = s->source1[o];
+          ctx.flux2[v] = s->flux2[o];
+          ctx.source2[v] = s->source2[o];
+          if (xform == 0) x[v] = s->cons[o];
+          else if (xform == 1) x[v] = s->U1[o];
+          else if (xform == 2) x[v] = s->U2[o] + dt * (s->flux1[o] + s->flux2[o]) / 4.0;
+          else x[v] = 0.5 * (s->cons[o] + s->U2[o] - dt * s->flux2[o]);
+        }
+        ctx.aux10 = zaux[IDX(s, 10, i, j, k)];
+        if (orc_hybrd1(imex_residual, &ctx, 14, x, fvec, tol, NULL) != 1) return 2;
+        for (int v = 0; v < 14; v++) out[IDX(s, v, i, j, k)] = x[v];
+        s->taux[IDX(s, 10, i, j, k)] = ctx.aux10;
+      }
+  return 0;
+}
+
+/* SSP3::step (SSP3.cc:43-216) */
+static int ssp3_step(orc_sim* s, double dt) {
+  const double tol = 0.0000000149011612;
+  int rc;
+  if ((rc = imex_stage_sweep(s, 1, 0, dt, tol, s->aux, s->U1))) return rc;
+  if (finalise(s, s->U1, s->tprims, s->taux)) return 1;
+  orc_source(s, s->U1, s->tprims, s->taux, s->source1);
+  orc_flux_F(s, s->U1, s->tprims, s->taux, s->flux1);
+  if ((rc = imex_stage_sweep(s, 2, 1, dt, tol, s->taux, s->U2))) return rc;
+  if (finalise(s, s->U2, s->tprims, s->taux)) return 1;
+  orc_source(s, s->U2, s->tprims, s->taux, s->source2);
+  orc_flux_F(s, s->U2, s->tprims, s->taux, s->flux2);
+  /* stage 3 starts from the step's own prims / aux (SSP3.cc:146-159) */
+  if ((rc = imex_stage_sweep(s, 3, 2, dt, tol, s->aux, s->U3))) return rc;
+  if (finalise(s, s->U3, s->tprims, s->taux)) return 1;
+  orc_source(s, s->U3, s->tprims, s->taux, s->source3);
+  orc_flux_F(s, s->U3, s->tprims, s->taux, s->flux3);
+  for (int v = 0; v < 14; v++)
+    for (int i = s->is; i < s->ie; i++)
+      for (int j = s->js; j < s->je; j++)
+        for (int k = s->ks; k < s->ke; k++) {
+          size_t o = IDX(s, v, i, j, k);
+          s->cons[o] = s->cons[o] - dt * (s->flux1[o] + s->flux2[o] + 4 * s->flux3[o]) / 6.0 +
+                       dt * (s->source1[o] + s->source2[o] + 4 * s->source3[o]) / 6.0;
+        }
+  return finalise(s, s->cons, s->prims, s->aux);
+}
+
+/* SSP2322::step (SSP2322.cc:68-249).  F(U1) is computed there but never
+ * used, so it is skipped. */
+static int ssp2322_step(orc_sim* s, double dt) {
+  const double tol = 1.48e-8;
+  int rc;
+  if ((rc = imex_stage_sweep(s, 4, 0, dt, tol, s->aux, s->U1))) return rc;
+  if (finalise(s, s->U1, s->tprims, s->taux)) return 1;
+  orc_source(s, s->U1, s->tprims, s->taux, s->source1);
+  if ((rc = imex_stage_sweep(s, 5, 0, dt, tol, s->aux, s->U2))) return rc;
+  if (finalise(s, s->U2, s->tprims, s->taux)) return 1;
+  orc_source(s, s->U2, s->tprims, s->taux, s->source2);
+  orc_flux_F(s, s->U2, s->tprims, s->taux, s->flux2);
+  if ((rc = imex_stage_sweep(s, 6, 3, dt, tol, s->aux, s->U3))) return rc;
+  if (finalise(s, s->U3, s->tprims, s->taux)) return 1;
+  orc_source(s, s->U3, s->tprims, s->taux, s->source3);
+  orc_flux_F(s, s->U3, s->tprims, s->taux, s->flux3);
+  for (int v = 0; v < 14; v++)
+    for (int i = s->is; i < s->ie; i++)
+      for (int j = s->js; j < s->je; j++)
+        for (int k = s->ks; k < s->ke; k++) {
+          size_t o = IDX(s, v, i, j, k);
+          s->cons[o] = s->cons[o] - dt * 0.5 * (s->flux2[o] + s->flux3[o] - s->source2[o] -
+                                                s->source3[o]);
+        }
+  /* prims / aux take U3's finalised values (SSP2322.cc:236-245): only aux[10]
+   * seeds the final recovery */
+  for (int i = s->is; i < s->ie; i++)
+    for (int j = s->js; j < s->je; j++)
+      for (int k = s->ks; k < s->ke; k++) {
+        for (int v = 0; v < s->NP; v++) s->prims[IDX(s, v, i, j, k)] = s->tprims[IDX(s, v, i, j, k)];
+        for (int v = 0; v < s->NA; v++) s->aux[IDX(s, v, i, j, k)] = s->taux[IDX(s, v, i, j, k)];
+      }
+  return finalise(s, s->cons, s->prims, s->aux);
 }
 
 static int ssp2_step(orc_sim* s, double dt) {
@@ -1028,7 +1152,7 @@ void orc_destroy(void* h) {
   double* arrs[] = {s->cons, s->prims, s->aux, s->f, s->p1cons, s->p1prims, s->p1aux, s->args1,
                     s->args2, s->U1, s->U2, s->flux1, s->flux2, s->source1, s->source2,
                     s->solution, s->fplus, s->fminus, s->fprec, s->fmrec, s->fx, s->fy, s->fz,
-                    s->source};
+                    s->source, s->U3, s->flux3, s->source3, s->tprims, s->taux};
   for (size_t q = 0; q < sizeof arrs / sizeof arrs[0]; q++) free(arrs[q]);
   free(s);
 }
@@ -1064,6 +1188,9 @@ void* orc_create(const orc_config* c, const double* prims) {
   s->U1 = (double*)calloc(nc, 8); s->U2 = (double*)calloc(nc, 8);
   s->flux1 = (double*)calloc(nc, 8); s->flux2 = (double*)calloc(nc, 8);
   s->source1 = (double*)calloc(nc, 8); s->source2 = (double*)calloc(nc, 8);
+  s->U3 = (double*)calloc(nc, 8); s->flux3 = (double*)calloc(nc, 8);
+  s->source3 = (double*)calloc(nc, 8);
+  s->tprims = (double*)calloc(np, 8); s->taux = (double*)calloc(na, 8);
   s->solution = (double*)calloc((size_t)2 * s->Ntot, 8);
   s->fplus = (double*)calloc(nc, 8); s->fminus = (double*)calloc(nc, 8);
   s->fprec = (double*)calloc(nc, 8); s->fmrec = (double*)calloc(nc, 8);
@@ -1084,6 +1211,8 @@ int orc_step(void* h, double dt) {
   orc_sim* s = (orc_sim*)h;
   if (s->c.integrator == 0) return rk2_step(s, dt);
   if (s->c.integrator == 1) return rksplit_step(s, dt);
+  if (s->c.integrator == 3) return ssp3_step(s, dt);
+  if (s->c.integrator == 4) return ssp2322_step(s, dt);
   return ssp2_step(s, dt);
 }
 

@@ -18,7 +18,7 @@ LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
 
 MODELS = {"srmhd": 0, "srrmhd": 1}
 BCS = {"outflow": 0, "periodic": 1, "flow": 2}
-INTEGRATORS = {"rk2": 0, "rksplit": 1, "ssp2": 2}
+INTEGRATORS = {"rk2": 0, "rksplit": 1, "ssp2": 2, "ssp3": 3, "ssp2322": 4}
 
 
 class PortConfig(C.Structure):

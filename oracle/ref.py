@@ -20,7 +20,7 @@ REF_DIR = os.path.join(HERE, "_ref")
 
 MODELS = {"srmhd": 0, "srrmhd": 1}
 BCS = {"outflow": 0, "periodic": 1, "flow": 2}
-INTEGRATORS = {"rk2": 0, "rksplit": 1, "ssp2": 2}
+INTEGRATORS = {"rk2": 0, "rksplit": 1, "ssp2": 2, "ssp3": 3, "ssp2322": 4}
 INITS = {"array": 0, "ot": 1, "kh": 2, "khrandom": 3, "briowu": 4, "currentsheet": 5}
 
 

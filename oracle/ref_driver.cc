@@ -30,7 +30,11 @@
 #include "RK2.h"
 #include "rkSplit.h"
 #include "SSP2.h"
+#include "SSP3.h"
 #include "serialEnv.h"
+
+// ref_driver_ssp2322.cc
+TimeIntegrator* mref_new_ssp2322(Data* data, Model* model, Bcs* bcs, FluxMethod* flux);
 #include "cminpack.h"
 
 extern "C" {
@@ -44,7 +48,7 @@ typedef struct {
   double gamma, sigma, cp;
   int weno;        // 3 or 5
   int bcs;         // 0 = Outflow, 1 = Periodic, 2 = Flow
-  int integrator;  // 0 = RK2, 1 = RKSplit, 2 = SSP2
+  int integrator;  // 0 = RK2, 1 = RKSplit, 2 = SSP2, 3 = SSP3, 4 = SSP2322
   int init;        // 0 = caller prims, 1 = OTVortexSingleFluid, 2 = KHInstabilitySingleFluid,
                    // 3 = KHRandomInstabilitySingleFluid, 4 = BrioWuSingleFluid,
                    // 5 = CurrentSheetSingleFluid
@@ -123,6 +127,8 @@ void* mref_create(const mref_config* c, const double* prims) {
     }
     if (c->integrator == 0) r->timeInt = new RK2(r->data, r->model, r->bcs, r->flux);
     else if (c->integrator == 1) r->timeInt = new RKSplit(r->data, r->model, r->bcs, r->flux);
+    else if (c->integrator == 3) r->timeInt = new SSP3(r->data, r->model, r->bcs, r->flux);
+    else if (c->integrator == 4) r->timeInt = mref_new_ssp2322(r->data, r->model, r->bcs, r->flux);
     else r->timeInt = new SSP2(r->data, r->model, r->bcs, r->flux);
     r->sim->set(r->init, r->model, r->timeInt, r->bcs, r->flux, NULL);
   } catch (const std::exception& e) {

@@ -140,6 +140,14 @@ LIVE = {
                         endTime=3.0, cfl=0.4, Ng=4, gamma=4.0 / 3.0, sigma=1e3, weno=3,
                         bcs="outflow", integrator="ssp2"),
                    lambda: initial.current_sheet(24, 48, seed=9), 3),
+    "sheet_ssp3": (dict(model="srrmhd", nx=16, ny=32, xmin=-0.5, xmax=0.5, ymin=-1.0, ymax=1.0,
+                        endTime=3.0, cfl=0.4, Ng=4, gamma=4.0 / 3.0, sigma=1e3, weno=3,
+                        bcs="outflow", integrator="ssp3"),
+                   lambda: initial.current_sheet(16, 32, seed=10), 2),
+    "sheet_ssp2322": (dict(model="srrmhd", nx=16, ny=32, xmin=-0.5, xmax=0.5, ymin=-1.0,
+                           ymax=1.0, endTime=3.0, cfl=0.4, Ng=4, gamma=4.0 / 3.0, sigma=1e3,
+                           weno=3, bcs="periodic", integrator="ssp2322"),
+                      lambda: initial.current_sheet(16, 32, seed=11), 2),
 }
 
 

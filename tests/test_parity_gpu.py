@@ -140,6 +140,40 @@ def test_srrmhd_ssp2(ref):
     assert_state_equal(g.state(), r.state(), "SSP2 3 steps")
 
 
+@pytest.mark.parametrize("integrator", ["ssp3", "ssp2322"])
+def test_srrmhd_imex3_brio_wu(ref, integrator):
+    """test_imex.cc IMEX3BenchmarkForParallelCode shape: SRRMHD Brio-Wu 64x16,
+    sigma 0, outflow, SSP3(332) (and SSP2(322) on the same case)."""
+    cfg = dict(model="srrmhd", nx=64, ny=16, xmin=0.0, xmax=1.0, ymin=0.0, ymax=1.0,
+               endTime=0.05, cfl=0.5, Ng=4, gamma=4.0 / 3.0, sigma=0.0, weno=3, bcs="outflow",
+               integrator=integrator)
+    import method_b200 as mb
+    r = ref.RefSim(init="briowu", init_arg0=0, **cfg)
+    _, prims, _ = r.state()
+    g = mb.Simulation(**cfg)
+    g.set_prims(prims)
+    r.update_time(3)
+    g.update_time(3)
+    assert_state_equal(g.state(), r.state(), f"{integrator} Brio-Wu 3 steps")
+
+
+@pytest.mark.parametrize("integrator,bcs,sigma",
+                         [("ssp3", "outflow", 1e3), ("ssp3", "flow", 1e5),
+                          ("ssp2322", "periodic", 1e3), ("ssp2322", "outflow", 1e5)])
+def test_srrmhd_imex3_current_sheet(ref, integrator, bcs, sigma):
+    """Resistive current sheet 32x64 with stiff conductivity, SSP3 / SSP2322."""
+    cfg = dict(model="srrmhd", nx=32, ny=64, xmin=-0.5, xmax=0.5, ymin=-1.0, ymax=1.0,
+               endTime=3.0, cfl=0.4, Ng=4, gamma=4.0 / 3.0, sigma=sigma, weno=3, bcs=bcs,
+               integrator=integrator)
+    p = initial.current_sheet(32, 64, seed=17)
+    g, r = make_pair(ref, prims=p, **cfg)
+    r.update_time(3)
+    g.update_time(3)
+    st = g.stats()
+    assert st["implicit_failed"] == 0
+    assert_state_equal(g.state(), r.state(), f"{integrator} current sheet")
+
+
 def test_3d_generic_path(ref):
     """3D (generic per-direction flux path), OT-like data, periodic."""
     n = 12
