@@ -247,6 +247,19 @@ mth_status mth_c2p_srmhd_noalloc(int nx, int ny, int nz, int Ng, double gamma,
                                  const double* aux_guess, double* prims, double* aux,
                                  double* solution, void* stream);
 
+/* SerialSaveData output (serialSaveData.cc:31-246) of the current state:
+ * `which` is a mask of MTH_SAVE_* bits; files are
+ * dir/Conserved/cons<app>.dat, dir/Primitive/prims<app>.dat,
+ * dir/Auxiliary/aux<app>.dat, dir/Domain/domain<app>.dat and
+ * dir/Constants/constants<app>.dat, byte for byte what the reference writes
+ * (values formatted as "%.16f" on the device).  The directories must exist;
+ * a file that cannot be opened gives MTH_ERR_INVALID (the reference exits).
+ * The constants' dt is the last updateTime step, or the constructor's CFL dt
+ * before the first one. */
+enum { MTH_SAVE_CONS = 1, MTH_SAVE_PRIMS = 2, MTH_SAVE_AUX = 4, MTH_SAVE_DOMAIN = 8,
+       MTH_SAVE_CONSTS = 16, MTH_SAVE_ALL = 31 };
+mth_status mth_save_text(mth_handle* h, const char* dir, const char* app, int which);
+
 /* Zero-copy access for frameworks that manage device memory themselves:
  * device pointers of cons, prims, aux (reference layout), valid until
  * mth_destroy. */

@@ -300,12 +300,37 @@ class HarrisCurrentSheet : public InitialFunc {  // SRRMHD sheet By = tanh(x / 0
   HarrisCurrentSheet(Data* data, int seed = 1234);
 };
 
-// ------------------------------------------------------------- output hook
+// ------------------------------------------------------------------ output
+// SaveData (saveData.h:17-95) and SerialSaveData (serialSaveData.h:23-86):
+// the same members, file layout and text format.  The cons / prims / aux
+// files are formatted on the device (mth_save_text); domain and constants
+// are written from Data.
 class SaveData {
  public:
+  Data* d = nullptr;
+  int Nouts = 0, Ncount = 0, test = 0;
+  char dir[50], app[50];
+  SaveData() { dir[0] = app[0] = '\0'; }
+  SaveData(Data* data, int test = 0);
   virtual ~SaveData() {}
   virtual void saveAll(bool timeSeries = false) {}
   virtual void saveVar(std::string variable, int num = 1) {}
+};
+class SerialSaveData : public SaveData {
+ public:
+  SerialEnv* env = nullptr;
+  SerialSaveData(Data* data, SerialEnv* env, int test = 0) : SaveData(data, test), env(env) {}
+  virtual ~SerialSaveData() {}
+  void saveCons();
+  void savePrims();
+  void saveAux();
+  void saveDomain();
+  void saveConsts();
+  // All of the above into Data/Final, or Data/TimeSeries with app = Nouts++
+  // (serialSaveData.cc:8-29).
+  void saveAll(bool timeSeries = false) override;
+  // One variable, every cell, into Data/TimeSeries/UserDef (serialSaveData.cc:248-361).
+  void saveVar(std::string variable, int num = 1) override;
 };
 
 // -------------------------------------------------------------- simulation

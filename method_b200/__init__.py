@@ -222,6 +222,13 @@ class Simulation:
                      total_ms=out[i].total_ms, bytes_per_launch=out[i].bytes_per_launch)
                 for i in range(min(n.value, 32))]
 
+    def save_text(self, dir, app="", which=31):
+        """SerialSaveData output: dir/Conserved/cons<app>.dat, Primitive, Auxiliary,
+        Domain and Constants files (which: mask cons 1, prims 2, aux 4, domain 8,
+        constants 16); the directories must exist."""
+        self._check(self.L.mth_save_text(self.h, str(dir).encode(), str(app).encode(),
+                                         int(which)), "save")
+
     def device_state(self):
         """Raw device pointers (cons, prims, aux) for zero-copy interop."""
         c, p, a = C.POINTER(C.c_double)(), C.POINTER(C.c_double)(), C.POINTER(C.c_double)()

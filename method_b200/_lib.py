@@ -24,7 +24,7 @@ SYMBOLS = [
     "mth_set_stream", "mth_profile_step", "mth_mlp_train", "mth_mlp_grad", "mth_mlp_forward",
     "mth_mlp_make_pairs", "mth_set_mlp", "mth_c2p_batch", "mth_c2p_ctx_create", "mth_c2p_ctx_destroy",
     "mth_c2p_ctx_set_mlp", "mth_c2p_ctx_run", "mth_c2p_ctx_stats", "mth_c2p_srmhd_noalloc",
-    "mth_device_state", "mth_ensemble_create", "mth_ensemble_destroy",
+    "mth_save_text", "mth_device_state", "mth_ensemble_create", "mth_ensemble_destroy",
     "mth_ensemble_last_error", "mth_ensemble_set_prims", "mth_ensemble_download",
     "mth_ensemble_set_mlp", "mth_ensemble_set_stream", "mth_ensemble_autotune", "mth_ensemble_step",
     "mth_ensemble_profile", "mth_ensemble_sync", "mth_ensemble_stats", "mth_ensemble_info",
@@ -105,6 +105,7 @@ def load():
     L.mth_update_time.argtypes = [H, C.c_int]
     L.mth_get_stats.argtypes = [H, C.POINTER(Stats)]
     L.mth_device_state.argtypes = [H, C.POINTER(D), C.POINTER(D), C.POINTER(D)]
+    L.mth_save_text.argtypes = [H, C.c_char_p, C.c_char_p, C.c_int]
     L.mth_step_host.argtypes = [H, D, D, D, C.c_double]
     L.mth_pin_host.argtypes = [C.c_void_p, C.c_ulonglong]
     L.mth_unpin_host.argtypes = [C.c_void_p]

@@ -10,6 +10,7 @@ Translation units and their floating-point contracts:
   mlp.cu            FMA allowed: guess-network inference / training kernels.
   api.cu            C-ABI, host logic only.
   ensemble.cu       C-ABI of ensembles (work lists, autotuner, step graph).
+  textout.cu        SerialSaveData text output formatted on the device.
   shim.cc           C++ mirror of the reference's class API over the C-ABI.
 """
 from __future__ import annotations
@@ -37,6 +38,7 @@ UNITS = [
     ("api.cu", []),
     ("noalloc.cu", []),
     ("ensemble.cu", []),
+    ("textout.cu", []),
     ("shim.cc", []),
 ]
 

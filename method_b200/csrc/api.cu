@@ -888,6 +888,91 @@ mth_status mth_c2p_batch(double gamma, long long n, const double* cons, double* 
   return rc;
 }
 
+mth_status mth_save_text(mth_handle* h, const char* dir, const char* app, int which) {
+  if (!h || !dir) return MTH_ERR_INVALID;
+  if (!app) app = "";
+  CU(h, cudaSetDevice(h->device));
+  CU(h, cudaStreamSynchronize(h->st));
+  const mth_config& c = h->cfg;
+  const Grid& g = h->g;
+  // Data labels of the two models (srmhd.cc / srrmhd.cc constructors)
+  static const char* srmhd_labels[3][13] = {
+      {"D", "Sx", "Sy", "Sz", "tau", "Bx", "By", "Bz", "phi"},
+      {"rho", "vx", "vy", "vz", "p", "Bx", "By", "Bz"},
+      {"h", "W", "e", "c", "b0", "bx", "by", "bz", "bsq", "vsq", "BS", "Bsq", "Ssq"}};
+  static const char* srrmhd_labels[3][17] = {
+      {"D", "Sx", "Sy", "Sz", "tau", "Bx", "By", "Bz", "Ex", "Ey", "Ez", "psi", "phi", "qch"},
+      {"rho", "vx", "vy", "vz", "p", "Bx", "By", "Bz", "Ex", "Ey", "Ez"},
+      {"h", "W", "e", "c", "Jx", "Jy", "Jz", "Bsq", "Esq", "vsq", "rhohWsq", "vE", "Sbarx",
+       "Sbary", "Sbarz", "Sbarsq", "tauBar"}};
+  const char* key[3] = {"cons", "prims", "aux"};
+  const char* sub[3] = {"/Conserved/cons", "/Primitive/prims", "/Auxiliary/aux"};
+  const int nv[3] = {h->NC, h->NP, h->NA};
+  const double* arr[3] = {h->cons, h->prims, h->aux};
+  for (int q = 0; q < 3; ++q) {
+    if (!(which & (1 << q))) continue;
+    std::string body;
+    CU(h, format_body(g, arr[q], nv[q], body, h->st));
+    const std::string fname = std::string(dir) + sub[q] + app + ".dat";
+    FILE* f = std::fopen(fname.c_str(), "w");
+    if (!f) return fail(h, MTH_ERR_INVALID, "could not open " + fname + " for writing");
+    std::fprintf(f, "%s = ", key[q]);
+    for (int v = 0; v < nv[q]; ++v) {
+      const char* lab = c.model == MTH_SRMHD ? srmhd_labels[q][v] : srrmhd_labels[q][v];
+      std::fprintf(f, v + 1 < nv[q] ? "%s, " : "%s\n", lab);
+    }
+    const bool ok = std::fwrite(body.data(), 1, body.size(), f) == body.size();
+    std::fclose(f);
+    if (!ok) return fail(h, MTH_ERR_INVALID, "short write to " + fname);
+  }
+  // Domain and constants: Data::initData moves the bounds of collapsed
+  // dimensions to +-1e20 (simData.cc:72-85); the Simulation constructor sets
+  // dx..dz, the cell centres and the initial dt (simulation.cc:34-61).
+  double ymin = c.ymin, ymax = c.ymax, zmin = c.zmin, zmax = c.zmax;
+  if (g.dims < 3) {
+    zmin = -1e20;
+    zmax = 1e20;
+  }
+  if (g.dims < 2) {
+    ymin = -1e20;
+    ymax = 1e20;
+  }
+  const double dx = (c.xmax - c.xmin) / (c.nx), dy = (ymax - ymin) / (c.ny),
+               dz = (zmax - zmin) / (c.nz);
+  if (which & MTH_SAVE_DOMAIN) {
+    const std::string fname = std::string(dir) + "/Domain/domain" + app + ".dat";
+    FILE* f = std::fopen(fname.c_str(), "w");
+    if (!f) return fail(h, MTH_ERR_INVALID, "could not open " + fname + " for writing");
+    for (int i = 0; i < g.Nx; ++i) std::fprintf(f, "%.16f ", c.xmin + (i + 0 + 0.5 - c.Ng) * dx);
+    std::fprintf(f, "\n");
+    for (int j = 0; j < g.Ny; ++j) std::fprintf(f, "%.16f ", ymin + (j + 0 + 0.5 - c.Ng) * dy);
+    std::fprintf(f, "\n");
+    for (int k = 0; k < g.Nz; ++k) std::fprintf(f, "%.16f ", zmin + (k + 0 + 0.5 - c.Ng) * dz);
+    std::fprintf(f, "\n");
+    std::fclose(f);
+  }
+  if (which & MTH_SAVE_CONSTS) {
+    const std::string fname = std::string(dir) + "/Constants/constants" + app + ".dat";
+    FILE* f = std::fopen(fname.c_str(), "w");
+    if (!f) return fail(h, MTH_ERR_INVALID, "could not open " + fname + " for writing");
+    const double sq = std::sqrt((double)g.dims);
+    const double dtX = c.cfl * dx / (1.0 * sq), dtY = c.cfl * dy / (1.0 * sq),
+                 dtZ = c.cfl * dz / (1.0 * sq);
+    const double dt0 = (dtX < dtY && dtX < dtZ) ? dtX : ((dtY < dtZ) ? dtY : dtZ);
+    std::fprintf(f, "constants = nx, ny, nz, Nx, Ny, Nz, xmin, xmax, ymin, ymax, zmin, zmax, "
+                    "endTime, cfl, Ng, gamma, sigma, ");
+    std::fprintf(f, "Ncons, Nprims, Naux, cp, dt, t, dx, dy, dz\n");
+    std::fprintf(f,
+                 "%d %d %d %d %d %d %.16f %.16f %.16f %.16f %.16f %.16f %.16f %.16f %d %.16f "
+                 "%.16f %d %d %d %.16f %.16f %.16f %.16f %.16f %.16f\n",
+                 c.nx, c.ny, c.nz, g.Nx, g.Ny, g.Nz, c.xmin, c.xmax, ymin, ymax, zmin, zmax,
+                 c.endTime, c.cfl, c.Ng, c.gamma, c.sigma, h->NC, h->NP, h->NA, c.cp,
+                 h->iters > 0 ? h->dt : dt0, h->t, dx, dy, dz);
+    std::fclose(f);
+  }
+  return MTH_OK;
+}
+
 mth_status mth_device_state(mth_handle* h, double** cons, double** prims, double** aux) {
   if (!h) return MTH_ERR_INVALID;
   if (cons) *cons = h->cons;

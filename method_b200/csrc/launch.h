@@ -2,6 +2,9 @@
 // C-ABI.  Every launcher enqueues on `st` and returns the launch status.
 #pragma once
 #include <cuda_runtime.h>
+
+#include <string>
+
 #include "common.cuh"
 
 namespace mth {
@@ -23,6 +26,11 @@ enum ErrFlag : long long {
 // Data::initData geometry (simData.cc:61-97) for a configuration; returns
 // false for a configuration the reference rejects.  `c` is an mth_config.
 bool grid_from_config(const void* c, Grid* g);
+
+// Body of a SerialSaveData array file (textout.cu): every interior value of
+// nvars variables as printf's "%.16f " with the reference's line breaks.
+cudaError_t format_body(const Grid& g, const double* arr, int nvars, std::string& out,
+                        cudaStream_t st);
 
 // ---- plain FP64 (bit-compatible with the reference) --------------------------
 cudaError_t launch_prims_to_all(const Grid& g, int model, const double* prims, double* cons,

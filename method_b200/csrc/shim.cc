@@ -497,3 +497,134 @@ void Simulation::evolve(bool output, int safety) {
   syncHost();
   if (output && save) save->saveVar("rho", 1);
 }
+
+// ---------------------------------------------------------------- SaveData
+SaveData::SaveData(Data* data, int test) : d(data), Nouts(0), Ncount(0), test(test) {
+  dir[0] = '\0';
+  app[0] = '\0';
+  if (test) std::strcpy(dir, "../../");
+}
+
+namespace {
+
+// The device state is authoritative unless the host arrays were changed
+// since the last download; bring the device up to date before formatting.
+mth_handle* current_device_state(Data* d) {
+  mth_handle* h = d->gpu();
+  if (!d->deviceCurrent) {
+    d->check(mth_upload(h, d->cons, d->prims, d->aux), "save");
+    d->deviceCurrent = true;
+  }
+  return h;
+}
+
+FILE* open_or_exit(const std::string& fname, const char* what) {
+  FILE* f = std::fopen(fname.c_str(), "w");
+  if (!f) {  // the reference prints and exits (serialSaveData.cc:45-48)
+    std::printf("Error: could not open '%s' for writing.\n", what);
+    std::exit(1);
+  }
+  return f;
+}
+
+void save_device_array(Data* d, const char* dir, const char* app, int which, const char* what) {
+  mth_status s = mth_save_text(current_device_state(d), dir, app, which);
+  if (s == MTH_ERR_INVALID) {
+    std::printf("Error: could not open '%s' for writing.\n", what);
+    std::exit(1);
+  }
+  d->check(s, "save");
+}
+
+}  // namespace
+
+void SerialSaveData::saveCons() { save_device_array(d, dir, app, MTH_SAVE_CONS, "cons.dat"); }
+void SerialSaveData::savePrims() { save_device_array(d, dir, app, MTH_SAVE_PRIMS, "prims.dat"); }
+void SerialSaveData::saveAux() { save_device_array(d, dir, app, MTH_SAVE_AUX, "aux.dat"); }
+
+void SerialSaveData::saveDomain() {
+  FILE* f = open_or_exit(std::string(dir) + "/Domain/domain" + app + ".dat", "domain.dat");
+  for (int i = 0; i < d->Nx; i++) std::fprintf(f, "%.16f ", d->x[i]);
+  std::fprintf(f, "\n");
+  for (int j = 0; j < d->Ny; j++) std::fprintf(f, "%.16f ", d->y[j]);
+  std::fprintf(f, "\n");
+  for (int k = 0; k < d->Nz; k++) std::fprintf(f, "%.16f ", d->z[k]);
+  std::fprintf(f, "\n");
+  std::fclose(f);
+}
+
+void SerialSaveData::saveConsts() {
+  FILE* f = open_or_exit(std::string(dir) + "/Constants/constants" + app + ".dat",
+                         "constants.dat");
+  std::fprintf(f, "constants = nx, ny, nz, Nx, Ny, Nz, xmin, xmax, ymin, ymax, zmin, zmax, "
+                  "endTime, cfl, Ng, gamma, sigma, ");
+  std::fprintf(f, "Ncons, Nprims, Naux, cp, dt, t, dx, dy, dz\n");
+  std::fprintf(f,
+               "%d %d %d %d %d %d %.16f %.16f %.16f %.16f %.16f %.16f %.16f %.16f %d %.16f %.16f "
+               "%d %d %d %.16f %.16f %.16f %.16f %.16f %.16f\n",
+               d->nx, d->ny, d->nz, d->Nx, d->Ny, d->Nz, d->xmin, d->xmax, d->ymin, d->ymax,
+               d->zmin, d->zmax, d->endTime, d->cfl, d->Ng, d->gamma, d->sigma, d->Ncons,
+               d->Nprims, d->Naux, d->cp, d->dt, d->t, d->dx, d->dy, d->dz);
+  std::fclose(f);
+}
+
+void SerialSaveData::saveAll(bool timeSeries) {
+  dir[0] = '\0';
+  if (test) std::strcpy(dir, "../../");
+  if (!timeSeries && std::strcmp(dir, "Data/Final") != 0) {
+    std::strcat(dir, "Data/Final");
+    app[0] = 0;
+  } else {
+    std::strcat(dir, "Data/TimeSeries");
+    std::snprintf(app, sizeof app, "%d", Nouts++);
+  }
+  saveCons();
+  savePrims();
+  saveAux();
+  saveDomain();
+  saveConsts();
+}
+
+void SerialSaveData::saveVar(std::string variable, int num) {
+  int cpa = 0, nvar = 0;  // cons = 1, prims = 2, aux = 3
+  for (int v = 0; v < d->Ncons && !cpa; v++)
+    if (d->consLabels[v] == variable) { cpa = 1; nvar = v; }
+  for (int v = 0; v < d->Nprims && !cpa; v++)
+    if (d->primsLabels[v] == variable) { cpa = 2; nvar = v; }
+  for (int v = 0; v < d->Naux && !cpa; v++)
+    if (d->auxLabels[v] == variable) { cpa = 3; nvar = v; }
+  if (!cpa) {
+    std::printf("Error: Could not find user specified variable '%s'\n", variable.c_str());
+    std::exit(1);
+  }
+  if (d->gpu_ && d->deviceCurrent)
+    d->check(mth_download(d->gpu_, d->cons, d->prims, d->aux), "save");
+  const std::string base = test ? "../../Data/TimeSeries/UserDef/" : "Data/TimeSeries/UserDef/";
+  std::snprintf(app, sizeof app, "%d", Nouts);
+  FILE* f = std::fopen((base + variable + app + ".dat").c_str(), "w");
+  if (!f) {
+    std::printf("Error: could not open user-defined file for writing.\n");
+    std::exit(1);
+  }
+  const double* arr = cpa == 1 ? d->cons : (cpa == 2 ? d->prims : d->aux);
+  std::fprintf(f, "var = %s, t = %18.16f\n", variable.c_str(), d->t);
+  for (int i = 0; i < d->Nx; i++)
+    for (int j = 0; j < d->Ny; j++) {
+      for (int k = 0; k < d->Nz; k++) std::fprintf(f, "%.16f ", arr[d->id(nvar, i, j, k)]);
+      std::fprintf(f, "\n");
+    }
+  std::fclose(f);
+  if (Nouts == 0) {  // the first output lists the saved variables
+    const std::string info = base + "info";
+    FILE* g = std::fopen(info.c_str(), Ncount == 0 ? "w" : "a");
+    if (g) {
+      std::fprintf(g, "%s\n", variable.c_str());
+      std::fclose(g);
+    }
+  }
+  Ncount++;
+  if (Ncount == num) {
+    Ncount = 0;
+    Nouts++;
+  }
+}

@@ -74,6 +74,8 @@ def lib(omp: bool = False):
     L.mref_weno5_upwind.restype = C.c_double
     L.mref_weno5_upwind.argtypes = [C.c_double] * 5
     L.mref_hybrd1_kat.argtypes = [C.c_int, C.c_int, D, D, C.c_double, C.c_int]
+    L.mref_save_text.argtypes = [P, C.c_char_p, C.c_char_p]
+    L.mref_save_text.restype = C.c_int
     _LIBS[name] = L
     return L
 
@@ -150,6 +152,10 @@ class RefSim:
         rc = self.L.mref_update_time(self.h, n)
         self._refresh()
         return rc
+
+    def save_text(self, dir: str, app: str = "") -> int:
+        """SerialSaveData cons/prims/aux/domain/constants files into dir."""
+        return self.L.mref_save_text(self.h, str(dir).encode(), str(app).encode())
 
     def step_dt(self, dt: float) -> int:
         rc = self.L.mref_step_dt(self.h, dt)

@@ -32,6 +32,7 @@
 #include "SSP2.h"
 #include "SSP3.h"
 #include "serialEnv.h"
+#include "serialSaveData.h"
 
 // ref_driver_ssp2322.cc
 TimeIntegrator* mref_new_ssp2322(Data* data, Model* model, Bcs* bcs, FluxMethod* flux);
@@ -172,6 +173,24 @@ void mref_info(void* h, int* ints, double* dbls) {
   ints[3] = d->Ncons; ints[4] = d->Nprims; ints[5] = d->Naux;
   ints[6] = d->iters; ints[7] = d->dims;
   dbls[0] = d->t; dbls[1] = d->dt; dbls[2] = d->dx; dbls[3] = d->dy; dbls[4] = d->dz;
+}
+
+// SerialSaveData::saveCons / savePrims / saveAux / saveDomain / saveConsts
+// (serialSaveData.cc:31-246) into dir (< 50 characters, as the reference's
+// char dir[50]; subdirectories must exist).  Returns 0, or 1 for a too-long
+// argument.
+int mref_save_text(void* h, const char* dir, const char* app) {
+  RefSim* r = static_cast<RefSim*>(h);
+  if (std::strlen(dir) >= 50 || std::strlen(app) >= 50) return 1;
+  SerialSaveData save(r->data, r->env);
+  std::strcpy(save.dir, dir);
+  std::strcpy(save.app, app);
+  save.saveCons();
+  save.savePrims();
+  save.saveAux();
+  save.saveDomain();
+  save.saveConsts();
+  return 0;
 }
 
 void mref_get_state(void* h, double* cons, double* prims, double* aux) {

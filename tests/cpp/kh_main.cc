@@ -3,7 +3,8 @@
 // drop-in headers of include/method_b200/ and linked with libmethod_b200.so.
 // Runs the SRMHD Kelvin-Helmholtz shear-layer workload for a few steps and
 // writes the final cons and prims as raw doubles to argv[1] and the initial
-// prims (after Simulation::set) to argv[2] (when given).
+// prims (after Simulation::set) to argv[2] (when given); with argv[3], also the
+// final state as SerialSaveData text files in that directory.
 #include "simData.h"
 #include "simulation.h"
 #include "initFunc.h"
@@ -12,6 +13,7 @@
 #include "RK2.h"
 #include "fluxVectorSplitting.h"
 #include "serialEnv.h"
+#include "serialSaveData.h"
 #include "weno.h"
 #include <cstdio>
 #include <cstring>
@@ -44,6 +46,15 @@ int main(int argc, char* argv[]) {
     std::fwrite(data.cons, sizeof(double), (size_t)data.Ncons * data.Ntot, f);
     std::fwrite(data.prims, sizeof(double), (size_t)data.Nprims * data.Ntot, f);
     std::fclose(f);
+  }
+  if (argc > 3) {
+    SerialSaveData save(&data, &env);
+    std::strcpy(save.dir, argv[3]);
+    save.saveCons();
+    save.savePrims();
+    save.saveAux();
+    save.saveDomain();
+    save.saveConsts();
   }
   return 0;
 }

@@ -27,7 +27,13 @@ def test_reference_style_driver_matches_reference(tmp_path, ref):
                        capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
     out, init = tmp_path / "state.bin", tmp_path / "prims0.bin"
-    r = subprocess.run([str(exe), str(out), str(init)], capture_output=True, text=True,
+    import tempfile
+    textdir = tempfile.mkdtemp(prefix="kh", dir="/tmp")  # the reference keeps dir in char[50]
+    refdir = tempfile.mkdtemp(prefix="khr", dir="/tmp")
+    for d in (textdir, refdir):
+        for sub in ("Conserved", "Primitive", "Auxiliary", "Domain", "Constants"):
+            os.makedirs(os.path.join(d, sub))
+    r = subprocess.run([str(exe), str(out), str(init), textdir], capture_output=True, text=True,
                        timeout=300)
     assert r.returncode == 0, r.stdout + r.stderr
     Nx, Ny = 72, 136
@@ -45,6 +51,13 @@ def test_reference_style_driver_matches_reference(tmp_path, ref):
     rc, rp, _ = rs.state()
     assert np.array_equal(cons, rc)
     assert np.array_equal(prims, rp)
+    # SerialSaveData files of the drop-in classes == the reference's, byte for byte
+    assert rs.save_text(refdir, "") == 0
+    for f in ("Conserved/cons.dat", "Primitive/prims.dat", "Auxiliary/aux.dat",
+              "Domain/domain.dat", "Constants/constants.dat"):
+        a = open(os.path.join(refdir, f), "rb").read()
+        b = open(os.path.join(textdir, f), "rb").read()
+        assert a == b, f
 
 
 def test_single_cell_c2p_batch_matches_oracle():
