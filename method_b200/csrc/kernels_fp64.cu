@@ -192,7 +192,10 @@ __device__ __forceinline__ long long c2p_srmhd_hybrd_cell(const Grid& g, long lo
   return res.nfev;
 }
 
-__global__ void __launch_bounds__(128)
+// Registers capped at 64 (8 resident CTAs of 128 threads): the occupancy gain
+// outweighs the spills of the hybrid method's cold branches (OT 1024^2: 0.415
+// -> 0.377 ms per launch).  Register allocation changes no result.
+__global__ void __launch_bounds__(128, 8)
     k_c2p_srmhd(Grid g, const double* __restrict__ cons, const double* prims_guess,
                 const double* aux_guess, double* prims, double* aux,
                 double* __restrict__ solution, C2PWork w) {
@@ -763,7 +766,7 @@ __global__ void __launch_bounds__(32 * TI)
   }
 }
 
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, 8)
     k_ens_c2p_srmhd_hybrd(const Member* __restrict__ mem, const Item* __restrict__ items,
                           int n_items, int ic, int ipg, int iag, int ip, int ia) {
   for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
