@@ -192,9 +192,10 @@ __device__ __forceinline__ long long c2p_srmhd_hybrd_cell(const Grid& g, long lo
   return res.nfev;
 }
 
-// Registers capped at 64 (8 resident CTAs of 128 threads): the occupancy gain
-// outweighs the spills of the hybrid method's cold branches (OT 1024^2: 0.415
-// -> 0.377 ms per launch).  Register allocation changes no result.
+// Registers capped at 64 (8 resident CTAs of 128 threads): twice the warps
+// outweigh the local-memory spills this causes (twice the DRAM writes at
+// 768^2), OT 1024^2 0.415 -> 0.377 ms per launch.  Register allocation
+// changes no result.
 __global__ void __launch_bounds__(128, 8)
     k_c2p_srmhd(Grid g, const double* __restrict__ cons, const double* prims_guess,
                 const double* aux_guess, double* prims, double* aux,

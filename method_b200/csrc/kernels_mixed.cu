@@ -201,10 +201,11 @@ __device__ __forceinline__ void tally_flush(NewtonTally tl, bool active, long lo
 }
 
 // Minimum resident CTAs the register allocation of the solver kernels is
-// sized for.  Their fallback paths (Powell hybrid, secant) are long and cold;
-// capping registers spills only there and doubles the warps that hide the
-// FP64 latency of the Newton iterations (OT 1024^2: 0.107 -> 0.090 ms per
-// C2P launch; SSP2 512x1024 stages 5-15% faster).
+// sized for.  Capping registers doubles the warps that hide the FP64 latency
+// of the Newton iterations; the values that no longer fit go to local memory
+// (the SRMHD C2P writes ~55% more DRAM bytes, much of it its long Powell-hybrid
+// fallback), and the net is faster: OT 1024^2 0.107 -> 0.090 ms per C2P
+// launch, SSP2 512x1024 stages 5-15%.
 constexpr int kNewtonMinBlocks = 8;     // 128 threads x 8 CTAs -> 64 registers
 constexpr int kEnsNewtonMinBlocks = 6;  // both models' cells in one kernel
 
