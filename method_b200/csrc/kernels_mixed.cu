@@ -499,7 +499,7 @@ __global__ void __launch_bounds__(128, kNewtonMinBlocks)
 // ---------------------------------------------------------------------------
 // Ensemble kernels (mixed form).
 template <class M, int ORDER, int TI>
-__global__ void __launch_bounds__(32 * TI)
+__global__ void __launch_bounds__(32 * TI, (fvs2d_min_blocks<M, float, ORDER, TI>()))
     k_ens_fvs_fp32(const Member* __restrict__ mem, const Item* __restrict__ items, int n_items,
                    int ic, int ip, int ia, int iu0, int iout, int mode) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
