@@ -102,7 +102,8 @@ mth_status mth_flux_F(mth_handle* h, double* fnet_host);
 /* Model::sourceTerm of the current state (every cell) into source_host. */
 mth_status mth_source(mth_handle* h, double* source_host);
 /* Model::fluxVector (model.h:121) of the current state for direction dir
- * (0, 1, 2), every cell, into f_host (Ncons*Nx*Ny*Nz doubles). */
+ * (0, 1, 2), every cell, into f_host (Ncons*Nx*Ny*Nz doubles).  As in the
+ * reference, SRRMHD's z direction leaves f_host's Sz plane as it was. */
 mth_status mth_flux_vector(mth_handle* h, int dir, double* f_host);
 
 /* Model::getPrimitiveVarsSingleCell (model.h:85) applied to n independent

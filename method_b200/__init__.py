@@ -164,6 +164,12 @@ class Simulation:
         self._check(self.L.mth_source(self.h, _dptr(s)), "sourceTerm")
         return s
 
+    def flux_vector(self, dir):
+        """Model::fluxVector of the current state along dir (0, 1, 2), every cell."""
+        f = self.zeros(self.Ncons)
+        self._check(self.L.mth_flux_vector(self.h, int(dir), _dptr(f)), "fluxVector")
+        return f
+
     def step(self, dt, sync=True):
         """TimeIntegrator::step with an explicit dt."""
         self._check(self.L.mth_step(self.h, float(dt)), "step")

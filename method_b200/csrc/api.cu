@@ -596,7 +596,17 @@ mth_status mth_flux_vector(mth_handle* h, int dir, double* f_host) {
   if (!h || !f_host || dir < 0 || dir >= 3) return MTH_ERR_INVALID;
   CU(h, cudaSetDevice(h->device));
   CU(h, launch_flux_vector(h->g, h->cfg.model, h->cons, h->prims, h->aux, dir, h->fnet, h->st));
-  CU(h, cudaMemcpyAsync(f_host, h->fnet, bytes(h, h->NC), cudaMemcpyDeviceToHost, h->st));
+  const size_t plane = bytes(h, 1);
+  if (h->cfg.model == MTH_SRRMHD && dir == 2) {
+    // SRRMHD's z flux writes Sy twice and never Sz (srrmhd.cc:159-171): the
+    // caller's Sz plane keeps what it held.  (Inside FVS::F that is the
+    // y-direction value, which the device flux supplies there.)
+    CU(h, cudaMemcpyAsync(f_host, h->fnet, 3 * plane, cudaMemcpyDeviceToHost, h->st));
+    CU(h, cudaMemcpyAsync(f_host + 4 * (plane / sizeof(double)), h->fnet + 4 * (plane / sizeof(double)),
+                          (h->NC - 4) * plane, cudaMemcpyDeviceToHost, h->st));
+  } else {
+    CU(h, cudaMemcpyAsync(f_host, h->fnet, h->NC * plane, cudaMemcpyDeviceToHost, h->st));
+  }
   CU(h, cudaStreamSynchronize(h->st));
   return MTH_OK;
 }
