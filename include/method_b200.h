@@ -46,8 +46,7 @@ typedef struct {
   double gamma, sigma, cp;
   int weno_order;            /* 3 or 5 (Weno3 / Weno5) */
   int bcs;                   /* MTH_OUTFLOW / MTH_PERIODIC / MTH_FLOW */
-  int integrator;            /* MTH_RK2 / MTH_RKSPLIT / MTH_SSP2 / MTH_SSP3 / MTH_SSP2322;
-                                SSP3 and SSP2322 run the plain FP64 form only */
+  int integrator;            /* MTH_RK2 / MTH_RKSPLIT / MTH_SSP2 / MTH_SSP3 / MTH_SSP2322 */
   int precision;             /* MTH_PLAIN_FP64 / MTH_MIXED */
   int guess;                 /* MTH_GUESS_PREVIOUS / MTH_GUESS_MLP */
   int device;                /* CUDA device ordinal */

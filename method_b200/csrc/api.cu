@@ -182,10 +182,14 @@ cudaError_t enqueue_ssp3(mth_handle* h, double dt) {
     // other stage from the step's own aux (SSP3.cc:103-107, 146-159;
     // SSP2322.cc:86-89, 127-130, 166-186)
     const double* zaux = (s3 && k == 1) ? h->taux : h->aux;
+    const bool fast = h->cfg.precision == MTH_MIXED;
     if ((e = timed(h, names[s3][k], 29 + 14 * k, [&] {
-           return launch_imex_sweep(h->g, f0 + k + 1, h->cons, zaux, h->u1, h->u2, h->flux1,
-                                    h->flux2, h->src1, h->src2, U[k], h->taux, dt, imex_work(h),
-                                    h->st);
+           return fast ? launch_imex_fast_form(h->g, f0 + k + 1, h->cons, zaux, h->u1, h->u2,
+                                               h->flux1, h->flux2, h->src1, h->src2, U[k],
+                                               h->taux, dt, imex_work(h), h->st)
+                       : launch_imex_sweep(h->g, f0 + k + 1, h->cons, zaux, h->u1, h->u2,
+                                           h->flux1, h->flux2, h->src1, h->src2, U[k], h->taux,
+                                           dt, imex_work(h), h->st);
          })))
       return e;
     if ((e = c2p(h, U[k], h->tprims, h->taux, h->tprims, h->taux))) return e;
@@ -405,7 +409,7 @@ mth_status mth_create(const mth_config* cfg, mth_handle** out) {
       c.Ng < (c.weno_order + 1) / 2 + 1 || c.nx <= 0 || c.ny < 0 || c.nz < 0 ||
       (c.ny == 0 && c.nz != 0) || c.bcs < 0 || c.bcs > 2 || c.integrator < 0 ||
       c.integrator > 4 || (c.integrator >= MTH_SSP2 && c.model != MTH_SRRMHD) ||
-      (c.integrator >= MTH_SSP3 && (c.precision != MTH_PLAIN_FP64 || c.guess != 0)) ||
+      (c.integrator >= MTH_SSP3 && c.guess != 0) ||
       c.precision < 0 || c.precision > 1 || c.guess < 0 || c.guess > 1) {
     delete h;
     return MTH_ERR_INVALID;

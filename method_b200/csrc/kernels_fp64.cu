@@ -558,6 +558,55 @@ constexpr double kSsp2322Tol = 1.48e-8;
 constexpr double kImexHmGam = 0.2071067811865475;
 
 template <int FORM, int XFORM>
+__device__ __forceinline__ long long imex_sweep_cell(
+    const Grid& g, long long cell, const double* __restrict__ cons, const double* zaux,
+    const double* __restrict__ u1, const double* __restrict__ u2,
+    const double* __restrict__ flux1, const double* __restrict__ flux2,
+    const double* __restrict__ source1, const double* __restrict__ source2,
+    double* __restrict__ out, double* zout, double dt, C2PWork w) {
+  const long long N = g.Ntot;
+  double u[14], f1[14], f2[14], s1[14], s2[14], x[14], fv[14];
+#pragma unroll
+  for (int v = 0; v < 14; ++v) {
+    const long long o = v * N + cell;
+    u[v] = cons[o];
+    f1[v] = (FORM == 2 || FORM == 3) ? flux1[o] : 0.0;
+    s1[v] = (FORM == 2 || FORM == 3 || FORM == 5) ? source1[o] : 0.0;
+    f2[v] = (FORM == 3 || FORM == 6) ? flux2[o] : 0.0;
+    s2[v] = (FORM == 6) ? source2[o] : 0.0;
+    if (XFORM == 0) x[v] = u[v];
+    else if (XFORM == 1) x[v] = u1[o];
+    else if (XFORM == 2) x[v] = u2[o] + dt * (f1[v] + f2[v]) / 4.0;
+    else x[v] = 0.5 * (u[v] + u2[o] - dt * f2[v]);
+  }
+  srrmhd::ImexResidual R;
+  R.u = u;
+  R.flux1 = f1;
+  R.source1 = s1;
+  R.flux2 = f2;
+  R.source2 = s2;
+  R.dt = dt;
+  R.gam = kImexGam;
+  R.om2gam = kImexOm2Gam;
+  R.hmgam = kImexHmGam;
+  R.g = g.gamma;
+  R.sigma = g.sigma;
+  R.cp = g.cp;
+  R.Z = zaux[10 * N + cell];
+  R.stage = FORM;
+  R.evals = 0;
+  HybrdResult res = Hybrd<14>::solve(R, x, fv, FORM <= 3 ? kSsp3Tol : kSsp2322Tol);
+#pragma unroll
+  for (int v = 0; v < 14; ++v) out[v * N + cell] = x[v];
+  zout[10 * N + cell] = R.Z;
+  if (res.info != 1) {
+    atomicAdd((unsigned long long*)&w.counters[2], 1ull);
+    atomicOr((unsigned long long*)&w.counters[3], (unsigned long long)ERR_IMPLICIT);
+  }
+  return res.nfev;
+}
+
+template <int FORM, int XFORM>
 __global__ void __launch_bounds__(64)
     k_imex_sweep(Grid g, const double* __restrict__ cons, const double* zaux,
                  const double* __restrict__ u1, const double* __restrict__ u2,
@@ -569,52 +618,31 @@ __global__ void __launch_bounds__(64)
   if (t < n_interior(g)) {
     int i, j, k;
     interior_ijk(g, t, i, j, k);
-    const long long N = g.Ntot, cell = cell_id(g, i, j, k);
-    double u[14], f1[14], f2[14], s1[14], s2[14], x[14], fv[14];
-#pragma unroll
-    for (int v = 0; v < 14; ++v) {
-      const long long o = v * N + cell;
-      u[v] = cons[o];
-      f1[v] = (FORM == 2 || FORM == 3) ? flux1[o] : 0.0;
-      s1[v] = (FORM == 2 || FORM == 3 || FORM == 5) ? source1[o] : 0.0;
-      f2[v] = (FORM == 3 || FORM == 6) ? flux2[o] : 0.0;
-      s2[v] = (FORM == 6) ? source2[o] : 0.0;
-      if (XFORM == 0) x[v] = u[v];
-      else if (XFORM == 1) x[v] = u1[o];
-      else if (XFORM == 2) x[v] = u2[o] + dt * (f1[v] + f2[v]) / 4.0;
-      else x[v] = 0.5 * (u[v] + u2[o] - dt * f2[v]);
-    }
-    srrmhd::ImexResidual R;
-    R.u = u;
-    R.flux1 = f1;
-    R.source1 = s1;
-    R.flux2 = f2;
-    R.source2 = s2;
-    R.dt = dt;
-    R.gam = kImexGam;
-    R.om2gam = kImexOm2Gam;
-    R.hmgam = kImexHmGam;
-    R.g = g.gamma;
-    R.sigma = g.sigma;
-    R.cp = g.cp;
-    R.Z = zaux[10 * N + cell];
-    R.stage = FORM;
-    R.evals = 0;
-    HybrdResult res = Hybrd<14>::solve(R, x, fv, FORM <= 3 ? kSsp3Tol : kSsp2322Tol);
-#pragma unroll
-    for (int v = 0; v < 14; ++v) out[v * N + cell] = x[v];
-    zout[10 * N + cell] = R.Z;
-    evals = res.nfev;
-    if (res.info != 1) {
-      atomicAdd((unsigned long long*)&w.counters[2], 1ull);
-      atomicOr((unsigned long long*)&w.counters[3], (unsigned long long)ERR_IMPLICIT);
-    }
+    evals = imex_sweep_cell<FORM, XFORM>(g, cell_id(g, i, j, k), cons, zaux, u1, u2, flux1,
+                                         flux2, source1, source2, out, zout, dt, w);
   }
   const unsigned mask = __ballot_sync(0xffffffffu, t < n_interior(g));
   for (int o = 16; o > 0; o >>= 1) evals += __shfl_down_sync(0xffffffffu, evals, o);
   if ((threadIdx.x & 31) == 0 && mask) {
     atomicAdd((unsigned long long*)&w.counters[0], (unsigned long long)__popc(mask));
     atomicAdd((unsigned long long*)&w.counters[1], (unsigned long long)evals);
+  }
+}
+
+// The same solve for the cells the mixed-form stage queued (grid stride over
+// the queue; the count is cleared afterwards by k_reset_count).
+template <int FORM, int XFORM>
+__global__ void __launch_bounds__(64)
+    k_imex_sweep_queued(Grid g, const double* __restrict__ cons, const double* zaux,
+                        const double* __restrict__ u1, const double* __restrict__ u2,
+                        const double* __restrict__ flux1, const double* __restrict__ flux2,
+                        const double* __restrict__ source1, const double* __restrict__ source2,
+                        double* __restrict__ out, double* zout, double dt, C2PWork w) {
+  const int n = *w.fail_count;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+    imex_sweep_cell<FORM, XFORM>(g, w.fail_list[q], cons, zaux, u1, u2, flux1, flux2, source1,
+                                 source2, out, zout, dt, w);
+    atomicAdd((unsigned long long*)&w.counters[8], 1ull);  // fallbacks
   }
 }
 
@@ -1085,6 +1113,28 @@ cudaError_t launch_imex_sweep(const Grid& g, int form, const double* cons, const
     default: return cudaErrorInvalidValue;
   }
 #undef SWEEP
+  return cudaGetLastError();
+}
+
+cudaError_t launch_imex_sweep_queued(const Grid& g, int form, const double* cons,
+                                     const double* zaux, const double* u1, const double* u2,
+                                     const double* flux1, const double* flux2,
+                                     const double* source1, const double* source2, double* out,
+                                     double* zout, double dt, C2PWork w, cudaStream_t st) {
+#define QSWEEP(F, X)                                                                     \
+  k_imex_sweep_queued<F, X><<<148, 64, 0, st>>>(g, cons, zaux, u1, u2, flux1, flux2, source1, \
+                                                source2, out, zout, dt, w)
+  switch (form) {
+    case 1: QSWEEP(1, 0); break;
+    case 2: QSWEEP(2, 1); break;
+    case 3: QSWEEP(3, 2); break;
+    case 4: QSWEEP(4, 0); break;
+    case 5: QSWEEP(5, 0); break;
+    case 6: QSWEEP(6, 3); break;
+    default: return cudaErrorInvalidValue;
+  }
+#undef QSWEEP
+  k_reset_count<<<1, 1, 0, st>>>(w.fail_count);
   return cudaGetLastError();
 }
 

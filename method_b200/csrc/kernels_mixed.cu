@@ -390,6 +390,7 @@ __global__ void __launch_bounds__(128)
 // converge is queued for the reference Powell-hybrid stage kernel.
 constexpr double kGam = 0.2928932188134525;
 constexpr double kOm2Gam = 0.4142135623730950;
+constexpr double kHmGam = 0.2071067811865475;
 
 __device__ __forceinline__ bool srrmhd_prims_newton(const double* x, double g, double& Z,
                                                     double* v, double& W, int& its) {
@@ -411,22 +412,38 @@ __device__ __forceinline__ bool srrmhd_prims_newton(const double* x, double g, d
 
 // One cell of the mixed-form implicit stage; returns false when Newton on E
 // did not converge (out then holds the last iterate).
-template <int STAGE>
-__device__ __forceinline__ bool imex_fast_cell(const Grid& g, long long cell,
+// One implicit stage x = c + a S(x) in the mixed form.  FORM selects c and a
+// from the stage's residual (srrmhd::ImexResidual forms): 1, 2 = SSP2 stages
+// and SSP3 stages 1, 2 (a = dt gam); 3 = SSP3 stage 3,
+// c = U - dt (F1 + F2) / 4 + dt hmgam S1; 4, 5, 6 = SSP2322 stages (a = dt / 2)
+// with c = U, U - dt S1 / 2, U - dt (F2 - S2 / 2).  psi and phi have closed
+// forms; E is Newton-iterated with the stiff Jacobian inverted by
+// Sherman-Morrison (v frozen per step).  The final Z goes to zout[10] when
+// zout is given (the seed of the stage's recovery).
+template <int FORM>
+__device__ __forceinline__ bool imex_fast_form(const Grid& g, long long cell,
                                                const double* __restrict__ cons,
                                                const double* __restrict__ aux_guess,
                                                const double* __restrict__ flux1,
+                                               const double* __restrict__ flux2,
                                                const double* __restrict__ source1,
-                                               double* __restrict__ out, double dt, int& its) {
+                                               const double* __restrict__ source2,
+                                               double* __restrict__ out, double* zout, double dt,
+                                               int& its) {
   const long long N = g.Ntot;
   double c[14], x[14];
 #pragma unroll
   for (int v = 0; v < 14; ++v) {
-    const double u = cons[v * N + cell];
-    c[v] = (STAGE == 1) ? u : u - dt * (flux1[v * N + cell] - kOm2Gam * source1[v * N + cell]);
+    const long long o = v * N + cell;
+    const double u = cons[o];
+    if (FORM == 1 || FORM == 4) c[v] = u;
+    else if (FORM == 2) c[v] = u - dt * (flux1[o] - kOm2Gam * source1[o]);
+    else if (FORM == 3) c[v] = u - dt * (flux1[o] + flux2[o]) / 4.0 + dt * kHmGam * source1[o];
+    else if (FORM == 5) c[v] = u - 0.5 * dt * source1[o];
+    else c[v] = u - dt * (flux2[o] - 0.5 * source2[o]);
     x[v] = c[v];
   }
-  const double a = dt * kGam, cp2 = g.cp * g.cp, sg = g.sigma;
+  const double a = FORM <= 3 ? dt * kGam : 0.5 * dt, cp2 = g.cp * g.cp, sg = g.sigma;
   x[12] = c[12] / (1 + a / cp2);
   x[11] = (c[11] + a * c[13]) / (1 + a / cp2);
   double Z = aux_guess[10 * N + cell];
@@ -465,7 +482,49 @@ __device__ __forceinline__ bool imex_fast_cell(const Grid& g, long long cell,
   }
 #pragma unroll
   for (int v = 0; v < 14; ++v) out[v * N + cell] = x[v];
+  if (zout) zout[10 * N + cell] = Z;
   return ok;
+}
+
+// SSP2 stages (forms 1, 2).
+template <int STAGE>
+__device__ __forceinline__ bool imex_fast_cell(const Grid& g, long long cell,
+                                               const double* __restrict__ cons,
+                                               const double* __restrict__ aux_guess,
+                                               const double* __restrict__ flux1,
+                                               const double* __restrict__ source1,
+                                               double* __restrict__ out, double dt, int& its) {
+  return imex_fast_form<STAGE>(g, cell, cons, aux_guess, flux1, nullptr, source1, nullptr, out,
+                               nullptr, dt, its);
+}
+
+// SSP3 / SSP2322 stages in the mixed form; failures queued for the exact solve.
+template <int FORM>
+__global__ void __launch_bounds__(128, kNewtonMinBlocks)
+    k_imex_fast_form(Grid g, const double* __restrict__ cons, const double* zaux,
+                     const double* __restrict__ flux1, const double* __restrict__ flux2,
+                     const double* __restrict__ source1, const double* __restrict__ source2,
+                     double* __restrict__ out, double* zout, double dt, C2PWork w) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  long long its_total = 0;
+  if (t < n_interior(g)) {
+    int i, j, k;
+    interior_ijk(g, t, i, j, k);
+    const long long cell = cell_id(g, i, j, k);
+    int its = 0;
+    if (!imex_fast_form<FORM>(g, cell, cons, zaux, flux1, flux2, source1, source2, out, zout, dt,
+                              its)) {
+      const int slot = atomicAdd(w.fail_count, 1);
+      w.fail_list[slot] = (int)cell;
+    }
+    its_total = its;
+  }
+  const unsigned mask = __ballot_sync(0xffffffffu, t < n_interior(g));
+  for (int o = 16; o > 0; o >>= 1) its_total += __shfl_down_sync(0xffffffffu, its_total, o);
+  if ((threadIdx.x & 31) == 0 && mask) {
+    atomicAdd((unsigned long long*)&w.counters[0], (unsigned long long)__popc(mask));
+    atomicAdd((unsigned long long*)&w.counters[1], (unsigned long long)its_total);
+  }
 }
 
 template <int STAGE>
@@ -709,6 +768,32 @@ cudaError_t launch_imex_fast(const Grid& g, int stage, const double* cons,
   if (e != cudaSuccess) return e;
   // cells the fast solve could not converge: the reference stage solve
   return launch_imex_stage_queued(g, stage, cons, aux_guess, u1, flux1, source1, out, dt, w, st);
+}
+
+cudaError_t launch_imex_fast_form(const Grid& g, int form, const double* cons,
+                                  const double* zaux, const double* u1, const double* u2,
+                                  const double* flux1, const double* flux2,
+                                  const double* source1, const double* source2, double* out,
+                                  double* zout, double dt, C2PWork w, cudaStream_t st) {
+  const int blocks = (int)((n_interior_host(g) + 127) / 128);
+#define FAST(F)                                                                          \
+  k_imex_fast_form<F><<<blocks, 128, 0, st>>>(g, cons, zaux, flux1, flux2, source1, source2, \
+                                              out, zout, dt, w)
+  switch (form) {
+    case 1: FAST(1); break;
+    case 2: FAST(2); break;
+    case 3: FAST(3); break;
+    case 4: FAST(4); break;
+    case 5: FAST(5); break;
+    case 6: FAST(6); break;
+    default: return cudaErrorInvalidValue;
+  }
+#undef FAST
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  // cells the fast solve could not converge: the reference stage solve
+  return launch_imex_sweep_queued(g, form, cons, zaux, u1, u2, flux1, flux2, source1, source2,
+                                  out, zout, dt, w, st);
 }
 
 cudaError_t mixed_init(MixedWork* w, const Grid& g, int model, cudaStream_t st) {

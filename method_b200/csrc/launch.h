@@ -79,6 +79,13 @@ cudaError_t launch_imex_sweep(const Grid& g, int form, const double* cons, const
                               const double* u1, const double* u2, const double* flux1,
                               const double* flux2, const double* source1, const double* source2,
                               double* out, double* zout, double dt, C2PWork w, cudaStream_t st);
+// The same solves for the cells queued in w.fail_list (mixed-form fallback);
+// clears the queue count afterwards.
+cudaError_t launch_imex_sweep_queued(const Grid& g, int form, const double* cons,
+                                     const double* zaux, const double* u1, const double* u2,
+                                     const double* flux1, const double* flux2,
+                                     const double* source1, const double* source2, double* out,
+                                     double* zout, double dt, C2PWork w, cudaStream_t st);
 cudaError_t launch_ssp3_combine(const Grid& g, double* cons, const double* f1, const double* f2,
                                 const double* f3, const double* s1, const double* s2,
                                 const double* s3, double dt, cudaStream_t st);

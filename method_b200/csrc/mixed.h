@@ -28,6 +28,13 @@ cudaError_t launch_zguess(const Grid& g, long long n_cells, bool batch, const do
 }  // namespace mlp
 
 // SSP2 implicit stage of the mixed form (closed-form psi/phi, Newton on E).
+// SSP3(332) / SSP2(322) implicit stage `form` (as launch_imex_sweep) in the
+// mixed form, with the exact solve for the cells it cannot converge.
+cudaError_t launch_imex_fast_form(const Grid& g, int form, const double* cons,
+                                  const double* zaux, const double* u1, const double* u2,
+                                  const double* flux1, const double* flux2,
+                                  const double* source1, const double* source2, double* out,
+                                  double* zout, double dt, C2PWork w, cudaStream_t st);
 cudaError_t launch_imex_fast(const Grid& g, int stage, const double* cons,
                              const double* aux_guess, const double* u1, const double* flux1,
                              const double* source1, double* out, double dt, C2PWork w,
