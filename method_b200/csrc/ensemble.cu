@@ -95,13 +95,6 @@ cudaError_t dalloc(mth_ensemble* e, void** p, size_t bytes) {
   return r;
 }
 
-int blocks_per_sm(const void* kern, int threads, size_t smem) {
-  int b = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kern, threads, smem) != cudaSuccess || b < 1)
-    b = 1;
-  return b;
-}
-
 // Rebuilds the flux work lists for the current tile heights (largest members
 // first, so the strided assignment starts the long tiles early).
 cudaError_t build_flux_items(mth_ensemble* e) {

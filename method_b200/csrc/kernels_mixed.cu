@@ -207,7 +207,6 @@ __device__ __forceinline__ void tally_flush(NewtonTally tl, bool active, long lo
 // fallback), and the net is faster: OT 1024^2 0.107 -> 0.090 ms per C2P
 // launch, SSP2 512x1024 stages 5-15%.
 constexpr int kNewtonMinBlocks = 8;     // 128 threads x 8 CTAs -> 64 registers
-constexpr int kEnsNewtonMinBlocks = 6;  // both models' cells in one kernel
 
 __global__ void __launch_bounds__(128, kNewtonMinBlocks)
     k_c2p_newton_srmhd(Grid g, int guess_mode, const double* __restrict__ cons,
@@ -572,7 +571,10 @@ __global__ void __launch_bounds__(32 * TI, (fvs2d_min_blocks<M, float, ORDER, TI
   }
 }
 
-__global__ void __launch_bounds__(128, kEnsNewtonMinBlocks)
+// One model's members per launch (the work list holds one model's cells), so
+// each instantiation carries one recovery method's registers.
+template <int MODEL>
+__global__ void __launch_bounds__(128, kNewtonMinBlocks)
     k_ens_c2p_newton(const Member* __restrict__ mem, const Item* __restrict__ items, int n_items,
                      int guess_mode, int ic, int ipg, int iag, int ip, int ia) {
   for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
@@ -586,7 +588,7 @@ __global__ void __launch_bounds__(128, kEnsNewtonMinBlocks)
       int i, j, k;
       interior_ijk(g, t, i, j, k);
       const long long cell = cell_id(g, i, j, k);
-      if (d.model == MODEL_SRMHD)
+      if (MODEL == MODEL_SRMHD)
         c2p_srmhd_newton_cell(g, cell, guess_mode, d.a[ic], d.a[ipg], d.a[iag], d.a[ip],
                               d.a[ia], d.a[EA_SOL], guess_mode ? d.a[EA_ZG] : nullptr, tl);
       else
@@ -597,7 +599,7 @@ __global__ void __launch_bounds__(128, kEnsNewtonMinBlocks)
 }
 
 template <int STAGE>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, kNewtonMinBlocks)
     k_ens_imex_fast(const Member* __restrict__ mem, const Item* __restrict__ items, int n_items) {
   for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
     const Item w = items[it];
@@ -697,8 +699,11 @@ cudaError_t ens_fvs_fp32(const Member* mem, const Item* items, int n, int model,
 cudaError_t ens_c2p_newton(const Member* mem, const Item* items, int n, int model,
                            int guess_mode, int ic, int ipg, int iag, int ip, int ia, int grid,
                            cudaStream_t st) {
-  k_ens_c2p_newton<<<grid, 128, 0, st>>>(mem, items, n, model == MODEL_SRMHD ? guess_mode : 0,
-                                         ic, ipg, iag, ip, ia);
+  if (model == MODEL_SRMHD)
+    k_ens_c2p_newton<MODEL_SRMHD><<<grid, 128, 0, st>>>(mem, items, n, guess_mode, ic, ipg, iag,
+                                                        ip, ia);
+  else
+    k_ens_c2p_newton<MODEL_SRRMHD><<<grid, 128, 0, st>>>(mem, items, n, 0, ic, ipg, iag, ip, ia);
   return cudaGetLastError();
 }
 
