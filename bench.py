@@ -280,15 +280,18 @@ def roofline_of(sim, dt, peak, reps=3):
                      "bytes_per_launch": top["bytes_per_launch"]}
 
 
-def ncu_traffic(kernel):
-    """DRAM bytes per launch of `kernel` from the committed ncu summary, or None."""
+def ncu_record(kernel):
+    """The committed ncu figures of `kernel` (profiles/ncu_traffic.json), or {}."""
     p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
     if not os.path.exists(p):
-        return None
+        return {}
     with open(p) as f:
-        d = json.load(f)
-    v = d.get(kernel)
-    return None if v is None else v.get("dram_bytes_per_launch_full_size")
+        return json.load(f).get(kernel) or {}
+
+
+def ncu_traffic(kernel):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary, or None."""
+    return ncu_record(kernel).get("dram_bytes_per_launch_full_size")
 
 
 def cpu_baseline(n, steps=2):
@@ -436,6 +439,11 @@ def main():
         ks, top, roof = roofline_of(r["sim"], dt, peak)
         roof["peak_kind"] = peak_kind + " (burst copy bandwidth, kernel timed alone)"
         roof["traffic"] = ncu_traffic(top["name"])
+        # what bounds the kernel instead (ncu, small case of the same workload)
+        rec = ncu_record(top["name"])
+        roof["ncu_pipes"] = {k: rec[k] for k in ("fp64_pipe_active_pct", "fma_pipe_active_pct",
+                                                 "issue_active_pct", "warps_active_pct")
+                             if k in rec} or None
         launches_per_step = sum(k["launches"] for k in ks) / 3.0
         r.update(roof=roof, kernels=ks, launches_per_step=launches_per_step)
         st = r["stats"]
