@@ -33,6 +33,34 @@ def test_invalid_configuration_rejected_on_host():
         mb.Simulation(nx=16, ny=16, sigma=-1.0)
     with pytest.raises(ValueError):  # SSP2 is provided for SRRMHD
         mb.Simulation(nx=16, ny=16, model="srmhd", integrator="ssp2")
+    for integ in ("ssp3", "ssp2322"):  # so are SSP3 and SSP2322
+        with pytest.raises(ValueError):
+            mb.Simulation(nx=16, ny=16, model="srmhd", integrator=integ)
+    with pytest.raises(ValueError):  # a 3D grid needs ny > 0 (simData.cc:66-84)
+        mb.Simulation(nx=16, ny=0, nz=8)
+    with pytest.raises(ValueError):  # WENO order 3 or 5
+        mb.Simulation(nx=16, ny=16, weno=7)
+    with pytest.raises(KeyError):  # no such boundary class
+        mb.Simulation(nx=16, ny=16, bcs="reflective")
+
+
+def test_invalid_ensembles_rejected_on_host():
+    import method_b200 as mb
+    base = dict(nx=32, ny=64, model="srmhd", integrator="rk2", precision="mixed")
+    bad = [
+        [base, dict(base, nz=8)],                                   # 3D member
+        [base, dict(base, precision="fp64")],                       # mixed precisions
+        [base, dict(base, weno=5)],                                 # mixed WENO orders
+        [dict(base, model="srrmhd", integrator="ssp2", precision="fp64")],  # plain SSP2 member
+        [dict(base, model="srrmhd", integrator="rk2")],             # SRRMHD needs SSP2 here
+        [dict(base, ny=0)],                                         # 1D member
+        [dict(base, guess="mlp", precision="fp64")],                # learned guess needs mixed
+    ]
+    for members in bad:
+        with pytest.raises(ValueError):
+            mb.Ensemble(members)
+    with pytest.raises(ValueError):  # no members
+        mb.Ensemble([])
 
 
 @pytest.mark.skipif(shutil.which("g++") is None, reason="no host compiler")
