@@ -141,13 +141,18 @@ __device__ __forceinline__ void fvs2d_tile(const Grid& g, const double* __restri
     split_cell<M, R>(g, cons, prims, aux, mapped_cell(g, gi, gj, 0), 0, sp + e, sm + e, S::RX);
   }
   __syncthreads();
-  for (int e = tid; e < NC * S::FX; e += NT) {
-    int v = e / S::FX, rem = e - v * S::FX;
-    int fi = rem / TJ, c = rem - fi * TJ;
-    const R* P = sp + v * S::RX + c;
-    const R* Mm = sm + v * S::RX + c;
+  // Item e = (v, fi, lane): a step of NT items is TI rows of faces, so the
+  // lane stays fixed and (v, fi) advance without a division.
+  for (int e = tid, v = 0, fi = ty; e < NC * S::FX; e += NT) {
+    const R* P = sp + v * S::RX + lane;
+    const R* Mm = sm + v * S::RX + lane;
     // face i0+fi: cell i-H sits at region row fi
-    sr[v * S::FX + rem] = weno_face<ORDER, R>(P, Mm, TJ, fi + H - (ORDER == 3 ? 2 : 3));
+    sr[e] = weno_face<ORDER, R>(P, Mm, TJ, fi + H - (ORDER == 3 ? 2 : 3));
+    fi += TI;
+    if (fi > TI) {
+      fi -= TI + 1;
+      ++v;
+    }
   }
   __syncthreads();
   {
@@ -168,12 +173,26 @@ __device__ __forceinline__ void fvs2d_tile(const Grid& g, const double* __restri
     split_cell<M, R>(g, cons, prims, aux, mapped_cell(g, gi, gj, 0), 1, sp + e, sm + e, S::RY);
   }
   __syncthreads();
-  for (int e = tid; e < NC * S::FY; e += NT) {
-    int v = e / S::FY, rem = e - v * S::FY;
-    int r = rem / (TJ + 1), fj = rem - r * (TJ + 1);
-    const R* P = sp + v * S::RY + r * WY;
-    const R* Mm = sm + v * S::RY + r * WY;
-    sr[v * S::FY + rem] = weno_face<ORDER, R>(P, Mm, 1, fj + H - (ORDER == 3 ? 2 : 3));
+  // Item e = (v, r, fj), rows of TJ + 1 faces; (v, r, fj) advance by NT items
+  // a step without a division (NT < FY, so v grows by one at most).
+  {
+    constexpr int RS = NT / (TJ + 1), FS = NT % (TJ + 1);
+    int v = 0, r = tid / (TJ + 1), fj = tid % (TJ + 1);
+    for (int e = tid; e < NC * S::FY; e += NT) {
+      const R* P = sp + v * S::RY + r * WY;
+      const R* Mm = sm + v * S::RY + r * WY;
+      sr[e] = weno_face<ORDER, R>(P, Mm, 1, fj + H - (ORDER == 3 ? 2 : 3));
+      fj += FS;
+      r += RS;
+      if (fj > TJ) {
+        fj -= TJ + 1;
+        ++r;
+      }
+      if (r >= TI) {
+        r -= TI;
+        ++v;
+      }
+    }
   }
   __syncthreads();
   if (ci < g.ie && cj < g.je) {

@@ -14,9 +14,55 @@ namespace srmhd {
 
 constexpr int NC = 9, NP = 8, NA = 13;
 
+// FP32 form of the same fluxes (mixed path): B^d / W and the total pressure
+// p + b^2/2 are formed once per cell instead of once per term.
+__device__ __forceinline__ void flux_fast(const float* c, const float* p, const float* a, int dir,
+                                          float* f) {
+  const float iW = __frcp_rn(a[1]);
+  const float pt = fmaf(a[8], 0.5f, p[4]);
+  if (dir == 0) {
+    const float bw = p[5] * iW;
+    f[0] = c[0] * p[1];
+    f[1] = fmaf(c[1], p[1], pt) - a[5] * bw;
+    f[2] = c[2] * p[1] - a[6] * bw;
+    f[3] = c[3] * p[1] - a[7] * bw;
+    f[4] = (c[4] + pt) * p[1] - a[4] * bw;
+    f[5] = c[8];
+    f[6] = p[6] * p[1] - p[5] * p[2];
+    f[7] = p[7] * p[1] - p[5] * p[3];
+    f[8] = p[5];
+  } else if (dir == 1) {
+    const float bw = p[6] * iW;
+    f[0] = c[0] * p[2];
+    f[1] = c[1] * p[2] - a[5] * bw;
+    f[2] = fmaf(c[2], p[2], pt) - a[6] * bw;
+    f[3] = c[3] * p[2] - a[7] * bw;
+    f[4] = (c[4] + pt) * p[2] - a[4] * bw;
+    f[5] = p[5] * p[2] - p[6] * p[1];
+    f[6] = c[8];
+    f[7] = p[7] * p[2] - p[6] * p[3];
+    f[8] = p[6];
+  } else {
+    const float bw = p[7] * iW;
+    f[0] = c[0] * p[3];
+    f[1] = c[1] * p[3] - a[5] * bw;
+    f[2] = c[2] * p[3] - a[6] * bw;
+    f[3] = fmaf(c[3], p[3], pt) - a[7] * bw;
+    f[4] = (c[4] + pt) * p[3] - a[4] * bw;
+    f[5] = p[5] * p[3] - p[7] * p[1];
+    f[6] = p[6] * p[3] - p[7] * p[2];
+    f[7] = c[8];
+    f[8] = p[6];  // as the reference (srmhd.cc:200)
+  }
+}
+
 // Model::fluxVector for one cell (srmhd.cc:72-206).  Only aux 1, 4-8 are read.
 template <typename R>
 __device__ __forceinline__ void flux(const R* c, const R* p, const R* a, int dir, R* f) {
+  if constexpr (sizeof(R) == 4) {
+    flux_fast(c, p, a, dir, f);
+    return;
+  }
   if (dir == 0) {
     f[0] = c[0] * p[1];
     f[1] = c[1] * p[1] + (p[4] + a[8] * R(0.5)) - a[5] * p[5] / a[1];

@@ -93,23 +93,26 @@ __device__ __forceinline__ float weno3_fast(float v0, float v1, float v2) {
 }
 
 __device__ __forceinline__ float weno5_fast(float v0, float v1, float v2, float v3, float v4) {
-  const float eps = 1e-16f;
-  // Jiang-Shu indicators: 13/12 (a - 2b + c)^2 + 1/4 (.)^2
-  float t0 = v0 - 2.0f * v1 + v2, u0 = v0 - 4.0f * v1 + 3.0f * v2;
-  float t1 = v1 - 2.0f * v2 + v3, u1 = v1 - v3;
-  float t2 = v2 - 2.0f * v3 + v4, u2 = 3.0f * v2 - 4.0f * v3 + v4;
-  const float c13 = 13.0f / 12.0f;
-  float b0 = fmaf(c13 * t0, t0, 0.25f * u0 * u0);
-  float b1 = fmaf(c13 * t1, t1, 0.25f * u1 * u1);
-  float b2 = fmaf(c13 * t2, t2, 0.25f * u2 * u2);
-  float a0 = __fdividef(0.1f, fmaf(b0, b0, eps));
-  float a1 = __fdividef(0.6f, fmaf(b1, b1, eps));
-  float a2 = __fdividef(0.3f, fmaf(b2, b2, eps));
-  float s0 = (2.0f * v0 - 7.0f * v1 + 11.0f * v2) * (1.0f / 6.0f);
-  float s1 = (-v1 + 5.0f * v2 + 2.0f * v3) * (1.0f / 6.0f);
-  float s2 = (2.0f * v2 + 5.0f * v3 - v4) * (1.0f / 6.0f);
-  float num = fmaf(a0, s0, fmaf(a1, s1, a2 * s2));
-  return __fdividef(num, a0 + a1 + a2);
+  // Jiang-Shu indicators times 4: 13/3 (a - 2b + c)^2 + (.)^2.  The factor
+  // scales every alpha by 1/16 once eps is scaled by 16, and the linear
+  // weights (0.1, 0.6, 0.3) are taken times 10; neither changes the
+  // normalised weights.
+  const float eps16 = 16e-16f;
+  const float t0 = fmaf(-2.0f, v1, v0) + v2, u0 = fmaf(3.0f, v2, fmaf(-4.0f, v1, v0));
+  const float t1 = fmaf(-2.0f, v2, v1) + v3, u1 = v1 - v3;
+  const float t2 = fmaf(-2.0f, v3, v2) + v4, u2 = fmaf(3.0f, v2, fmaf(-4.0f, v3, v4));
+  const float c13 = 13.0f / 3.0f;
+  const float b0 = fmaf(c13 * t0, t0, u0 * u0);
+  const float b1 = fmaf(c13 * t1, t1, u1 * u1);
+  const float b2 = fmaf(c13 * t2, t2, u2 * u2);
+  const float a0 = __fdividef(1.0f, fmaf(b0, b0, eps16));
+  const float a1 = __fdividef(6.0f, fmaf(b1, b1, eps16));
+  const float a2 = __fdividef(3.0f, fmaf(b2, b2, eps16));
+  // candidate stencils at the face, the 1/6 folded into the coefficients
+  const float s0 = fmaf(11.0f / 6.0f, v2, fmaf(-7.0f / 6.0f, v1, (1.0f / 3.0f) * v0));
+  const float s1 = fmaf(1.0f / 3.0f, v3, fmaf(5.0f / 6.0f, v2, (-1.0f / 6.0f) * v1));
+  const float s2 = fmaf(-1.0f / 6.0f, v4, fmaf(5.0f / 6.0f, v3, (1.0f / 3.0f) * v2));
+  return __fdividef(fmaf(a0, s0, fmaf(a1, s1, a2 * s2)), a0 + a1 + a2);
 }
 
 }  // namespace mth
