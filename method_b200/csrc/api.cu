@@ -113,11 +113,13 @@ cudaError_t alloc0(double** p, size_t n, cudaStream_t st) {
 }
 
 // Model::getPrimitiveVars of `cons` into prims/aux, seeded by the guess arrays.
+// `lean`: the result is read only by the fused flux tile (the RK2 predictor
+// state), so the Newton recovery writes the flux inputs alone.
 cudaError_t c2p_raw(mth_handle* h, const double* cons, const double* pg, const double* ag,
-                double* prims, double* aux) {
+                double* prims, double* aux, bool lean) {
   if (h->cfg.precision == MTH_MIXED || h->cfg.guess == MTH_GUESS_MLP)
     return launch_c2p_mixed(h->g, h->cfg.model, h->cfg.guess, cons, pg, ag, prims, aux,
-                            h->solution, c2p_work(h), h->mixed, h->st);
+                            h->solution, c2p_work(h), h->mixed, lean && h->fused, h->st);
   if (h->cfg.model == MTH_SRMHD)
     return launch_c2p_srmhd(h->g, cons, pg, ag, prims, aux, h->solution, c2p_work(h), h->st);
   return launch_c2p_srrmhd(h->g, cons, ag, prims, aux, c2p_work(h), h->st);
@@ -143,13 +145,15 @@ cudaError_t flux_stage_raw(mth_handle* h, double* c, double* p, double* a, const
 }
 
 cudaError_t c2p(mth_handle* h, const double* cons, const double* pg, const double* ag,
-                double* prims, double* aux) {
+                double* prims, double* aux, bool lean = false) {
   const bool srmhd = h->cfg.model == MTH_SRMHD;
   const bool mixed = h->cfg.precision == MTH_MIXED || h->cfg.guess == MTH_GUESS_MLP;
   const char* name = srmhd ? (mixed ? "c2p_newton_srmhd" : "c2p_hybrd_srmhd")
                            : (mixed ? "c2p_newton_srrmhd" : "c2p_secant_srrmhd");
-  return timed(h, name, srmhd ? 37 : 43,
-               [&] { return c2p_raw(h, cons, pg, ag, prims, aux); });
+  // doubles per cell: 14 read; 23 written (13 by the lean Newton recovery)
+  const bool lean_run = lean && mixed && srmhd && h->fused;
+  return timed(h, name, srmhd ? (lean_run ? 27 : 37) : 43,
+               [&] { return c2p_raw(h, cons, pg, ag, prims, aux, lean); });
 }
 
 cudaError_t flux_stage(mth_handle* h, double* c, double* p, double* a, const double* u0,
@@ -221,7 +225,7 @@ cudaError_t enqueue_step(mth_handle* h, double dt) {
     // RK2::step (RK2.cc:93-100): predictor, finalise(p1), corrector, finalise.
     if ((e = flux_stage(h, h->cons, h->prims, h->aux, nullptr, h->p1cons, dt, STAGE_EULER)))
       return e;
-    if ((e = c2p(h, h->p1cons, h->prims, h->aux, h->p1prims, h->p1aux))) return e;
+    if ((e = c2p(h, h->p1cons, h->prims, h->aux, h->p1prims, h->p1aux, true))) return e;
     if ((e = flux_stage(h, h->p1cons, h->p1prims, h->p1aux, h->cons, h->cons, dt,
                         STAGE_RK2_CORR)))
       return e;

@@ -176,8 +176,10 @@ cudaError_t flux_phase(mth_ensemble* e, cudaStream_t s, int md, int ic, int ip, 
   return cudaSuccess;
 }
 
+// lean: the recovered state is the RK2 predictor's, which only the
+// corrector's flux reads (mixed form: only the flux inputs are written).
 cudaError_t c2p_phase(mth_ensemble* e, cudaStream_t s, int md, int ic, int ipg, int iag, int ip,
-                      int ia) {
+                      int ia, bool lean = false) {
   const int n = e->n_cells[md];
   if (!n) return cudaSuccess;
   const int grid = std::max(1, std::min(n, e->grid_cells));
@@ -191,7 +193,8 @@ cudaError_t c2p_phase(mth_ensemble* e, cudaStream_t s, int md, int ic, int ipg, 
       if (r != cudaSuccess) return r;
     }
     return phase(e, s, md == MODEL_SRMHD ? "c2p_newton_srmhd" : "c2p_newton_srrmhd", [&] {
-      return ens_c2p_newton(e->d_mem, e->d_cells[md], n, md, gm, ic, ipg, iag, ip, ia, grid, s);
+      return ens_c2p_newton(e->d_mem, e->d_cells[md], n, md, gm, ic, ipg, iag, ip, ia, lean, grid,
+                            s);
     });
   }
   cudaError_t r = phase(e, s, "c2p_hybrd_srmhd", [&] {
@@ -206,7 +209,7 @@ cudaError_t srmhd_rk2(mth_ensemble* e, cudaStream_t s) {
   const int md = MODEL_SRMHD;
   cudaError_t r;
   if ((r = flux_phase(e, s, md, EA_CONS, EA_PRIMS, EA_AUX, -1, EA_P1C, STAGE_EULER))) return r;
-  if ((r = c2p_phase(e, s, md, EA_P1C, EA_PRIMS, EA_AUX, EA_P1P, EA_P1A))) return r;
+  if ((r = c2p_phase(e, s, md, EA_P1C, EA_PRIMS, EA_AUX, EA_P1P, EA_P1A, true))) return r;
   if ((r = flux_phase(e, s, md, EA_P1C, EA_P1P, EA_P1A, EA_CONS, EA_CONS, STAGE_RK2_CORR)))
     return r;
   return c2p_phase(e, s, md, EA_CONS, EA_PRIMS, EA_AUX, EA_PRIMS, EA_AUX);

@@ -61,9 +61,11 @@ cudaError_t ens_fvs_fp32(const Member* mem, const Item* items, int n_items, int 
                          int TI, int ic, int ip, int ia, int iu0, int iout, int mode, int grid,
                          cudaStream_t st);
 // guess_mode 1: SRMHD members start Newton from the learned guess in EA_ZG.
+// lean (SRMHD): write only the flux inputs (prims 1-7, aux 1 and 4-8), no
+// solution, for the RK2 predictor state that only the corrector's flux reads.
 cudaError_t ens_c2p_newton(const Member* mem, const Item* items, int n_items, int model,
-                           int guess_mode, int ic, int ipg, int iag, int ip, int ia, int grid,
-                           cudaStream_t st);
+                           int guess_mode, int ic, int ipg, int iag, int ip, int ia, bool lean,
+                           int grid, cudaStream_t st);
 cudaError_t ens_imex_fast(const Member* mem, const Item* items, int n_items, int stage, int grid,
                           cudaStream_t st);
 // ---- guess network (mlp.cu): EA_ZG of the SRMHD members from state `ic`.

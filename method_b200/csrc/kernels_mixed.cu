@@ -129,6 +129,10 @@ struct NewtonTally {
 };
 
 // Mixed-form SRMHD recovery of one cell (Newton in Z, fallbacks).
+// LEAN writes only what FVS::F reads back (prims 1-7; aux 1 and 4-8) and no
+// solution: the recovered RK2 predictor state feeds nothing but the
+// corrector's flux, so the other values would be dead stores.
+template <bool LEAN>
 __device__ __forceinline__ void c2p_srmhd_newton_cell(const Grid& g, long long cell,
                                                       int guess_mode,
                                                       const double* __restrict__ cons,
@@ -171,14 +175,22 @@ __device__ __forceinline__ void c2p_srmhd_newton_cell(const Grid& g, long long c
     if (res.info != 1) tl.bad += 1;
   }
   tl.its += it;
-  solution[cell] = x[0];
-  solution[N + cell] = x[1];
   double p[8], a[13];
   srmhd::from_solution(c, x, g.gamma, R.BS, R.Bsq, R.Ssq, p, a);
+  if constexpr (LEAN) {
 #pragma unroll
-  for (int v = 0; v < 8; ++v) prims[v * N + cell] = p[v];
+    for (int v = 1; v < 8; ++v) prims[v * N + cell] = p[v];
+    aux[N + cell] = a[1];
 #pragma unroll
-  for (int v = 0; v < 13; ++v) aux[v * N + cell] = a[v];
+    for (int v = 4; v < 9; ++v) aux[v * N + cell] = a[v];
+  } else {
+    solution[cell] = x[0];
+    solution[N + cell] = x[1];
+#pragma unroll
+    for (int v = 0; v < 8; ++v) prims[v * N + cell] = p[v];
+#pragma unroll
+    for (int v = 0; v < 13; ++v) aux[v * N + cell] = a[v];
+  }
 }
 
 __device__ __forceinline__ void tally_flush(NewtonTally tl, bool active, long long* counters) {
@@ -208,6 +220,7 @@ __device__ __forceinline__ void tally_flush(NewtonTally tl, bool active, long lo
 // launch, SSP2 512x1024 stages 5-15%.
 constexpr int kNewtonMinBlocks = 8;     // 128 threads x 8 CTAs -> 64 registers
 
+template <bool LEAN>
 __global__ void __launch_bounds__(128, kNewtonMinBlocks)
     k_c2p_newton_srmhd(Grid g, int guess_mode, const double* __restrict__ cons,
                        const double* prims_guess, const double* aux_guess, double* prims,
@@ -218,7 +231,8 @@ __global__ void __launch_bounds__(128, kNewtonMinBlocks)
   if (t < n_interior(g)) {
     int i, j, k;
     interior_ijk(g, t, i, j, k);
-    c2p_srmhd_newton_cell(g, cell_id(g, i, j, k), guess_mode, cons, prims_guess, aux_guess, prims,
+    c2p_srmhd_newton_cell<LEAN>(g, cell_id(g, i, j, k), guess_mode, cons, prims_guess, aux_guess,
+                                prims,
                           aux, solution, zguess, tl);
   }
   tally_flush(tl, t < n_interior(g), w.counters);
@@ -573,7 +587,7 @@ __global__ void __launch_bounds__(32 * TI, (fvs2d_min_blocks<M, float, ORDER, TI
 
 // One model's members per launch (the work list holds one model's cells), so
 // each instantiation carries one recovery method's registers.
-template <int MODEL>
+template <int MODEL, bool LEAN>
 __global__ void __launch_bounds__(128, kNewtonMinBlocks)
     k_ens_c2p_newton(const Member* __restrict__ mem, const Item* __restrict__ items, int n_items,
                      int guess_mode, int ic, int ipg, int iag, int ip, int ia) {
@@ -589,8 +603,8 @@ __global__ void __launch_bounds__(128, kNewtonMinBlocks)
       interior_ijk(g, t, i, j, k);
       const long long cell = cell_id(g, i, j, k);
       if (MODEL == MODEL_SRMHD)
-        c2p_srmhd_newton_cell(g, cell, guess_mode, d.a[ic], d.a[ipg], d.a[iag], d.a[ip],
-                              d.a[ia], d.a[EA_SOL], guess_mode ? d.a[EA_ZG] : nullptr, tl);
+        c2p_srmhd_newton_cell<LEAN>(g, cell, guess_mode, d.a[ic], d.a[ipg], d.a[iag], d.a[ip],
+                                    d.a[ia], d.a[EA_SOL], guess_mode ? d.a[EA_ZG] : nullptr, tl);
       else
         c2p_srrmhd_newton_cell(g, cell, d.a[ic], d.a[iag], d.a[ip], d.a[ia], tl, d.counters);
     }
@@ -697,13 +711,17 @@ cudaError_t ens_fvs_fp32(const Member* mem, const Item* items, int n, int model,
 }
 
 cudaError_t ens_c2p_newton(const Member* mem, const Item* items, int n, int model,
-                           int guess_mode, int ic, int ipg, int iag, int ip, int ia, int grid,
-                           cudaStream_t st) {
-  if (model == MODEL_SRMHD)
-    k_ens_c2p_newton<MODEL_SRMHD><<<grid, 128, 0, st>>>(mem, items, n, guess_mode, ic, ipg, iag,
-                                                        ip, ia);
+                           int guess_mode, int ic, int ipg, int iag, int ip, int ia, bool lean,
+                           int grid, cudaStream_t st) {
+  if (model == MODEL_SRMHD && lean)
+    k_ens_c2p_newton<MODEL_SRMHD, true><<<grid, 128, 0, st>>>(mem, items, n, guess_mode, ic, ipg,
+                                                              iag, ip, ia);
+  else if (model == MODEL_SRMHD)
+    k_ens_c2p_newton<MODEL_SRMHD, false><<<grid, 128, 0, st>>>(mem, items, n, guess_mode, ic, ipg,
+                                                               iag, ip, ia);
   else
-    k_ens_c2p_newton<MODEL_SRRMHD><<<grid, 128, 0, st>>>(mem, items, n, 0, ic, ipg, iag, ip, ia);
+    k_ens_c2p_newton<MODEL_SRRMHD, false><<<grid, 128, 0, st>>>(mem, items, n, 0, ic, ipg, iag, ip,
+                                                                ia);
   return cudaGetLastError();
 }
 
@@ -741,7 +759,7 @@ cudaError_t launch_c2p_batch(long long n, double gamma, int method, int guess,
 cudaError_t launch_c2p_mixed(const Grid& g, int model, int guess, const double* cons,
                              const double* prims_guess, const double* aux_guess, double* prims,
                              double* aux, double* solution, C2PWork w, const MixedWork& mw,
-                             cudaStream_t st) {
+                             bool lean, cudaStream_t st) {
   const long long nI = (long long)(g.ie - g.is) * (g.je - g.js) * (g.ke - g.ks);
   const int blocks = (int)((nI + 127) / 128);
   if (model == MODEL_SRMHD && guess == 1 && mw.has_mlp) {
@@ -750,9 +768,13 @@ cudaError_t launch_c2p_mixed(const Grid& g, int model, int guess, const double* 
     if (e != cudaSuccess) return e;
   }
   if (model == MODEL_SRMHD) {
-    k_c2p_newton_srmhd<<<blocks, 128, 0, st>>>(
-        g, (guess == 1 && mw.has_mlp) ? 1 : 0, cons, prims_guess, aux_guess, prims, aux, solution,
-        w, mw.zguess);
+    const int gm = (guess == 1 && mw.has_mlp) ? 1 : 0;
+    if (lean)
+      k_c2p_newton_srmhd<true><<<blocks, 128, 0, st>>>(g, gm, cons, prims_guess, aux_guess, prims,
+                                                       aux, solution, w, mw.zguess);
+    else
+      k_c2p_newton_srmhd<false><<<blocks, 128, 0, st>>>(g, gm, cons, prims_guess, aux_guess, prims,
+                                                        aux, solution, w, mw.zguess);
   } else {
     k_c2p_newton_srrmhd<<<blocks, 128, 0, st>>>(g, cons, aux_guess, prims, aux, w);
   }
