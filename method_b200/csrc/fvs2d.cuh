@@ -33,8 +33,10 @@ __device__ __forceinline__ R weno_face(const R* p, const R* m, int stride, int b
       return weno3_exact(p[(base + 0) * stride], p[(base + 1) * stride], p[(base + 2) * stride]) +
              weno3_exact(m[(base + 3) * stride], m[(base + 2) * stride], m[(base + 1) * stride]);
     } else {
-      return weno3_fast(p[(base + 0) * stride], p[(base + 1) * stride], p[(base + 2) * stride]) +
-             weno3_fast(m[(base + 3) * stride], m[(base + 2) * stride], m[(base + 1) * stride]);
+      const float2 r = weno3_fast2(make_float2(p[(base + 0) * stride], m[(base + 3) * stride]),
+                                   make_float2(p[(base + 1) * stride], m[(base + 2) * stride]),
+                                   make_float2(p[(base + 2) * stride], m[(base + 1) * stride]));
+      return r.x + r.y;
     }
   } else {
     // upwind cells i-3 .. i+1 ; downwind cells i+2 .. i-2 (weno.cc:175-228)
@@ -44,10 +46,12 @@ __device__ __forceinline__ R weno_face(const R* p, const R* m, int stride, int b
              weno5_exact(m[(base + 5) * stride], m[(base + 4) * stride], m[(base + 3) * stride],
                          m[(base + 2) * stride], m[(base + 1) * stride]);
     } else {
-      return weno5_fast(p[(base + 0) * stride], p[(base + 1) * stride], p[(base + 2) * stride],
-                        p[(base + 3) * stride], p[(base + 4) * stride]) +
-             weno5_fast(m[(base + 5) * stride], m[(base + 4) * stride], m[(base + 3) * stride],
-                        m[(base + 2) * stride], m[(base + 1) * stride]);
+      const float2 r = weno5_fast2(make_float2(p[(base + 0) * stride], m[(base + 5) * stride]),
+                                   make_float2(p[(base + 1) * stride], m[(base + 4) * stride]),
+                                   make_float2(p[(base + 2) * stride], m[(base + 3) * stride]),
+                                   make_float2(p[(base + 3) * stride], m[(base + 2) * stride]),
+                                   make_float2(p[(base + 4) * stride], m[(base + 1) * stride]));
+      return r.x + r.y;
     }
   }
 }
@@ -96,8 +100,16 @@ __device__ __forceinline__ void split_cell(const Grid& g, const double* __restri
   M::template flux<R>(c, p, a, dir, f);
 #pragma unroll
   for (int v = 0; v < M::NC; ++v) {
-    sp[v * stride] = R(0.5) * (f[v] + c[v]);
-    sm[v * stride] = R(0.5) * (f[v] - c[v]);
+    if constexpr (sizeof(R) == 4) {
+      // 0.5 f +- 0.5 c in one FP32x2 FMA: the same values, as halving is exact
+      const float2 h = __ffma2_rn(make_float2(f[v], f[v]), f2(0.5f),
+                                  __fmul2_rn(make_float2(c[v], c[v]), make_float2(0.5f, -0.5f)));
+      sp[v * stride] = h.x;
+      sm[v * stride] = h.y;
+    } else {
+      sp[v * stride] = R(0.5) * (f[v] + c[v]);
+      sm[v * stride] = R(0.5) * (f[v] - c[v]);
+    }
   }
 }
 

@@ -10,8 +10,9 @@
 // function applied to the mirrored stencil (Project/CPU/Src/weno.cc:145-164,
 // 208-228), so only the upwind form exists here.
 //
-// `weno3_fast` / `weno5_fast` are the FP32 forms of the mixed-precision path:
-// the same Jiang-Shu weights, regrouped for FMA and one reciprocal per face.
+// `weno3_fast2` / `weno5_fast2` are the FP32 forms of the mixed-precision
+// path: the same Jiang-Shu weights, regrouped for FMA, with approximate
+// reciprocals, evaluating the upwind and downwind sides of a face together.
 #pragma once
 
 namespace mth {
@@ -78,41 +79,53 @@ __device__ __forceinline__ double weno5_exact(double v0, double v1, double v2, d
   return (w0 * s0 + w1 * s1 + w2 * s2);
 }
 
-// FP32 forms (mixed-precision path).  Same weights, factored smoothness
-// indicators, one reciprocal for the normalisation.
-__device__ __forceinline__ float weno3_fast(float v0, float v1, float v2) {
-  const float eps = 1e-16f;
-  float d0 = v1 - v0, d1 = v2 - v1;
-  float b0 = d0 * d0, b1 = d1 * d1;
-  float a0 = __fdividef(1.0f / 3.0f, fmaf(b0, b0, eps));
-  float a1 = __fdividef(2.0f / 3.0f, fmaf(b1, b1, eps));
-  float s0 = fmaf(1.5f, v1, -0.5f * v0);
-  float s1 = 0.5f * (v2 + v1);
-  float num = fmaf(a0, s0, a1 * s1);
-  return __fdividef(num, a0 + a1);
+// FP32 forms: the upwind (.x) and downwind (.y) reconstructions of one face
+// in FP32x2 arithmetic (sm_100 __ffma2_rn / __fadd2_rn / __fmul2_rn: one
+// instruction for both sides, each lane rounded as the scalar operation);
+// the reciprocals stay scalar.  Linear weights are taken times 3 (WENO3) and
+// times 10 (WENO5), and the WENO5 Jiang-Shu indicators times 4,
+// 13/3 (a - 2b + c)^2 + (.)^2, with eps times 16: none of these scalings
+// changes the normalised weights.
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+
+__device__ __forceinline__ float2 rcp2(float2 q) {
+  return make_float2(__fdividef(1.0f, q.x), __fdividef(1.0f, q.y));
 }
 
-__device__ __forceinline__ float weno5_fast(float v0, float v1, float v2, float v3, float v4) {
-  // Jiang-Shu indicators times 4: 13/3 (a - 2b + c)^2 + (.)^2.  The factor
-  // scales every alpha by 1/16 once eps is scaled by 16, and the linear
-  // weights (0.1, 0.6, 0.3) are taken times 10; neither changes the
-  // normalised weights.
-  const float eps16 = 16e-16f;
-  const float t0 = fmaf(-2.0f, v1, v0) + v2, u0 = fmaf(3.0f, v2, fmaf(-4.0f, v1, v0));
-  const float t1 = fmaf(-2.0f, v2, v1) + v3, u1 = v1 - v3;
-  const float t2 = fmaf(-2.0f, v3, v2) + v4, u2 = fmaf(3.0f, v2, fmaf(-4.0f, v3, v4));
-  const float c13 = 13.0f / 3.0f;
-  const float b0 = fmaf(c13 * t0, t0, u0 * u0);
-  const float b1 = fmaf(c13 * t1, t1, u1 * u1);
-  const float b2 = fmaf(c13 * t2, t2, u2 * u2);
-  const float a0 = __fdividef(1.0f, fmaf(b0, b0, eps16));
-  const float a1 = __fdividef(6.0f, fmaf(b1, b1, eps16));
-  const float a2 = __fdividef(3.0f, fmaf(b2, b2, eps16));
+__device__ __forceinline__ float2 weno3_fast2(float2 v0, float2 v1, float2 v2) {
+  const float2 d0 = __ffma2_rn(f2(-1.0f), v0, v1), d1 = __ffma2_rn(f2(-1.0f), v1, v2);
+  const float2 b0 = __fmul2_rn(d0, d0), b1 = __fmul2_rn(d1, d1);
+  const float2 a0 = rcp2(__ffma2_rn(b0, b0, f2(1e-16f)));
+  const float2 a1 = __fmul2_rn(f2(2.0f), rcp2(__ffma2_rn(b1, b1, f2(1e-16f))));
+  const float2 s0 = __ffma2_rn(f2(1.5f), v1, __fmul2_rn(f2(-0.5f), v0));
+  const float2 s1 = __fmul2_rn(f2(0.5f), __fadd2_rn(v2, v1));
+  const float2 num = __ffma2_rn(a0, s0, __fmul2_rn(a1, s1));
+  return __fmul2_rn(num, rcp2(__fadd2_rn(a0, a1)));
+}
+
+__device__ __forceinline__ float2 weno5_fast2(float2 v0, float2 v1, float2 v2, float2 v3,
+                                              float2 v4) {
+  const float2 t0 = __fadd2_rn(__ffma2_rn(f2(-2.0f), v1, v0), v2);
+  const float2 u0 = __ffma2_rn(f2(3.0f), v2, __ffma2_rn(f2(-4.0f), v1, v0));
+  const float2 t1 = __fadd2_rn(__ffma2_rn(f2(-2.0f), v2, v1), v3);
+  const float2 u1 = __ffma2_rn(f2(-1.0f), v3, v1);
+  const float2 t2 = __fadd2_rn(__ffma2_rn(f2(-2.0f), v3, v2), v4);
+  const float2 u2 = __ffma2_rn(f2(3.0f), v2, __ffma2_rn(f2(-4.0f), v3, v4));
+  const float2 c13 = f2(13.0f / 3.0f);
+  const float2 b0 = __ffma2_rn(__fmul2_rn(c13, t0), t0, __fmul2_rn(u0, u0));
+  const float2 b1 = __ffma2_rn(__fmul2_rn(c13, t1), t1, __fmul2_rn(u1, u1));
+  const float2 b2 = __ffma2_rn(__fmul2_rn(c13, t2), t2, __fmul2_rn(u2, u2));
+  const float2 a0 = rcp2(__ffma2_rn(b0, b0, f2(16e-16f)));
+  const float2 a1 = __fmul2_rn(f2(6.0f), rcp2(__ffma2_rn(b1, b1, f2(16e-16f))));
+  const float2 a2 = __fmul2_rn(f2(3.0f), rcp2(__ffma2_rn(b2, b2, f2(16e-16f))));
   // candidate stencils at the face, the 1/6 folded into the coefficients
-  const float s0 = fmaf(11.0f / 6.0f, v2, fmaf(-7.0f / 6.0f, v1, (1.0f / 3.0f) * v0));
-  const float s1 = fmaf(1.0f / 3.0f, v3, fmaf(5.0f / 6.0f, v2, (-1.0f / 6.0f) * v1));
-  const float s2 = fmaf(-1.0f / 6.0f, v4, fmaf(5.0f / 6.0f, v3, (1.0f / 3.0f) * v2));
-  return __fdividef(fmaf(a0, s0, fmaf(a1, s1, a2 * s2)), a0 + a1 + a2);
+  const float2 c3 = f2(1.0f / 3.0f), c6 = f2(-1.0f / 6.0f), c56 = f2(5.0f / 6.0f);
+  const float2 s0 = __ffma2_rn(f2(11.0f / 6.0f), v2,
+                               __ffma2_rn(f2(-7.0f / 6.0f), v1, __fmul2_rn(c3, v0)));
+  const float2 s1 = __ffma2_rn(c3, v3, __ffma2_rn(c56, v2, __fmul2_rn(c6, v1)));
+  const float2 s2 = __ffma2_rn(c6, v4, __ffma2_rn(c56, v3, __fmul2_rn(c3, v2)));
+  const float2 num = __ffma2_rn(a0, s0, __ffma2_rn(a1, s1, __fmul2_rn(a2, s2)));
+  return __fmul2_rn(num, rcp2(__fadd2_rn(__fadd2_rn(a0, a1), a2)));
 }
 
 }  // namespace mth
