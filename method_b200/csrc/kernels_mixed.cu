@@ -34,41 +34,59 @@ namespace {
 // and g > 0 its right; a Newton step that leaves the bracket (or a zero or
 // negative slope) is replaced by bisection (geometric while the bracket spans
 // decades).  On success Z and vsq hold the root.
+//
+// One division and one reciprocal square root per evaluation: 1/(Z^2 (Z +
+// B^2)^2) also gives 1/Z^2 and 1/Z.
 __device__ __forceinline__ bool srmhd_g(double Z, double D, double tau, double BS2, double Bsq,
                                         double Ssq, double k, double& gv, double& dg,
                                         double& v2) {
   const double Z2 = Z * Z, ZB = Z + Bsq;
-  const double Dn = Z2 * ZB * ZB;
-  v2 = fma(Ssq, Z2, (2 * Z + Bsq) * BS2) / Dn;
+  const double iDn = 1 / (Z2 * ZB * ZB);
+  v2 = fma(Ssq, Z2, (2 * Z + Bsq) * BS2) * iDn;
   if (!(v2 < 1.0)) return false;
+  const double iZ2 = iDn * ZB * ZB, iZ = iZ2 * Z;
   const double om = 1 - v2;
-  const double s = sqrt(om);
+  const double is = rsqrt(om), s = om * is;
   const double p = k * (Z * om - D * s);
-  gv = Z + Bsq - p - 0.5 * Bsq * om - BS2 / (2 * Z2) - D - tau;
-  const double dv2 = (fma(2 * Ssq, Z, 2 * BS2) - v2 * (2 * Z * ZB * (2 * Z + Bsq))) / Dn;
-  const double dp = k * (om - Z * dv2 + D * dv2 / (2 * s));
-  dg = 1 - dp + 0.5 * Bsq * dv2 + BS2 / (Z2 * Z);
+  gv = Z + Bsq - p - 0.5 * Bsq * om - 0.5 * BS2 * iZ2 - D - tau;
+  const double dv2 = (fma(2 * Ssq, Z, 2 * BS2) - v2 * (2 * Z * ZB * (2 * Z + Bsq))) * iDn;
+  const double dp = k * (om - Z * dv2 + 0.5 * D * dv2 * is);
+  dg = 1 - dp + 0.5 * Bsq * dv2 + BS2 * iZ2 * iZ;
   return true;
 }
 
+// The right end of the bracket is searched for only when a step needs it (an
+// unusable guess, v^2 >= 1, a step out of the bracket, a non-positive slope);
+// a Newton run that converges from a good guess never evaluates it.
 __device__ __forceinline__ bool newton_srmhd(double D, double tau, double BS2, double Bsq,
                                              double Ssq, double g, double& Z, double& vsq,
                                              int& iters) {
   const double k = (g - 1) / g;
   double gv, dg, v2;
-  // right end of the bracket: g(Z) ~ (1 - k) Z for large Z
-  double hi = fmax(g * (tau + D + Bsq), 1e-300);
-  for (int q = 0; q < 64; ++q) {
-    if (srmhd_g(hi, D, tau, BS2, Bsq, Ssq, k, gv, dg, v2) && gv > 0) break;
-    hi *= 2;
+  double lo = 0.0, hi = 0.0;
+  bool have_hi = false;
+  auto find_hi = [&]() {
+    if (have_hi) return;
+    // g(Z) ~ (1 - k) Z for large Z
+    hi = fmax(g * (tau + D + Bsq), 1e-300);
+    for (int q = 0; q < 64; ++q) {
+      double gh, dh, vh;
+      if (srmhd_g(hi, D, tau, BS2, Bsq, Ssq, k, gh, dh, vh) && gh > 0) break;
+      hi *= 2;
+    }
+    have_hi = true;
+  };
+  double Zc = Z;
+  if (!(Z > 0 && isfinite(Z))) {
+    find_hi();
+    Zc = 0.5 * hi;
   }
-  double lo = 0.0;
-  double Zc = (Z > 0 && Z < hi && isfinite(Z)) ? Z : 0.5 * hi;
   for (int it = 0; it < 100; ++it) {
     ++iters;
     double Zn;
     if (!srmhd_g(Zc, D, tau, BS2, Bsq, Ssq, k, gv, dg, v2)) {
       lo = Zc;  // v^2 >= 1: left of the root
+      find_hi();
       Zn = lo > 0 ? sqrt(lo * hi) : 0.5 * hi;
     } else {
       if (gv == 0) {
@@ -76,11 +94,19 @@ __device__ __forceinline__ bool newton_srmhd(double D, double tau, double BS2, d
         vsq = v2;
         break;
       }
-      if (gv < 0) lo = Zc; else hi = Zc;
+      if (gv < 0) {
+        lo = Zc;
+      } else {
+        hi = Zc;
+        have_hi = true;
+      }
       Zn = Zc - gv / dg;
-      if (!(dg > 0) || !(Zn > lo && Zn < hi)) Zn = (lo > 0 && hi > 4 * lo) ? sqrt(lo * hi) : 0.5 * (lo + hi);
+      if (!(dg > 0) || !(Zn > lo && (!have_hi || Zn < hi))) {
+        find_hi();
+        Zn = (lo > 0 && hi > 4 * lo) ? sqrt(lo * hi) : 0.5 * (lo + hi);
+      }
     }
-    if (fabs(Zn - Zc) <= 1e-14 * Zn || hi - lo <= 1e-15 * hi) {
+    if (fabs(Zn - Zc) <= 1e-14 * Zn || (have_hi && hi - lo <= 1e-15 * hi)) {
       Zc = Zn;
       if (!srmhd_g(Zc, D, tau, BS2, Bsq, Ssq, k, gv, dg, v2)) return false;
       Z = Zc;
@@ -93,6 +119,40 @@ __device__ __forceinline__ bool newton_srmhd(double D, double tau, double BS2, d
   const double rn = D * sqrt(1 - vsq);
   const double pn = k * (Z * (1 - vsq) - rn);
   return pn >= 0 && rn >= 0;
+}
+
+// Model primitives and aux from a converged (v^2, Z), the quantities of
+// srmhd::from_solution (srmhd.cc:509-560) with reciprocals in place of most
+// divisions: W = 1/sqrt(1 - v^2), rho = D/W, h = Z/(rho W^2) = Z/(D W),
+// e = (h - 1)/gamma, v = (B (B.S) + S Z)/(Z (B^2 + Z)), c_s^2 = (h - 1)(gamma - 1)/h.
+__device__ __forceinline__ void from_solution_fast(const double* c, const double* sol,
+                                                   double gamma, double BS, double Bsq,
+                                                   double Ssq, double* p, double* a) {
+  p[5] = c[5];
+  p[6] = c[6];
+  p[7] = c[7];
+  a[10] = BS;
+  a[11] = Bsq;
+  a[12] = Ssq;
+  const double om = 1 - sol[0];
+  const double W = rsqrt(om), iW = om * W;
+  a[1] = W;
+  p[0] = c[0] * iW;
+  a[0] = sol[1] * iW / c[0];
+  const double ig = 1 / gamma;
+  p[4] = (a[0] - 1) * p[0] * ((gamma - 1) * ig);
+  a[2] = (a[0] - 1) * ig;
+  const double iq = 1 / (sol[1] * (Bsq + sol[1]));
+  p[1] = fma(c[5], BS, c[1] * sol[1]) * iq;
+  p[2] = fma(c[6], BS, c[2] * sol[1]) * iq;
+  p[3] = fma(c[7], BS, c[3] * sol[1]) * iq;
+  a[9] = p[1] * p[1] + p[2] * p[2] + p[3] * p[3];
+  a[3] = sqrt((a[0] - 1) * (gamma - 1) / a[0]);
+  a[4] = W * (c[5] * p[1] + c[6] * p[2] + c[7] * p[3]);
+  a[5] = fma(c[5], iW, a[4] * p[1]);
+  a[6] = fma(c[6], iW, a[4] * p[2]);
+  a[7] = fma(c[7], iW, a[4] * p[3]);
+  a[8] = (Bsq + a[4] * a[4]) * om;
 }
 
 // Newton in Z for SRRMHD's residual (srrmhd.cc:512-537).
@@ -176,7 +236,7 @@ __device__ __forceinline__ void c2p_srmhd_newton_cell(const Grid& g, long long c
   }
   tl.its += it;
   double p[8], a[13];
-  srmhd::from_solution(c, x, g.gamma, R.BS, R.Bsq, R.Ssq, p, a);
+  from_solution_fast(c, x, g.gamma, R.BS, R.Bsq, R.Ssq, p, a);
   if constexpr (LEAN) {
 #pragma unroll
     for (int v = 1; v < 8; ++v) prims[v * N + cell] = p[v];
