@@ -168,10 +168,11 @@ __device__ __forceinline__ bool newton_srrmhd(double Sb2, double D, double tauT,
       Zc = 2 * sqrt(Sb2) + 1e-300;
       continue;
     }
-    const double q = Sb2 / Z2;
-    const double s = sqrt(1 - q);
-    const double r = Zc - k * (Zc - Sb2 / Zc) + (k * s - 1) * D - tauT;
-    const double dr = 1 - k * (1 + q) + k * D * (q / Zc) / s;
+    // one division and one reciprocal square root per step
+    const double iZ = 1 / Zc, Sz = Sb2 * iZ, q = Sz * iZ;
+    const double is = rsqrt(1 - q), s = (1 - q) * is;
+    const double r = Zc - k * (Zc - Sz) + (k * s - 1) * D - tauT;
+    const double dr = 1 - k * (1 + q) + k * D * q * iZ * is;
     double Zn = Zc - r / dr;
     if (!(Zn > 0) || !isfinite(Zn)) Zn = 0.5 * Zc;
     if (fabs(Zn - Zc) <= 1e-13 * Zn) {
@@ -329,17 +330,22 @@ __device__ __forceinline__ void c2p_srrmhd_newton_cell(const Grid& g, long long 
     if (!ok) bad = true;
   }
   tl.its += it;
+  // srrmhd.cc:283-301 with reciprocals: W = 1/sqrt(1 - v^2), rho = D/W,
+  // h = Z/(rho W^2) = Z/(D W), c_s^2 = e gamma (gamma - 1)/h = (h - 1)(gamma - 1)/h
   a[10] = Z;
-  a[9] = a[15] / (a[10] * a[10]);
-  a[1] = 1.0 / sqrt(1 - a[9]);
-  p[0] = c[0] / a[1];
-  a[0] = a[10] / (p[0] * a[1] * a[1]);
+  const double iZ = 1 / Z;
+  a[9] = a[15] * iZ * iZ;
+  const double om = 1 - a[9];
+  a[1] = rsqrt(om);
+  const double iW = om * a[1];
+  p[0] = c[0] * iW;
+  a[0] = Z * iW / c[0];
   a[2] = (a[0] - 1) / gm;
-  a[3] = sqrt((a[2] * gm * (gm - 1)) / a[0]);
+  a[3] = sqrt((a[0] - 1) * (gm - 1) / a[0]);
   p[4] = p[0] * a[2] * (gm - 1);
-  p[1] = a[12] / a[10];
-  p[2] = a[13] / a[10];
-  p[3] = a[14] / a[10];
+  p[1] = a[12] * iZ;
+  p[2] = a[13] * iZ;
+  p[3] = a[14] * iZ;
   a[11] = p[1] * c[8] + p[2] * c[9] + p[3] * c[10];
   const double sg = g.sigma;
   a[4] = c[13] * p[1] + a[1] * sg * (c[8] + (p[2] * c[7] - p[3] * c[6]) - a[11] * p[1]);
@@ -475,11 +481,12 @@ __device__ __forceinline__ bool srrmhd_prims_newton(const double* x, double g, d
   const double Esq = x[8] * x[8] + x[9] * x[9] + x[10] * x[10];
   const double tauB = x[4] - 0.5 * (Bsq + Esq);
   if (!newton_srrmhd(Sbsq, x[0], tauB, g, Z, its)) return false;
-  const double vsq = Sbsq / (Z * Z);
-  W = 1.0 / sqrt(1 - vsq);
-  v[0] = Sb0 / Z;
-  v[1] = Sb1 / Z;
-  v[2] = Sb2 / Z;
+  const double iZ = 1 / Z;
+  const double vsq = Sbsq * iZ * iZ;
+  W = rsqrt(1 - vsq);
+  v[0] = Sb0 * iZ;
+  v[1] = Sb1 * iZ;
+  v[2] = Sb2 * iZ;
   return true;
 }
 
@@ -538,11 +545,12 @@ __device__ __forceinline__ bool imex_fast_form(const Grid& g, long long cell,
     const double beta = a * Ws, alpha = 1 + beta;
     const double vv = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
     const double vR = v[0] * R[0] + v[1] * R[1] + v[2] * R[2];
-    const double f = beta * vR / (alpha * (alpha - beta * vv));
+    const double iA = 1 / alpha;
+    const double f = beta * vR * iA / (alpha - beta * vv);
     double dE[3];
-    dE[0] = -(R[0] / alpha + f * v[0]);
-    dE[1] = -(R[1] / alpha + f * v[1]);
-    dE[2] = -(R[2] / alpha + f * v[2]);
+    dE[0] = -(R[0] * iA + f * v[0]);
+    dE[1] = -(R[1] * iA + f * v[1]);
+    dE[2] = -(R[2] * iA + f * v[2]);
     x[8] += dE[0];
     x[9] += dE[1];
     x[10] += dE[2];
