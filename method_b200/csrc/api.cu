@@ -113,8 +113,9 @@ cudaError_t alloc0(double** p, size_t n, cudaStream_t st) {
 }
 
 // Model::getPrimitiveVars of `cons` into prims/aux, seeded by the guess arrays.
-// `lean`: the result is read only by the fused flux tile (the RK2 predictor
-// state), so the Newton recovery writes the flux inputs alone.
+// `lean`: an intermediate state (RK2 predictor, SSP2 stage) read only by the
+// fused flux tile, the source and the next implicit solve, so the Newton
+// recovery writes their inputs alone.
 cudaError_t c2p_raw(mth_handle* h, const double* cons, const double* pg, const double* ag,
                 double* prims, double* aux, bool lean) {
   if (h->cfg.precision == MTH_MIXED || h->cfg.guess == MTH_GUESS_MLP)
@@ -150,9 +151,9 @@ cudaError_t c2p(mth_handle* h, const double* cons, const double* pg, const doubl
   const bool mixed = h->cfg.precision == MTH_MIXED || h->cfg.guess == MTH_GUESS_MLP;
   const char* name = srmhd ? (mixed ? "c2p_newton_srmhd" : "c2p_hybrd_srmhd")
                            : (mixed ? "c2p_newton_srrmhd" : "c2p_secant_srrmhd");
-  // doubles per cell: 14 read; 23 written (13 by the lean Newton recovery)
-  const bool lean_run = lean && mixed && srmhd && h->fused;
-  return timed(h, name, srmhd ? (lean_run ? 27 : 37) : 43,
+  // doubles per cell: SRMHD 14 read, 23 written (13 lean); SRRMHD 15 read, 28 written (10 lean)
+  const bool lean_run = lean && mixed && h->fused;
+  return timed(h, name, srmhd ? (lean_run ? 27 : 37) : (lean_run ? 25 : 43),
                [&] { return c2p_raw(h, cons, pg, ag, prims, aux, lean); });
 }
 
@@ -251,7 +252,7 @@ cudaError_t enqueue_step(mth_handle* h, double dt) {
                                          h->u1, dt, imex_work(h), h->st);
        })))
     return e;
-  if ((e = c2p(h, h->u1, h->prims, h->aux, h->prims, h->aux))) return e;
+  if ((e = c2p(h, h->u1, h->prims, h->aux, h->prims, h->aux, true))) return e;
   if ((e = timed(h, "source", 31, [&] {
          return launch_source(h->g, h->cfg.model, h->u1, h->aux, h->src1, h->st);
        })))
@@ -264,7 +265,7 @@ cudaError_t enqueue_step(mth_handle* h, double dt) {
                                          h->u2, dt, imex_work(h), h->st);
        })))
     return e;
-  if ((e = c2p(h, h->u2, h->prims, h->aux, h->prims, h->aux))) return e;
+  if ((e = c2p(h, h->u2, h->prims, h->aux, h->prims, h->aux, true))) return e;
   if ((e = timed(h, "source", 31, [&] {
          return launch_source(h->g, h->cfg.model, h->u2, h->aux, h->src2, h->st);
        })))

@@ -176,8 +176,9 @@ cudaError_t flux_phase(mth_ensemble* e, cudaStream_t s, int md, int ic, int ip, 
   return cudaSuccess;
 }
 
-// lean: the recovered state is the RK2 predictor's, which only the
-// corrector's flux reads (mixed form: only the flux inputs are written).
+// lean: an intermediate recovered state (RK2 predictor, SSP2 stage) that only
+// the next flux, source and implicit solve read (mixed form: only their
+// inputs are written).
 cudaError_t c2p_phase(mth_ensemble* e, cudaStream_t s, int md, int ic, int ipg, int iag, int ip,
                       int ia, bool lean = false) {
   const int n = e->n_cells[md];
@@ -231,7 +232,7 @@ cudaError_t srrmhd_ssp2(mth_ensemble* e, cudaStream_t s) {
       return r;
     if ((r = phase(e, s, "imex_queued", [&] { return ens_imex_queued(e->d_mem, e->n, stage, s); })))
       return r;
-    if ((r = c2p_phase(e, s, md, u, EA_PRIMS, EA_AUX, EA_PRIMS, EA_AUX))) return r;
+    if ((r = c2p_phase(e, s, md, u, EA_PRIMS, EA_AUX, EA_PRIMS, EA_AUX, true))) return r;
     if ((r = phase(e, s, "source", [&] {
            return ens_source(e->d_mem, it, n, u, EA_AUX, src, grid, s);
          })))

@@ -61,8 +61,9 @@ cudaError_t ens_fvs_fp32(const Member* mem, const Item* items, int n_items, int 
                          int TI, int ic, int ip, int ia, int iu0, int iout, int mode, int grid,
                          cudaStream_t st);
 // guess_mode 1: SRMHD members start Newton from the learned guess in EA_ZG.
-// lean (SRMHD): write only the flux inputs (prims 1-7, aux 1 and 4-8), no
-// solution, for the RK2 predictor state that only the corrector's flux reads.
+// lean: write only what the stage's flux, source and next implicit solve read
+// (SRMHD: prims 1-7, aux 1 and 4-8, no solution; SRRMHD: prims 1-4, aux 4-8
+// and 10), for the intermediate recovered states of RK2 and SSP2.
 cudaError_t ens_c2p_newton(const Member* mem, const Item* items, int n_items, int model,
                            int guess_mode, int ic, int ipg, int iag, int ip, int ia, bool lean,
                            int grid, cudaStream_t st);

@@ -300,6 +300,10 @@ __global__ void __launch_bounds__(128, kNewtonMinBlocks)
 }
 
 // Mixed-form SRRMHD recovery of one cell (Newton in Z, secant fallback).
+// LEAN writes only what the stage's flux, source and next implicit solve read
+// back (prims 1-4; aux 4-8 and 10): the recovered SSP2 stage states (and the
+// RK2 predictor state) feed nothing else.
+template <bool LEAN>
 __device__ __forceinline__ void c2p_srrmhd_newton_cell(const Grid& g, long long cell,
                                                        const double* __restrict__ cons,
                                                        const double* aux_guess, double* prims,
@@ -354,6 +358,12 @@ __device__ __forceinline__ void c2p_srrmhd_newton_cell(const Grid& g, long long 
   if (bad) {
     tl.bad += 1;
     atomicOr((unsigned long long*)&counters[3], (unsigned long long)ERR_C2P);
+  } else if constexpr (LEAN) {
+#pragma unroll
+    for (int v = 1; v < 5; ++v) prims[v * N + cell] = p[v];
+#pragma unroll
+    for (int v = 4; v < 9; ++v) aux[v * N + cell] = a[v];
+    aux[10 * N + cell] = a[10];
   } else {
 #pragma unroll
     for (int v = 0; v < 11; ++v) prims[v * N + cell] = p[v];
@@ -362,6 +372,7 @@ __device__ __forceinline__ void c2p_srrmhd_newton_cell(const Grid& g, long long 
   }
 }
 
+template <bool LEAN>
 __global__ void __launch_bounds__(128, kNewtonMinBlocks)
     k_c2p_newton_srrmhd(Grid g, const double* __restrict__ cons, const double* aux_guess,
                         double* prims, double* aux, C2PWork w) {
@@ -370,7 +381,8 @@ __global__ void __launch_bounds__(128, kNewtonMinBlocks)
   if (t < n_interior(g)) {
     int i, j, k;
     interior_ijk(g, t, i, j, k);
-    c2p_srrmhd_newton_cell(g, cell_id(g, i, j, k), cons, aux_guess, prims, aux, tl, w.counters);
+    c2p_srrmhd_newton_cell<LEAN>(g, cell_id(g, i, j, k), cons, aux_guess, prims, aux, tl,
+                                 w.counters);
   }
   tally_flush(tl, t < n_interior(g), w.counters);
 }
@@ -674,7 +686,8 @@ __global__ void __launch_bounds__(128, kNewtonMinBlocks)
         c2p_srmhd_newton_cell<LEAN>(g, cell, guess_mode, d.a[ic], d.a[ipg], d.a[iag], d.a[ip],
                                     d.a[ia], d.a[EA_SOL], guess_mode ? d.a[EA_ZG] : nullptr, tl);
       else
-        c2p_srrmhd_newton_cell(g, cell, d.a[ic], d.a[iag], d.a[ip], d.a[ia], tl, d.counters);
+        c2p_srrmhd_newton_cell<LEAN>(g, cell, d.a[ic], d.a[iag], d.a[ip], d.a[ia], tl,
+                                     d.counters);
     }
     tally_flush(tl, act, d.counters);
   }
@@ -787,6 +800,9 @@ cudaError_t ens_c2p_newton(const Member* mem, const Item* items, int n, int mode
   else if (model == MODEL_SRMHD)
     k_ens_c2p_newton<MODEL_SRMHD, false><<<grid, 128, 0, st>>>(mem, items, n, guess_mode, ic, ipg,
                                                                iag, ip, ia);
+  else if (lean)
+    k_ens_c2p_newton<MODEL_SRRMHD, true><<<grid, 128, 0, st>>>(mem, items, n, 0, ic, ipg, iag, ip,
+                                                               ia);
   else
     k_ens_c2p_newton<MODEL_SRRMHD, false><<<grid, 128, 0, st>>>(mem, items, n, 0, ic, ipg, iag, ip,
                                                                 ia);
@@ -844,7 +860,10 @@ cudaError_t launch_c2p_mixed(const Grid& g, int model, int guess, const double* 
       k_c2p_newton_srmhd<false><<<blocks, 128, 0, st>>>(g, gm, cons, prims_guess, aux_guess, prims,
                                                         aux, solution, w, mw.zguess);
   } else {
-    k_c2p_newton_srrmhd<<<blocks, 128, 0, st>>>(g, cons, aux_guess, prims, aux, w);
+    if (lean)
+      k_c2p_newton_srrmhd<true><<<blocks, 128, 0, st>>>(g, cons, aux_guess, prims, aux, w);
+    else
+      k_c2p_newton_srrmhd<false><<<blocks, 128, 0, st>>>(g, cons, aux_guess, prims, aux, w);
   }
   return cudaGetLastError();
 }

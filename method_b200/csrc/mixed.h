@@ -57,8 +57,9 @@ cudaError_t launch_fvs2d_fp32(const Grid& g, int model, int order, const double*
 
 // guess: 0 = previous state, 1 = guess network (falls back to the previous
 // state, then to the reference Powell-hybrid, when Newton does not converge).
-// lean (SRMHD): write only the flux inputs (prims 1-7, aux 1 and 4-8), for a
-// recovered state that only FVS::F reads; `solution` is then left untouched.
+// lean: write only what the flux tile, the source and the next implicit solve
+// read back (SRMHD: prims 1-7, aux 1 and 4-8, no solution; SRRMHD: prims 1-4,
+// aux 4-8 and 10), for an intermediate recovered state.
 cudaError_t launch_c2p_mixed(const Grid& g, int model, int guess, const double* cons,
                              const double* prims_guess, const double* aux_guess, double* prims,
                              double* aux, double* solution, C2PWork w, const MixedWork& mw,
