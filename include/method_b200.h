@@ -129,10 +129,16 @@ mth_status mth_get_stats(mth_handle* h, mth_stats* s);
 mth_status mth_reset_stats(mth_handle* h);
 
 /* Drop-in form of TimeIntegrator::step(cons, prims, aux, dt) (timeInt.h:61)
- * on HOST arrays, the reference's own calling convention: uploads the three
- * arrays, runs one step, downloads them, and returns the step's status.
+ * on HOST arrays, the reference's own calling convention: uploads the
+ * arrays the step reads, runs one step, downloads all three, and returns the
+ * step's status.  The mixed form on 2D grids reads cons and only part of
+ * prims / aux (SRMHD RK2: all prims, aux 0, 1, 4-8; SRRMHD RK2: prims 1-4,
+ * aux 4-8, 10; SRRMHD SSP2: aux 10); every other case uploads all three.
  * Pinned host memory (mth_pin_host) makes the copies asynchronous DMA. */
 mth_status mth_step_host(mth_handle* h, double* cons, double* prims, double* aux, double dt);
+/* Bytes mth_step_host copies to and from the device per call. No reference
+ * counterpart (accounting for the host-array step). */
+mth_status mth_step_host_bytes(mth_handle* h, unsigned long long* h2d, unsigned long long* d2h);
 /* Page-locks / releases a host range for fast copies (cudaHostRegister). */
 mth_status mth_pin_host(void* ptr, unsigned long long bytes);
 mth_status mth_unpin_host(void* ptr);

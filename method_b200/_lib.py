@@ -20,7 +20,8 @@ SYMBOLS = [
     "mth_create", "mth_destroy", "mth_last_error", "mth_get_dims", "mth_set_prims",
     "mth_upload", "mth_download", "mth_apply_bcs", "mth_prims_to_all", "mth_c2p",
     "mth_flux_F", "mth_source", "mth_flux_vector", "mth_c2p_cells", "mth_step", "mth_update_time", "mth_evolve", "mth_sync",
-    "mth_get_stats", "mth_reset_stats", "mth_step_host", "mth_pin_host", "mth_unpin_host",
+    "mth_get_stats", "mth_reset_stats", "mth_step_host", "mth_step_host_bytes", "mth_pin_host",
+    "mth_unpin_host",
     "mth_set_stream", "mth_profile_step", "mth_mlp_train", "mth_mlp_grad", "mth_mlp_forward",
     "mth_mlp_make_pairs", "mth_set_mlp", "mth_c2p_batch", "mth_c2p_ctx_create", "mth_c2p_ctx_destroy",
     "mth_c2p_ctx_set_mlp", "mth_c2p_ctx_run", "mth_c2p_ctx_stats", "mth_c2p_srmhd_noalloc",
@@ -107,6 +108,7 @@ def load():
     L.mth_device_state.argtypes = [H, C.POINTER(D), C.POINTER(D), C.POINTER(D)]
     L.mth_save_text.argtypes = [H, C.c_char_p, C.c_char_p, C.c_int]
     L.mth_step_host.argtypes = [H, D, D, D, C.c_double]
+    L.mth_step_host_bytes.argtypes = [H, C.POINTER(C.c_ulonglong), C.POINTER(C.c_ulonglong)]
     L.mth_pin_host.argtypes = [C.c_void_p, C.c_ulonglong]
     L.mth_unpin_host.argtypes = [C.c_void_p]
     L.mth_set_stream.argtypes = [H, C.c_void_p]

@@ -738,12 +738,66 @@ mth_status mth_unpin_host(void* ptr) {
   return cudaHostUnregister(ptr) == cudaSuccess ? MTH_OK : MTH_ERR_CUDA;
 }
 
+// Variables of the input prims / aux that one step reads (bit v = variable
+// v).  Mixed form on the fused 2D path: the flux tile reads prims 1-7 and aux
+// 1, 4-8 (SRMHD) or prims 1-4 and aux 4-8, 10 (SRRMHD); the Newton recoveries
+// seed from prims 0-3 and aux 0 (SRMHD) or aux 10 (SRRMHD); SSP2 reads only
+// aux 10, its stage recoveries supplying the rest.  Everything else (the
+// plain form's retry reads aux 10-12 of failed cells, the generic path reads
+// whole arrays) is uploaded whole.
+static void step_inputs(const mth_handle* h, unsigned& pmask, unsigned& amask) {
+  pmask = (1u << h->NP) - 1;
+  amask = (1u << h->NA) - 1;
+  if (!h->fused || h->cfg.precision != MTH_MIXED) return;
+  const int integ = h->cfg.integrator;
+  const bool rk = integ == MTH_RK2 || integ == MTH_RKSPLIT;
+  if (h->cfg.model == MTH_SRMHD && rk) {
+    amask = 0x1F3u;  // aux 0, 1, 4-8
+  } else if (h->cfg.model == MTH_SRRMHD && rk) {
+    pmask = 0x1Eu;   // prims 1-4
+    amask = 0x5F0u;  // aux 4-8, 10
+  } else if (h->cfg.model == MTH_SRRMHD && integ == MTH_SSP2) {
+    pmask = 0u;
+    amask = 1u << 10;
+  }
+}
+
+// Uploads the variables of `mask`, one copy per run of consecutive variables.
+static cudaError_t upload_vars(mth_handle* h, double* dst, const double* src, unsigned mask,
+                               int nv) {
+  const size_t per = bytes(h, 1) / sizeof(double);
+  for (int v = 0; v < nv;) {
+    if (!(mask >> v & 1u)) {
+      ++v;
+      continue;
+    }
+    int e = v;
+    while (e < nv && (mask >> e & 1u)) ++e;
+    cudaError_t r = cudaMemcpyAsync(dst + v * per, src + v * per, bytes(h, e - v),
+                                    cudaMemcpyHostToDevice, h->st);
+    if (r != cudaSuccess) return r;
+    v = e;
+  }
+  return cudaSuccess;
+}
+
+mth_status mth_step_host_bytes(mth_handle* h, unsigned long long* h2d, unsigned long long* d2h) {
+  if (!h || !h2d || !d2h) return MTH_ERR_INVALID;
+  unsigned pm, am;
+  step_inputs(h, pm, am);
+  *h2d = bytes(h, h->NC + __builtin_popcount(pm) + __builtin_popcount(am));
+  *d2h = bytes(h, h->NC + h->NP + h->NA);
+  return MTH_OK;
+}
+
 mth_status mth_step_host(mth_handle* h, double* cons, double* prims, double* aux, double dt) {
   if (!h || !cons || !prims || !aux || !(dt > 0)) return MTH_ERR_INVALID;
   CU(h, cudaSetDevice(h->device));
+  unsigned pm, am;
+  step_inputs(h, pm, am);
   CU(h, cudaMemcpyAsync(h->cons, cons, bytes(h, h->NC), cudaMemcpyHostToDevice, h->st));
-  CU(h, cudaMemcpyAsync(h->prims, prims, bytes(h, h->NP), cudaMemcpyHostToDevice, h->st));
-  CU(h, cudaMemcpyAsync(h->aux, aux, bytes(h, h->NA), cudaMemcpyHostToDevice, h->st));
+  CU(h, upload_vars(h, h->prims, prims, pm, h->NP));
+  CU(h, upload_vars(h, h->aux, aux, am, h->NA));
   h->dt = dt;
   mth_status s = launch_step(h, dt);
   if (s != MTH_OK) return s;
