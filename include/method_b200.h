@@ -235,23 +235,28 @@ mth_status mth_c2p_ctx_stats(mth_c2p_ctx* c, void* stream, mth_c2p_batch_stats* 
  * application that owns all device memory through its own fixed pool, or a
  * latency-critical loop that cannot afford cudaMalloc and the synchronisation
  * it may bring.  No counterpart in the reference (its C2P is a host method).
- * All pointers are device arrays in the reference layout for a grid of
- * nx x ny x nz interior cells with Ng ghosts (ny = 0: 1D, nz = 0: 2D):
- * cons (9 vars), prims_guess / aux_guess (the previous state, 8 / 13 vars),
- * prims / aux (8 / 13 vars, out; may alias the guesses), solution (2 vars,
- * in/out, the per-cell (v^2, rho h W^2) the retry averages; keep it across
- * calls as the reference's SRMHD::solution).  Work is enqueued on `stream`
- * (a cudaStream_t, NULL = default stream) of the calling thread's current
- * device; the call allocates nothing.  The failure queue and counters live in
- * one fixed device array (about 4 MiB per GPU, held until exit) shared by all
- * calls: calls that overlap on the GPU race on it, so order them on one
- * stream.  The first call on each device looks up that array's address;
- * make it before any stream capture.  Returns MTH_ERR_INVALID, with a message
- * on stderr, when the grid has more than MTH_NOALLOC_MAX_CELLS interior cells. */
+ * All pointers but `unconverged` are device arrays in the reference layout
+ * for a grid of nx x ny x nz interior cells with Ng ghosts (ny = 0: 1D,
+ * nz = 0: 2D): cons (9 vars), prims_guess / aux_guess (the previous state,
+ * 8 / 13 vars), prims / aux (8 / 13 vars, out; may alias the guesses),
+ * solution (2 vars, in/out, the per-cell (v^2, rho h W^2) the retry averages,
+ * ghost cells included; keep it across calls as the reference's
+ * SRMHD::solution).  Work is enqueued on `stream` (a cudaStream_t, NULL =
+ * default stream) of the calling thread's current context; the call
+ * allocates nothing.  The failure queue and counters live in one fixed device
+ * array (about 4 MiB per GPU, held until exit) shared by all calls: calls
+ * that overlap on the GPU race on it, so order them on one stream.  Its
+ * address is looked up once per CUDA context, by the first call made in that
+ * context; make that call before any stream capture.  `unconverged` (host
+ * memory, may be NULL): when given, the call waits for the stream and stores
+ * the number of cells the retry left unconverged (the reference only prints
+ * these, srmhd.cc:495-498; the status stays MTH_OK, as for mth_c2p).  Returns
+ * MTH_ERR_INVALID, with a message on stderr, when the grid has more than
+ * MTH_NOALLOC_MAX_CELLS interior cells or cell ids that overflow an int. */
 mth_status mth_c2p_srmhd_noalloc(int nx, int ny, int nz, int Ng, double gamma,
                                  const double* cons, const double* prims_guess,
                                  const double* aux_guess, double* prims, double* aux,
-                                 double* solution, void* stream);
+                                 double* solution, void* stream, long long* unconverged);
 
 /* SerialSaveData output (serialSaveData.cc:31-246) of the current state:
  * `which` is a mask of MTH_SAVE_* bits; files are

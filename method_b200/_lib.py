@@ -130,7 +130,8 @@ def load():
     L.mth_c2p_ctx_stats.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C2PBatchStats)]
     L.mth_c2p_srmhd_noalloc.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
                                          C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
-                                         C.c_void_p, C.c_void_p, C.c_void_p]
+                                         C.c_void_p, C.c_void_p, C.c_void_p,
+                                         C.POINTER(C.c_longlong)]
     E = C.c_void_p
     L.mth_ensemble_create.argtypes = [C.POINTER(Config), C.c_int, C.POINTER(E)]
     L.mth_ensemble_destroy.argtypes = [E]

@@ -337,6 +337,11 @@ mth_status read_status(mth_handle* h) {
   long long cnt[16];
   CU(h, cudaMemcpy(cnt, h->counters, sizeof cnt, cudaMemcpyDeviceToHost));
   long long flags = cnt[3] | cnt[7];
+  if (flags) {  // the error words are sticky until read here; the counts stay
+    CU(h, cudaMemsetAsync(h->counters + 3, 0, sizeof(long long), h->st));
+    CU(h, cudaMemsetAsync(h->counters + 7, 0, sizeof(long long), h->st));
+    CU(h, cudaStreamSynchronize(h->st));
+  }
   if (flags & ERR_IMPLICIT)
     return fail(h, MTH_ERR_IMPLICIT,
                 "IMEX time integrator could not converge to a solution (implicit stage)");

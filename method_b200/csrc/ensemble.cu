@@ -575,7 +575,12 @@ mth_status mth_ensemble_sync(mth_ensemble* e) {
     long long c[16];
     ECU(e, cudaMemcpy(c, e->mem[m].counters, sizeof c, cudaMemcpyDeviceToHost));
     flags |= c[3] | c[7];
+    if (c[3] | c[7]) {  // sticky until read here; the counts stay
+      ECU(e, cudaMemsetAsync(e->mem[m].counters + 3, 0, sizeof(long long), e->st));
+      ECU(e, cudaMemsetAsync(e->mem[m].counters + 7, 0, sizeof(long long), e->st));
+    }
   }
+  ECU(e, cudaStreamSynchronize(e->st));
   if (flags & ERR_IMPLICIT) return efail(e, MTH_ERR_IMPLICIT, "implicit stage did not converge");
   if (flags & ERR_C2P) return efail(e, MTH_ERR_C2P, "C2P could not converge.");
   return MTH_OK;

@@ -55,6 +55,7 @@ typedef struct {
   double *solution;                                   /* SRMHD C2P */
   double *fplus, *fminus, *fprec, *fmrec, *fx, *fy, *fz, *source;
   int failed; /* 1 C2P, 2 implicit */
+  int c2p_unconverged; /* SRMHD C2P: cells the last call's retry left unconverged */
 } orc_sim;
 
 #define IDX(s, v, i, j, k) ((size_t)(v) * (s)->Ntot + ((size_t)(i) * (s)->Ny + (j)) * (s)->Nz + (k))
@@ -516,6 +517,7 @@ static void srmhd_c2p(orc_sim* s, double* cons, double* prims, double* aux) {
   int* fails = NULL;
   int nf = 0, cap = 0;
   memset(&args, 0, sizeof args);
+  s->c2p_unconverged = 0;
   for (int i = s->is; i < s->ie; i++)
     for (int j = s->js; j < s->je; j++)
       for (int k = s->ks; k < s->ke; k++) {
@@ -551,7 +553,7 @@ static void srmhd_c2p(orc_sim* s, double* cons, double* prims, double* aux) {
     }
     sol[0] /= (double)cnt;
     sol[1] /= (double)cnt;
-    orc_hybrd1(srmhd_residual, &args, 2, sol, res, tol, NULL);
+    if (orc_hybrd1(srmhd_residual, &args, 2, sol, res, tol, NULL) != 1) s->c2p_unconverged++;
     s->solution[IDX(s, 0, x, y, z)] = sol[0];
     s->solution[IDX(s, 1, x, y, z)] = sol[1];
   }
@@ -872,6 +874,17 @@ int orc_c2p(void* h, double* cons, double* prims, double* aux) {
   orc_sim* s = (orc_sim*)h;
   if (s->NC == 9) { srmhd_c2p(s, cons, prims, aux); return 0; }
   return srrmhd_c2p(s, cons, prims, aux);
+}
+
+/* SRMHD::solution (2 x Ntot, per cell (v^2, rho h W^2)): copied out into
+ * `get` and/or replaced by `set` (either may be NULL).  Returns the number of
+ * cells the last SRMHD C2P's neighbour-average retry left unconverged (the
+ * reference prints these, srmhd.cc:495-498). */
+int orc_srmhd_solution(void* h, double* get, const double* set) {
+  orc_sim* s = (orc_sim*)h;
+  if (get) memcpy(get, s->solution, (size_t)2 * s->Ntot * 8);
+  if (set) memcpy(s->solution, set, (size_t)2 * s->Ntot * 8);
+  return s->c2p_unconverged;
 }
 
 void orc_prims_to_all(void* h, double* cons, double* prims, double* aux) {

@@ -67,6 +67,7 @@ def lib():
     L.orc_weno5_upwind.restype = C.c_double
     L.orc_weno5_upwind.argtypes = [C.c_double] * 5
     L.orc_hybrd1_kat.argtypes = [C.c_int, C.c_int, D, D, C.c_double, C.c_int]
+    L.orc_srmhd_solution.argtypes = [P, D, D]
     L.orc_srmhd_c2p_cells.argtypes = [C.c_int, C.c_double, C.c_double, D, D, D, I, I]
     _LIB = L
     return L
@@ -150,6 +151,15 @@ class PortSim:
 
     def c2p(self, cons, prims, aux):
         return self.L.orc_c2p(self.h, _ptr(cons), _ptr(prims), _ptr(aux))
+
+    def solution(self, new=None):
+        """SRMHD::solution as (2, Nx, Ny, Nz), replaced by `new` when given, and the
+        number of cells the last C2P's retry left unconverged."""
+        got = np.zeros((2, self.Nx, self.Ny, self.Nz), dtype=np.float64)
+        if new is not None:
+            new = np.ascontiguousarray(new, dtype=np.float64)
+        still = self.L.orc_srmhd_solution(self.h, _ptr(got), _ptr(new))
+        return got, still
 
     def prims_to_all(self, cons, prims, aux):
         self.L.orc_prims_to_all(self.h, _ptr(cons), _ptr(prims), _ptr(aux))

@@ -168,3 +168,44 @@ def test_ensemble_256_members_sampled_against_single_runs():
             assert np.array_equal(a, b), (m, name)
         s.close()
     ens.close()
+
+
+def test_ot1024_50_steps_match_reference(ref):
+    """The measured configuration for its first 50 updateTime calls (slow start
+    included), against the reference build's OpenMP form (its threads split
+    the WENO/FVS loops only; the arithmetic is the serial build's)."""
+    import method_b200 as mb
+    if not ref.available(omp=True):
+        pytest.skip("OpenMP reference build missing")
+    n, steps = 1024, 50
+    p0 = initial.orszag_tang(n, Ng=4)
+    g = mb.Simulation(nx=n, ny=n, **OT)
+    g.set_prims(p0)
+    g.update_time(steps)
+    r = ref.RefSim(prims=p0, omp=True, nx=n, ny=n, **OT)
+    assert r.update_time(steps) == 0
+    assert g.stats()["iters"] == r.iters == steps
+    for name, a, b in zip(("cons", "prims", "aux"), g.state(), r.state()):
+        assert np.array_equal(a, b), name
+
+
+@pytest.mark.parametrize("seed", [3, 0, 10])
+def test_sheet64x128_ssp2_matches_reference_at_seeded_sigma(ref, seed):
+    """The resistive current-sheet workload at reduced size (64x128), IMEX
+    SSP2, 10 updateTime calls, conductivity drawn per run as 10^U(1, 5) from
+    the seed (seeds 3, 0, 10: sigma 22, 3.5e3, 6.7e4)."""
+    import method_b200 as mb
+    sigma = initial.sigma_for_seed(seed)
+    cfg = dict(model="srrmhd", nx=64, ny=128, xmin=-0.5, xmax=0.5, ymin=-1.0, ymax=1.0,
+               endTime=3.0, cfl=0.4, Ng=4, gamma=4.0 / 3.0, sigma=sigma, weno=3,
+               bcs="outflow", integrator="ssp2")
+    p0 = initial.current_sheet(64, 128, seed=seed)
+    g = mb.Simulation(**cfg)
+    g.set_prims(p0)
+    g.update_time(10)
+    st = g.stats()
+    assert st["status"] == 0 and st["implicit_failed"] == 0
+    r = ref.RefSim(prims=p0, **cfg)
+    assert r.update_time(10) == 0
+    for name, a, b in zip(("cons", "prims", "aux"), g.state(), r.state()):
+        assert np.array_equal(a, b), (name, sigma)
