@@ -50,6 +50,8 @@ typedef struct {
   int precision;             /* MTH_PLAIN_FP64 / MTH_MIXED */
   int guess;                 /* MTH_GUESS_PREVIOUS / MTH_GUESS_MLP */
   int device;                /* CUDA device ordinal */
+  int functional_sigma;      /* Data::functionalSigma: conductivity sigma * D^sigma_exp */
+  double sigma_exp;          /* Data::gam (simData.h:86; the reference's default is 12) */
 } mth_config;
 
 typedef struct {

@@ -54,6 +54,7 @@ class Config(C.Structure):
         ("gamma", C.c_double), ("sigma", C.c_double), ("cp", C.c_double),
         ("weno_order", C.c_int), ("bcs", C.c_int), ("integrator", C.c_int),
         ("precision", C.c_int), ("guess", C.c_int), ("device", C.c_int),
+        ("functional_sigma", C.c_int), ("sigma_exp", C.c_double),
     ]
 
 

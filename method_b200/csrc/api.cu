@@ -395,6 +395,8 @@ bool grid_from_config(const void* cfg, Grid* out) {
   g.dz = (zmax - zmin) / (c.nz);
   g.gamma = c.gamma;
   g.sigma = c.sigma;
+  g.functional_sigma = c.functional_sigma ? 1 : 0;
+  g.sigma_exp = c.sigma_exp;
   g.cp = c.cp;
   g.Ntot = (long long)g.Nx * g.Ny * g.Nz;
   return true;

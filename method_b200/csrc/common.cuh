@@ -34,7 +34,19 @@ struct Grid {
   double dx, dy, dz;
   double gamma, sigma, cp;
   long long Ntot;        // Nx*Ny*Nz
+  double sigma_exp;      // Data::gam, exponent of a functional conductivity
+  int functional_sigma;  // Data::functionalSigma
 };
+
+// Data::sigmaFunc (simData.cc:114-127): the conductivity of a cell whose
+// conserved density is D -- sigma, or sigma * D^gam when it is functional.
+__host__ __device__ inline double sigma_of(double sigma, double sigma_exp, int functional,
+                                           double D) {
+  return functional ? sigma * pow(D, sigma_exp) : sigma;
+}
+__host__ __device__ inline double sigma_of(const Grid& g, double D) {
+  return sigma_of(g.sigma, g.sigma_exp, g.functional_sigma, D);
+}
 
 __host__ __device__ inline long long cell_id(const Grid& g, int i, int j, int k) {
   return ((long long)i * g.Ny + j) * g.Nz + k;

@@ -365,7 +365,7 @@ __global__ void k_prims_to_all_srrmhd(Grid g, const double* __restrict__ prims,
   } else {
     qfd = false;
   }
-  srrmhd::prims_to_all(p, g.gamma, g.sigma, qfd, divE, c, a);
+  srrmhd::prims_to_all(p, g.gamma, g.sigma, g.sigma_exp, g.functional_sigma, qfd, divE, c, a);
 #pragma unroll
   for (int v = 0; v < 14; ++v) cons[v * N + cell] = c[v];
 #pragma unroll
@@ -388,7 +388,7 @@ __global__ void __launch_bounds__(128)
     for (int v = 0; v < 14; ++v) c[v] = cons[v * N + cell];
     a[10] = aux_guess[10 * N + cell];
     int ev = 0;
-    bool ok = srrmhd::c2p_cell(c, g.gamma, g.sigma, p, a, ev);
+    bool ok = srrmhd::c2p_cell(c, g.gamma, sigma_of(g, c[0]), p, a, ev);
     evals = ev;
     if (ok) {
 #pragma unroll
@@ -492,6 +492,8 @@ __device__ __forceinline__ long long imex_cell(const Grid& g, long long cell,
   R.om2gam = kImexOm2Gam;
   R.g = g.gamma;
   R.sigma = g.sigma;
+  R.sigma_exp = g.sigma_exp;
+  R.functional = g.functional_sigma;
   R.cp = g.cp;
   R.Z = aux_guess[10 * N + cell];
   R.stage = STAGE;
@@ -591,6 +593,8 @@ __device__ __forceinline__ long long imex_sweep_cell(
   R.hmgam = kImexHmGam;
   R.g = g.gamma;
   R.sigma = g.sigma;
+  R.sigma_exp = g.sigma_exp;
+  R.functional = g.functional_sigma;
   R.cp = g.cp;
   R.Z = zaux[10 * N + cell];
   R.stage = FORM;

@@ -351,7 +351,7 @@ __device__ __forceinline__ void c2p_srrmhd_newton_cell(const Grid& g, long long 
   p[2] = a[13] * iZ;
   p[3] = a[14] * iZ;
   a[11] = p[1] * c[8] + p[2] * c[9] + p[3] * c[10];
-  const double sg = g.sigma;
+  const double sg = sigma_of(g, c[0]);
   a[4] = c[13] * p[1] + a[1] * sg * (c[8] + (p[2] * c[7] - p[3] * c[6]) - a[11] * p[1]);
   a[5] = c[13] * p[2] + a[1] * sg * (c[9] + (p[3] * c[5] - p[1] * c[7]) - a[11] * p[2]);
   a[6] = c[13] * p[3] + a[1] * sg * (c[10] + (p[1] * c[6] - p[2] * c[5]) - a[11] * p[3]);
@@ -535,7 +535,8 @@ __device__ __forceinline__ bool imex_fast_form(const Grid& g, long long cell,
     else c[v] = u - dt * (flux2[o] - 0.5 * source2[o]);
     x[v] = c[v];
   }
-  const double a = FORM <= 3 ? dt * kGam : 0.5 * dt, cp2 = g.cp * g.cp, sg = g.sigma;
+  // D has no source: x[0] = c[0] throughout, so the conductivity is fixed per cell
+  const double a = FORM <= 3 ? dt * kGam : 0.5 * dt, cp2 = g.cp * g.cp, sg = sigma_of(g, c[0]);
   x[12] = c[12] / (1 + a / cp2);
   x[11] = (c[11] + a * c[13]) / (1 + a / cp2);
   double Z = aux_guess[10 * N + cell];

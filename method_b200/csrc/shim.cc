@@ -71,13 +71,16 @@ Data::Data(int nx, int ny, int nz, double xmin, double xmax, double ymin, double
     throw std::invalid_argument(
         "Species 1 must have negative charge, mu1 < 0, and species 2 must have positive charge, "
         "mu2 > 0.\n");
-  if (functionalSigma)
-    throw std::invalid_argument("METHOD-B200 supports the constant conductivity sigma only");
 }
 
 Data::~Data() { invalidateGpu(); }
 
-double Data::sigmaFunc(double*, double*, double*, int, int, int) { return sigma; }
+// Data::sigmaFunc (simData.cc:114-127).
+double Data::sigmaFunc(double* cons, double*, double*, int i, int j, int k) {
+  if (!functionalSigma) return sigma;
+  if (i < 0 || j < 0 || k < 0) return sigma * pow(cons[0], gam);
+  return sigma * pow(cons[id(0, i, j, k)], gam);
+}
 
 void Data::invalidateGpu() {
   if (gpu_) mth_destroy(gpu_);
@@ -110,6 +113,8 @@ mth_handle* Data::gpu() {
   c.precision = precision;
   c.guess = guess;
   c.device = device;
+  c.functional_sigma = functionalSigma ? 1 : 0;
+  c.sigma_exp = gam;
   mth_status s = mth_create(&c, &gpu_);
   if (s != MTH_OK) {
     gpu_ = nullptr;
@@ -206,8 +211,8 @@ void SRMHD::getPrimitiveVarsSingleCell(double* cons, double* prims, double* aux,
   throw_status(s, nullptr, "getPrimitiveVarsSingleCell");
 }
 void SRRMHD::getPrimitiveVarsSingleCell(double* cons, double* prims, double* aux, int, int, int) {
-  mth_status s = mth_c2p_cells(MTH_SRRMHD, data->gamma, data->sigma, 1, cons, prims, aux, 0.0,
-                               data->device);
+  mth_status s = mth_c2p_cells(MTH_SRRMHD, data->gamma, data->sigmaFunc(cons, prims, aux), 1,
+                               cons, prims, aux, 0.0, data->device);
   if (s == MTH_ERR_C2P) throw std::runtime_error("C2P could not converge.\n");
   throw_status(s, nullptr, "getPrimitiveVarsSingleCell");
 }

@@ -157,7 +157,8 @@ __device__ __forceinline__ bool c2p_cell(const double* c, double g, double sigma
 // Per-cell part of SRRMHD::primsToAll (srrmhd.cc:358-510).  `qfd` tells
 // whether the 4th-order charge-density stencil applies at this cell and
 // `divE` is its value.
-__device__ __forceinline__ void prims_to_all(const double* p, double g, double sigma, bool qfd,
+__device__ __forceinline__ void prims_to_all(const double* p, double g, double sigma0,
+                                             double sigma_exp, int functional, bool qfd,
                                              double divE, double* c, double* a) {
   c[11] = c[12] = 0.0;
   c[5] = p[5]; c[6] = p[6]; c[7] = p[7];
@@ -172,6 +173,7 @@ __device__ __forceinline__ void prims_to_all(const double* p, double g, double s
   a[0] = 1 + a[2] * g;
   a[3] = sqrt((a[2] * g * (g - 1)) / a[0]);
   a[10] = p[0] * a[0] * a[1] * a[1];
+  const double sigma = sigma_of(sigma0, sigma_exp, functional, c[0]);  // srrmhd.cc:410
   if (qfd) {
     c[13] = divE;
     a[4] = c[13] * p[1] + a[1] * sigma * (c[8] + p[2] * c[7] - p[3] * c[6] - a[11] * p[1]);
@@ -205,13 +207,15 @@ struct ImexResidual {
   const double* flux2;    // forms 3, 6
   const double* source2;  // form 6
   double dt, gam, om2gam, hmgam, g, sigma, cp;
+  double sigma_exp;  // functional conductivity sigma * D^sigma_exp when `functional`
+  int functional;
   double Z;
   int stage;
   int evals;
   __device__ __forceinline__ void operator()(const double* x, double* fv) {
     double p[NP], a[NA], s[NC];
     a[10] = Z;
-    bool ok = c2p_cell(x, g, sigma, p, a, evals);
+    bool ok = c2p_cell(x, g, sigma_of(sigma, sigma_exp, functional, x[0]), p, a, evals);
     Z = a[10];
     if (!ok) {
 #pragma unroll

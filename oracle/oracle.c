@@ -40,7 +40,14 @@ typedef struct {
   int weno;       /* 3 or 5 */
   int bcs;        /* 0 outflow, 1 periodic, 2 flow */
   int integrator; /* 0 RK2, 1 RKSplit, 2 SSP2, 3 SSP3, 4 SSP2322 */
+  int functional_sigma; /* Data::functionalSigma */
+  double sigma_exp;     /* Data::gam */
 } orc_config;
+
+/* Data::sigmaFunc (simData.cc:114-127) of a cell whose density is D. */
+static double sigma_func(const orc_config* c, double D) {
+  return c->functional_sigma ? c->sigma * pow(D, c->sigma_exp) : c->sigma;
+}
 
 typedef struct {
   orc_config c;
@@ -699,7 +706,7 @@ static int srrmhd_c2p(orc_sim* s, double* cons, double* prims, double* aux) {
       for (int k = s->ks; k < s->ke; k++) {
         for (int v = 0; v < 14; v++) c[v] = C(v);
         a[10] = A(10);
-        if (!srrmhd_c2p_cell(c, s->c.gamma, s->c.sigma, p, a)) return 1;
+        if (!srrmhd_c2p_cell(c, s->c.gamma, sigma_func(&s->c, c[0]), p, a)) return 1;
         for (int v = 0; v < 11; v++) P(v) = p[v];
         for (int v = 0; v < 17; v++) A(v) = a[v];
       }
@@ -707,7 +714,7 @@ static int srrmhd_c2p(orc_sim* s, double* cons, double* prims, double* aux) {
 }
 
 static void srrmhd_prims_to_all(orc_sim* s, double* cons, double* prims, double* aux) {
-  double g = s->c.gamma, sg = s->c.sigma, dx = s->dx, dy = s->dy, dz = s->dz;
+  double g = s->c.gamma, sg, dx = s->dx, dy = s->dy, dz = s->dz;
 #define PN(v, a, b, cc) prims[IDX(s, v, a, b, cc)]
   for (int i = 0; i < s->Nx; i++)
     for (int j = 0; j < s->Ny; j++)
@@ -726,6 +733,7 @@ static void srrmhd_prims_to_all(orc_sim* s, double* cons, double* prims, double*
         A(0) = 1 + A(2) * g;
         A(3) = sqrt((A(2) * g * (g - 1)) / A(0));
         A(10) = P(0) * A(0) * A(1) * A(1);
+        sg = sigma_func(&s->c, C(0)); /* srrmhd.cc:410, after D is set */
         if (i > 1 && j > 1 && k > 1 && i < s->Nx - 2 && j < s->Ny - 2 && k < s->Nz - 2) {
           C(13) = (-PN(8, i + 2, j, k) + 8 * PN(8, i + 1, j, k) - 8 * PN(8, i - 1, j, k) + PN(8, i - 2, j, k)) / (12 * dx) +
                   (-PN(9, i, j + 2, k) + 8 * PN(9, i, j + 1, k) - 8 * PN(9, i, j - 1, k) + PN(9, i, j - 2, k)) / (12 * dy) +
@@ -971,6 +979,7 @@ static int rksplit_step(orc_sim* s, double dt) {
 typedef struct {
   double cons[14], aux10, flux1[14], source1[14], flux2[14], source2[14], dt, g, sigma, cp;
   int stage;
+  const orc_config* cfg; /* for a functional conductivity */
 } imex_ctx;
 
 static void imex_residual(void* ctx, int n, const double* x, double* fvec) {
@@ -981,7 +990,7 @@ static void imex_residual(void* ctx, int n, const double* x, double* fvec) {
   const double gam = 0.2928932188134525, om2gam = 0.4142135623730950;
   double p[11], ax[17], src[14];
   ax[10] = a->aux10;
-  int ok = srrmhd_c2p_cell(x, a->g, a->sigma, p, ax);
+  int ok = srrmhd_c2p_cell(x, a->g, sigma_func(a->cfg, x[0]), p, ax);
   a->aux10 = ax[10];
   if (!ok) { for (int i = 0; i < n; i++) fvec[i] = 1.0e6; return; }
   srrmhd_source_cell(x, ax, a->cp, src);
@@ -1023,7 +1032,7 @@ static int imex_stage_sweep(orc_sim* s, int kind, int xform, double dt, double t
                             const double* zaux, double* out) {
   imex_ctx ctx;
   double x[14], fvec[14];
-  ctx.dt = dt; ctx.g = s->c.gamma; ctx.sigma = s->c.sigma; ctx.cp = s->c.cp;
+  ctx.dt = dt; ctx.g = s->c.gamma; ctx.sigma = s->c.sigma; ctx.cp = s->c.cp; ctx.cfg = &s->c;
   ctx.stage = kind;
   for (int i = s->is; i < s->ie; i++)
     for (int j = s->js; j < s->je; j++)
@@ -1115,7 +1124,7 @@ static int ssp2_step(orc_sim* s, double dt) {
   const double tol = 0.000000149011612;
   imex_ctx ctx;
   double x[14], fvec[14];
-  ctx.dt = dt; ctx.g = s->c.gamma; ctx.sigma = s->c.sigma; ctx.cp = s->c.cp;
+  ctx.dt = dt; ctx.g = s->c.gamma; ctx.sigma = s->c.sigma; ctx.cp = s->c.cp; ctx.cfg = &s->c;
   ctx.stage = 1;
   for (int i = s->is; i < s->ie; i++)
     for (int j = s->js; j < s->je; j++)

@@ -29,6 +29,7 @@ class PortConfig(C.Structure):
         ("endTime", C.c_double), ("cfl", C.c_double), ("Ng", C.c_int),
         ("gamma", C.c_double), ("sigma", C.c_double), ("cp", C.c_double),
         ("weno", C.c_int), ("bcs", C.c_int), ("integrator", C.c_int),
+        ("functional_sigma", C.c_int), ("sigma_exp", C.c_double),
     ]
 
 
@@ -96,6 +97,8 @@ class PortSim:
         c.weno = kw.get("weno", 3)
         c.bcs = BCS[kw.get("bcs", "periodic")]
         c.integrator = INTEGRATORS[kw.get("integrator", "rk2")]
+        c.functional_sigma = 1 if kw.get("functionalSigma", False) else 0
+        c.sigma_exp = kw.get("gam", 12.0)
         self.cfg = c
         prims = np.ascontiguousarray(prims, dtype=np.float64)
         self.h = self.L.orc_create(C.byref(c), _ptr(prims))

@@ -54,6 +54,8 @@ typedef struct {
                    // 3 = KHRandomInstabilitySingleFluid, 4 = BrioWuSingleFluid,
                    // 5 = CurrentSheetSingleFluid
   int init_arg0, init_arg1;
+  int functional_sigma;  // Data::functionalSigma
+  double sigma_exp;      // Data::gam
 } mref_config;
 
 }  // extern "C"
@@ -108,7 +110,8 @@ void* mref_create(const mref_config* c, const double* prims) {
     // reportItersPeriod is set large so updateTime prints nothing.
     r->data = new Data(c->nx, c->ny, c->nz, c->xmin, c->xmax, c->ymin, c->ymax,
                        c->zmin, c->zmax, c->endTime, r->env, c->cfl, c->Ng,
-                       c->gamma, c->sigma, c->cp, -1.0e4, 1.0e4, 10, 1 << 30);
+                       c->gamma, c->sigma, c->cp, -1.0e4, 1.0e4, 10, 1 << 30,
+                       c->functional_sigma != 0, c->sigma_exp);
     if (c->model == 0) r->model = new SRMHD(r->data);
     else r->model = new SRRMHD(r->data);
     if (c->weno == 3) r->weno = new Weno3(r->data);

@@ -148,7 +148,32 @@ LIVE = {
                            ymax=1.0, endTime=3.0, cfl=0.4, Ng=4, gamma=4.0 / 3.0, sigma=1e3,
                            weno=3, bcs="periodic", integrator="ssp2322"),
                       lambda: initial.current_sheet(16, 32, seed=11), 2),
+    # Data::functionalSigma: conductivity sigma * D^gam per cell (simData.cc:114-127)
+    "sheet_ssp2_functional_sigma": (dict(model="srrmhd", nx=24, ny=48, xmin=-0.5, xmax=0.5,
+                                         ymin=-1.0, ymax=1.0, endTime=3.0, cfl=0.4, Ng=4,
+                                         gamma=4.0 / 3.0, sigma=1e3, weno=3, bcs="outflow",
+                                         integrator="ssp2", functionalSigma=True, gam=12.0),
+                                    lambda: _dense_sheet(24, 48, seed=12), 3),
+    "kh_srrmhd_rk2_functional_sigma": (dict(model="srrmhd", nx=24, ny=48, xmin=-0.5, xmax=0.5,
+                                            ymin=-1.0, ymax=1.0, endTime=3.0, cfl=0.4, Ng=4,
+                                            gamma=4.0 / 3.0, sigma=10.0, weno=3, bcs="flow",
+                                            integrator="rk2", functionalSigma=True, gam=3.0),
+                                       lambda: _dense_kh(24, 48, seed=13), 4),
 }
+
+
+def _dense_sheet(nx, ny, seed):
+    """Current sheet with a density that varies over the grid, so that a
+    functional conductivity sigma * D^gam differs from cell to cell."""
+    p = initial.current_sheet(nx, ny, seed=seed)
+    p[0] *= 1.0 + 0.3 * np.sin(np.linspace(0, 3.0, p.shape[2]))[None, :, None]
+    return p
+
+
+def _dense_kh(nx, ny, seed):
+    p = initial.kelvin_helmholtz(nx, ny, seed=seed, model="srrmhd")
+    p[0] *= 1.0 + 0.2 * np.cos(np.linspace(0, 2.0, p.shape[1]))[:, None, None]
+    return p
 
 
 @pytest.mark.parametrize("case", list(LIVE))
