@@ -62,6 +62,24 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+class quiet_stdout:
+    """Silences the process's C-level stdout (the reference build prints its
+    per-cell diagnostics there) for the duration of a CPU baseline."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        self.null = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(self.null, 1)
+        return self
+
+    def __exit__(self, *a):
+        sys.stdout.flush()
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+        os.close(self.null)
+
+
 class Clocks:
     """nvidia-smi sampling during the timed region."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -142,6 +160,34 @@ ENS_WORKLOAD = ("256 independent 2D Kelvin-Helmholtz simulations (ideal SRMHD + 
                 "one persistent launch per phase, step graph-captured, autotuned tile heights")
 
 
+def cpu_ensemble(initial):
+    """Reference-build (serial) estimate for one ensemble step: each member's
+    cells divided by its model's measured reference rate on a KH member of the
+    family (64x128: SRMHD RK2 for 20 steps, SRRMHD SSP2 for 2 steps)."""
+    from oracle import ref
+    if not ref.available():
+        return None
+    mem = initial.kh_ensemble(ENS_MEMBERS, seed=2024)
+    rates = {}
+    for model in ("srmhd", "srrmhd"):
+        c, ic = next((c, ic) for c, ic in mem if c["model"] == model)
+        c = dict(c, nx=64, ny=128, endTime=1e9)
+        c.pop("precision", None)
+        c.pop("guess", None)
+        ic = dict(ic, nx=64, ny=128)
+        sim = ref.RefSim(prims=initial.kelvin_helmholtz(**ic), **c)
+        steps = 20 if model == "srmhd" else 2
+        t0 = time.perf_counter()
+        sim.update_time(steps)
+        rates[model] = 64 * 128 * steps / (time.perf_counter() - t0)
+    cells = sum(c["nx"] * c["ny"] for c, _ in mem)
+    secs = sum(c["nx"] * c["ny"] / rates[c["model"]] for c, _ in mem)
+    return {"value": cells / secs, "unit": "zone-updates/s", "cores": 1, "kind": "reference",
+            "sample": "estimate: member cells / the reference build's serial rate per model "
+                      f"(SRMHD RK2 {rates['srmhd']:.3g}, SRRMHD SSP2 {rates['srrmhd']:.3g} "
+                      "zone-updates/s on a 64x128 member)"}
+
+
 def run_ensemble(mb, initial, torch, ranks, K, W, guess):
     """The ensemble workload, members split over ranks by cost (LPT)."""
     from method_b200.ranks import lpt_partition
@@ -180,6 +226,10 @@ def run_ensemble(mb, initial, torch, ranks, K, W, guess):
                                               "implicit_fallbacks", "implicit_failed")}
     ens.close()
     n_res = sum(1 for c, _ in mem if c["model"] == "srrmhd")
+    bytes_step = sum(mem[i][0]["nx"] * mem[i][0]["ny"] *
+                     (SHEET_BYTES if mem[i][0]["model"] == "srrmhd" else 616) for i in mine)
+    peak = measured_peaks()[0]
+    ach = ranks.sum(bytes_step) / (ms / K * 1e-3) / 1e9
     return {"value": total * K / (ms * 1e-3), "unit": "zone-updates/s", "ms_per_step": ms / K,
             "steps": K, "warmup": W, "members": ENS_MEMBERS, "resistive_members": n_res,
             "members_this_rank": len(mine), "interior_cells_total": int(total),
@@ -188,6 +238,10 @@ def run_ensemble(mb, initial, torch, ranks, K, W, guess):
             "implicit_iters_per_cell": agg["implicit_evals"] / max(agg["implicit_cells"], 1),
             **{k: agg[k] for k in ("c2p_unconverged", "c2p_fallbacks", "implicit_fallbacks",
                                    "implicit_failed")},
+            "roofline": {"bound": "hbm", "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(ach / peak, 4),
+                         "bytes": "sum over members of cells x (616 B SRMHD RK2, 1624 B SRRMHD "
+                                  "SSP2) per step"},
             "workload": ENS_WORKLOAD}
 
 
@@ -197,7 +251,41 @@ C2P_WORKLOAD = ("SRMHD primitive recovery of 256^3 independent random states (W 
                 "gamma 4/3; previous-step guess = generating rho and h 1% high, speed 1% low")
 
 
-def run_c2p_batch(mb, torch, ranks, guess, reps=3):
+C2P_BYTES = 152  # cons 9 + guess 2 doubles in, prims 8 out, per cell
+
+
+def cpu_c2p(cons, prims, aux, gamma, n=64):
+    """SRMHD::getPrimitiveVars of the reference build (serial) on an n^3 grid
+    holding the first n^3 of the same random states and guesses."""
+    from oracle import ref
+    if not ref.available():
+        return None
+    Ng = 4
+    cfg = dict(model="srmhd", nx=n, ny=n, nz=n, xmin=0.0, xmax=1.0, ymin=0.0, ymax=1.0,
+               zmin=0.0, zmax=1.0, endTime=1.0, cfl=0.4, Ng=Ng, gamma=gamma, weno=3,
+               bcs="outflow", integrator="rk2")
+    N = n + 2 * Ng
+    sl = (slice(None), slice(Ng, -Ng), slice(Ng, -Ng), slice(Ng, -Ng))
+
+    def grid(vals, nv):
+        a = np.zeros((nv, N, N, N))
+        a[sl] = vals.reshape(nv, n, n, n)
+        return a
+    # ghost cells hold the first state: getPrimitiveVars recovers the interior only
+    p0 = np.zeros((8, N, N, N))
+    p0[:] = prims[:, :1, None, None]
+    p0[sl] = prims.reshape(8, n, n, n)
+    sim = ref.RefSim(prims=p0, **cfg)
+    c, p, a = grid(cons, 9), p0, grid(aux, 13)
+    t0 = time.perf_counter()
+    sim.c2p(c, p, a)
+    el = time.perf_counter() - t0
+    return {"value": n ** 3 / el, "unit": "cells/s", "cores": 1, "kind": "reference",
+            "sample": f"SRMHD::getPrimitiveVars on a {n}^3 grid of the same states and "
+                      f"previous-step guesses, serial build (-O3), {el:.2f} s on the host"}
+
+
+def run_c2p_batch(mb, torch, ranks, guess, reps=3, cpu=False):
     """Batched primitive recovery: the reference method (Powell hybrid) and
     Newton from the previous-step, cold and learned guesses, each timed with
     CUDA events on its stream, iterations and error against the generating
@@ -262,12 +350,243 @@ def run_c2p_batch(mb, torch, ranks, guess, reps=3):
                      "median_rel_err_rho": float(rel.nan_to_num(1.0).median()),
                      "max_rel_err_rho": float(rel.nan_to_num(1.0).max())}
     L.mth_c2p_ctx_destroy(ctx)
+    peak = measured_peaks()[0]
+    for name, rec in out.items():
+        ach = C2P_BYTES * n / (rec["ms"] * 1e-3) / 1e9
+        rec["roofline"] = {"bound": "hbm", "achieved": round(ach, 1), "peak": peak,
+                           "unit": "GB/s", "frac": round(ach / peak, 4),
+                           "bytes_per_cell": C2P_BYTES}
     res = {"workload": C2P_WORKLOAD, "cells": n, "unit": "cells/s", "methods": out,
-           "iterations": "hybrd: residual evaluations; newton: Newton steps (incl. fallbacks)"}
+           "iterations": "hybrd: residual evaluations; newton: Newton steps (incl. fallbacks)",
+           "roofline": out["newton_previous"]["roofline"],
+           "hybrd_unconverged_fraction": out["hybrd_previous"]["unconverged"] / n}
+    if cpu:
+        m = 64 ** 3
+        with quiet_stdout():
+            res["cpu_baseline"] = cpu_c2p(cons[:, :m].cpu().numpy(), pg0[:, :m].cpu().numpy(),
+                                          ag0[:, :m].cpu().numpy(), gamma)
     if "newton_mlp" in out:
         res["mlp_iters_saved_vs_cold"] = (out["newton_cold"]["iters_per_cell"]
                                           - out["newton_mlp"]["iters_per_cell"])
     return res
+
+
+SHEET_SEED = 0
+SHEET_N = (512, 1024)
+SHEET_WORKLOAD = ("SRRMHD resistive current sheet 2D 512x1024 on [-0.5,0.5]x[-1,1], outflow, "
+                  "rho 1, p 50, By tanh(x/0.01), E = -v x B, seeded velocity noise 1e-3, "
+                  "gamma 4/3, sigma 10^U(1,5) per run from the seed, FVS+WENO3, IMEX SSP2, "
+                  "CFL 0.4")
+SHEET_BYTES = 1624  # algorithmic bytes per SSP2 zone-update (three passes over the state)
+
+
+def sheet_cfg(sigma):
+    nx, ny = SHEET_N
+    return dict(model="srrmhd", nx=nx, ny=ny, xmin=-0.5, xmax=0.5, ymin=-1.0, ymax=1.0,
+                endTime=1e9, cfl=0.4, Ng=4, gamma=4.0 / 3.0, sigma=sigma, weno=3,
+                bcs="outflow", integrator="ssp2")
+
+
+def timed_steps(sim, torch, device, dt, K, W, barrier, max_over_ranks):
+    """W warm-up steps, then K graph-launched steps timed with CUDA
+    events on the simulation's stream; returns ms (max over ranks)."""
+    stream = torch.cuda.Stream(device=device)
+    sim.set_stream(stream.cuda_stream)
+    for _ in range(W):
+        sim.step(dt, sync=False)
+    sim.sync()
+    sim.reset_stats()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    e0.record(stream)
+    for _ in range(K):
+        sim.step(dt, sync=False)
+    e1.record(stream)
+    barrier()
+    sim.sync()
+    return max_over_ranks(e0.elapsed_time(e1))
+
+
+def run_sheet(mb, initial, torch, ranks, K, W, peak, cpu):
+    """Config 3: SSP2 on the resistive current sheet, plain and mixed forms,
+    the reference CPU build's SSP2::step beside them (rank 0, N = 1)."""
+    sigma = initial.sigma_for_seed(SHEET_SEED)
+    cfg = sheet_cfg(sigma)
+    nx, ny = SHEET_N
+    cells = nx * ny
+    p0 = initial.current_sheet(nx, ny, seed=SHEET_SEED)
+    dt = 0.4 * min(1.0 / nx, 2.0 / ny) / np.sqrt(2.0)  # steady-state CFL dt
+    out, states = {}, {}
+    for form, prec in (("plain", "fp64"), ("mixed", "mixed")):
+        sim = mb.Simulation(precision=prec, device=ranks.local, **cfg)
+        sim.set_prims(p0)
+        kk = max(2, K // 5) if form == "plain" else K
+        ms = timed_steps(sim, torch, ranks.local, dt, kk, W, ranks.barrier, ranks.max)
+        st = sim.stats()
+        c, p, _ = sim.state()  # before the profiled steps below advance it
+        states[form] = (interior(c), interior(p))
+        ks, top, roof = roofline_of(sim, dt, peak)
+        roof["peak_kind"] = "measured (burst copy bandwidth, kernel timed alone)"
+        out[form] = {
+            "value": ranks.world * cells * kk / (ms * 1e-3), "ms_per_step": ms / kk,
+            "steps": kk, "implicit_failed": st["implicit_failed"],
+            "implicit_iters_per_cell": st["implicit_evals"] / max(st["implicit_cells"], 1),
+            "implicit_fallbacks": st["implicit_fallbacks"], "c2p_unconverged":
+                st["c2p_unconverged"], "roofline": roof,
+            "step_roofline": {"bytes_per_zone_update": SHEET_BYTES, "achieved_gbs": round(
+                SHEET_BYTES * cells / (ms / kk * 1e-3) / 1e9, 1), "peak": peak,
+                "frac": round(SHEET_BYTES * cells / (ms / kk * 1e-3) / 1e9 / peak, 4)},
+            "kernels": [{"name": k["name"], "launches_per_step": k["launches"] / 3.0,
+                         "ms_per_launch": round(k["total_ms"] / k["launches"], 4)} for k in ks],
+        }
+        sim.close()
+    l1 = {}
+    # both forms ran W + K(form) steps of the same dt; compare after equal step counts
+    # by re-running the plain form's count in the mixed form
+    sim = mb.Simulation(precision="mixed", device=ranks.local, **cfg)
+    sim.set_prims(p0)
+    for _ in range(W + out["plain"]["steps"]):
+        sim.step(dt, sync=False)
+    sim.sync()
+    c, p, _ = sim.state()
+    sim.close()
+    for k, name in enumerate(("cons", "prims")):
+        a, b = (interior(c), interior(p))[k], states["plain"][k]
+        d = np.abs(a - b)
+        l1[name] = {"l1_rel": float(d.sum() / np.abs(b).sum()), "max_abs": float(d.max())}
+    res = {"workload": SHEET_WORKLOAD, "seed": SHEET_SEED, "sigma": sigma, "dt": dt,
+           "unit": "zone-updates/s", "plain": out["plain"], "mixed": out["mixed"],
+           "speedup_mixed_vs_plain": out["mixed"]["value"] / out["plain"]["value"],
+           "l1_mixed_vs_fp64": {"steps": W + out["plain"]["steps"], **l1}}
+    if cpu:
+        res["cpu_baseline"] = cpu_sheet(cfg, p0, dt)
+    return res
+
+
+def cpu_sheet(cfg, p0, dt, steps=1):
+    """The reference build's serial SSP2::step on the full grid (bounded sample)."""
+    try:
+        from oracle import ref
+        if not ref.available():
+            raise FileNotFoundError
+        sim = ref.RefSim(prims=p0, **cfg)
+        kind = "reference"
+    except (FileNotFoundError, OSError):
+        from oracle import port
+        sim = port.PortSim(p0, **cfg)
+        kind = "port"
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        sim.step_dt(dt)
+    el = time.perf_counter() - t0
+    n = cfg["nx"] * cfg["ny"]
+    return {"value": n * steps / el, "unit": "zone-updates/s", "cores": 1, "kind": kind,
+            "sample": f"{steps} SSP2 step(s) of the {cfg['nx']}x{cfg['ny']} sheet, serial build "
+                      f"(-O3), {el:.1f} s on the host"}
+
+
+KH_WORKLOAD = ("SRMHD Kelvin-Helmholtz 2D 64x128 on [-0.5,0.5]x[-1,1], Flow boundaries "
+               "(periodic x, outflow y), rho 1, p 1, vx +-0.5 tanh shear layers at y = +-0.5 "
+               "(width 0.01), seeded vy noise 0.01, B 0, gamma 4/3, FVS+WENO3, RK2, CFL 0.4, "
+               "Simulation::evolve to t = 3")
+
+
+def run_kh_full(mb, initial, torch, ranks, peak, cpu):
+    """Config 1: the whole Kelvin-Helmholtz run (updateTime until t = 3), device
+    time with CUDA events on the simulation's stream, both forms."""
+    cfg = dict(model="srmhd", nx=64, ny=128, xmin=-0.5, xmax=0.5, ymin=-1.0, ymax=1.0,
+               endTime=3.0, cfl=0.4, Ng=4, gamma=4.0 / 3.0, weno=3, bcs="flow",
+               integrator="rk2")
+    p0 = initial.kelvin_helmholtz(64, 128, seed=1234)
+    cells = 64 * 128
+    res = {"workload": KH_WORKLOAD, "unit": "zone-updates/s"}
+    for form, prec in (("plain", "fp64"), ("mixed", "mixed")):
+        # one untimed run builds the per-dt step graphs; the timed run replays them
+        for rep in range(2):
+            sim = mb.Simulation(precision=prec, device=ranks.local, **cfg)
+            sim.set_prims(p0)
+            stream = torch.cuda.Stream(device=ranks.local)
+            sim.set_stream(stream.cuda_stream)
+            if rep == 0:
+                sim.evolve()
+                sim.close()
+                continue
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ranks.barrier()
+            e0.record(stream)
+            sim.evolve()
+            e1.record(stream)
+            ranks.barrier()
+            ms = ranks.max(e0.elapsed_time(e1))
+            st = sim.stats()
+            ks = sim.profile_step(0.4 * (1.0 / 64) / np.sqrt(2.0), reps=3)  # steady dt
+            top = max(ks, key=lambda k: k["total_ms"])
+            avg = top["total_ms"] / top["launches"]
+            ach = top["bytes_per_launch"] / (avg * 1e-3) / 1e9
+            sim.close()
+        res[form] = {"value": ranks.world * cells * st["iters"] / (ms * 1e-3),
+                     "ms_total": ms, "iters": st["iters"], "t": st["t"],
+                     "ms_per_step": ms / st["iters"],
+                     "roofline": {"kernel": top["name"], "bound": "hbm", "achieved": round(ach, 1),
+                                  "peak": peak, "unit": "GB/s", "frac": round(ach / peak, 4),
+                                  "note": "state (0.7 MB cons) lives in L2: launch/latency bound"}}
+    if cpu:
+        res["cpu_baseline"] = cpu_kh(cfg, p0)
+    return res
+
+
+def cpu_kh(cfg, p0, steps=100):
+    """The reference build's serial updateTime on the KH run's first `steps` calls."""
+    try:
+        from oracle import ref
+        if not ref.available():
+            raise FileNotFoundError
+        sim = ref.RefSim(prims=p0, **cfg)
+        kind = "reference"
+    except (FileNotFoundError, OSError):
+        from oracle import port
+        sim = port.PortSim(p0, **cfg)
+        kind = "port"
+    t0 = time.perf_counter()
+    sim.update_time(steps)
+    el = time.perf_counter() - t0
+    return {"value": cfg["nx"] * cfg["ny"] * steps / el, "unit": "zone-updates/s", "cores": 1,
+            "kind": kind, "sample": f"the first {steps} updateTime calls of the 64x128 run, "
+                                    f"serial build (-O3), {el:.1f} s on the host"}
+
+
+def cpu_legs(initial, sheet, kh, ensemble):
+    """The reference build's CPU baselines of the side workloads."""
+    if sheet is not None:
+        sheet["cpu_baseline"] = cpu_sheet(sheet_cfg(sheet["sigma"]),
+                                          initial.current_sheet(*SHEET_N, seed=SHEET_SEED),
+                                          sheet["dt"])
+    if kh is not None:
+        kh["cpu_baseline"] = cpu_kh(
+            dict(model="srmhd", nx=64, ny=128, xmin=-0.5, xmax=0.5, ymin=-1.0, ymax=1.0,
+                 endTime=3.0, cfl=0.4, Ng=4, gamma=4.0 / 3.0, weno=3, bcs="flow",
+                 integrator="rk2"), initial.kelvin_helmholtz(64, 128, seed=1234))
+    if ensemble is not None:
+        ensemble["cpu_baseline"] = cpu_ensemble(initial)
+
+
+def long_run_l1(mb, initial, ranks, n, steps=500):
+    """Mixed against plain after the configuration's full 500 updateTime calls."""
+    st = {}
+    for prec in ("fp64", "mixed"):
+        sim = mb.Simulation(nx=n, ny=n, precision=prec, device=ranks.local, **CFG)
+        sim.set_prims(initial.orszag_tang(n, Ng=4))
+        sim.update_time(steps)
+        c, p, _ = sim.state()
+        s = sim.stats()
+        st[prec] = (interior(c), interior(p), s)
+        sim.close()
+    out = {"steps": steps, "t": st["fp64"][2]["t"]}
+    for k, name in enumerate(("cons", "prims")):
+        a, b = st["mixed"][k], st["fp64"][k]
+        d = np.abs(a - b)
+        out[name] = {"l1_rel": float(d.sum() / np.abs(b).sum()), "max_abs": float(d.max())}
+    return out
 
 
 def roofline_of(sim, dt, peak, reps=3):
@@ -373,6 +692,9 @@ def main():
                     help="forms to run (profiling runs one at a time)")
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--no-c2p-batch", action="store_true")
+    ap.add_argument("--no-sheet", action="store_true", help="skip the SSP2 current sheet")
+    ap.add_argument("--no-kh", action="store_true", help="skip the whole KH 64x128 run")
+    ap.add_argument("--no-long-l1", action="store_true", help="skip the 500-step L1 check")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
@@ -430,9 +752,21 @@ def main():
                     k: e_mlp[k] for k in ("value", "ms_per_step", "c2p_newton_iters_per_cell",
                                           "c2p_unconverged", "c2p_fallbacks")}
         c2p_batch = None
+        want_cpu = rank == 0 and world == 1 and not args.no_cpu
         if not args.no_c2p_batch:
-            c2p_batch = run_c2p_batch(mb, torch, ranks, guess)
+            c2p_batch = run_c2p_batch(mb, torch, ranks, guess, cpu=want_cpu)
+        sheet = None
+        if not args.no_sheet:
+            sheet = run_sheet(mb, initial, torch, ranks, max(K // 5, 5), max(W, 3), peak,
+                              cpu=False)
+        kh = None
+        if not args.no_kh:
+            kh = run_kh_full(mb, initial, torch, ranks, peak, cpu=False)
     clk = clocks.summary()
+    long_l1 = None if args.no_long_l1 else long_run_l1(mb, initial, ranks, n)
+    if want_cpu:  # reference-build baselines on the host, after the timed GPU work
+        with quiet_stdout():
+            cpu_legs(initial, sheet, kh, ensemble)
 
     cells = n * n
     for form in forms:
@@ -505,7 +839,8 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_baseline(n)
+        with quiet_stdout():
+            cpu = cpu_baseline(n)
 
     if rank == 0:
         m = results["mixed"]["summary"]
@@ -525,6 +860,9 @@ def main():
             "mixed_mlp": results["mixed_mlp"]["summary"] if "mixed_mlp" in results else None,
             "guess_training": train,
             "l1_mixed_vs_fp64": l1,
+            "l1_mixed_vs_fp64_500_steps": long_l1,
+            "kh64x128_full_run": kh,
+            "sheet_ssp2": sheet,
             "ensemble": ensemble,
             "c2p_batch": c2p_batch,
             "speedup_mixed_vs_plain": results["plain"]["ms"] / results["mixed"]["ms"],

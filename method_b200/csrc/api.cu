@@ -130,12 +130,13 @@ cudaError_t c2p_raw(mth_handle* h, const double* cons, const double* pg, const d
 cudaError_t flux_stage_raw(mth_handle* h, double* c, double* p, double* a, const double* u0,
                        double* out, double dt, int mode) {
   const Grid& g = h->g;
+  const StageTail tail{h->flux1, h->src1, g.cp};
   if (h->fused) {
     if (h->cfg.precision == MTH_MIXED)
       return launch_fvs2d_fp32(g, h->cfg.model, h->cfg.weno_order, c, p, a, u0, out, dt, mode,
-                               h->st);
+                               h->st, tail);
     return launch_fvs2d_fp64(g, h->cfg.model, h->cfg.weno_order, c, p, a, u0, out, dt, mode,
-                             h->st);
+                             h->st, tail);
   }
   cudaError_t e = launch_fvs_generic(g, h->cfg.model, h->cfg.weno_order, c, p, a, h->fplus,
                                      h->fminus, h->frecon, h->fnet, h->st);
@@ -161,7 +162,10 @@ cudaError_t flux_stage(mth_handle* h, double* c, double* p, double* a, const dou
                        double* out, double dt, int mode) {
   const bool srmhd = h->cfg.model == MTH_SRMHD;
   const double in = srmhd ? 22 : 24, nc = h->NC;
-  const double dpc = in + nc + (mode == STAGE_RK2_CORR ? nc : 0);
+  // flux inputs + the written state (+ u0 for the corrector; + u0, flux1,
+  // source1 and the 6 source inputs for the fused SSP2 closing stage)
+  const double dpc = in + nc + (mode == STAGE_RK2_CORR ? nc : 0) +
+                     (mode == STAGE_SSP2_FINAL ? 3 * nc + 6 : 0);
   const char* name = h->fused ? (h->cfg.precision == MTH_MIXED ? "fvs2d_fp32" : "fvs2d_fp64")
                               : "fvs_generic";
   return timed(h, name, dpc, [&] { return flux_stage_raw(h, c, p, a, u0, out, dt, mode); });
@@ -266,6 +270,13 @@ cudaError_t enqueue_step(mth_handle* h, double dt) {
        })))
     return e;
   if ((e = c2p(h, h->u2, h->prims, h->aux, h->prims, h->aux, true))) return e;
+  // flux2 = F(U2), source2 = S(U2) and the combination (SSP2.cc:150-170) in
+  // one pass: the stage-2 flux tile's epilogue updates cons in place
+  if (h->fused) {
+    if ((e = flux_stage(h, h->u2, h->prims, h->aux, h->cons, h->cons, dt, STAGE_SSP2_FINAL)))
+      return e;
+    return c2p(h, h->cons, h->prims, h->aux, h->prims, h->aux);
+  }
   if ((e = timed(h, "source", 31, [&] {
          return launch_source(h->g, h->cfg.model, h->u2, h->aux, h->src2, h->st);
        })))

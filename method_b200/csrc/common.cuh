@@ -23,6 +23,17 @@ enum StageMode : int {
   STAGE_FNET = 0,      // out = fnet (FVS::F)
   STAGE_EULER = 1,     // out = in - dt * fnet (RK2 predictor, RK2.cc:58-66)
   STAGE_RK2_CORR = 2,  // out = 0.5 * (u0 + in - dt * fnet) (RK2.cc:81-89)
+  // SSP2's closing combination (SSP2.cc:155-166) fused into the stage-2 flux:
+  // out = u0 + -0.5 dt (flux1 + fnet - source1 - S(in)), S(in) from the
+  // stage state's own cons / aux in registers.
+  STAGE_SSP2_FINAL = 3,
+};
+
+// Extra inputs of STAGE_SSP2_FINAL: the stage-1 flux and source and cp.
+struct StageTail {
+  const double* flux1;
+  const double* source1;
+  double cp;
 };
 
 struct Grid {

@@ -224,8 +224,7 @@ cudaError_t srrmhd_ssp2(mth_ensemble* e, cudaStream_t s) {
   Item* it = e->d_cells[md];
   cudaError_t r;
   for (int stage = 1; stage <= 2; ++stage) {
-    const int u = stage == 1 ? EA_U1 : EA_U2, src = stage == 1 ? EA_S1 : EA_S2,
-              fl = stage == 1 ? EA_F1 : EA_F2;
+    const int u = stage == 1 ? EA_U1 : EA_U2;
     if ((r = phase(e, s, "imex_newton", [&] {
            return ens_imex_fast(e->d_mem, it, n, stage, grid, s);
          })))
@@ -233,13 +232,16 @@ cudaError_t srrmhd_ssp2(mth_ensemble* e, cudaStream_t s) {
     if ((r = phase(e, s, "imex_queued", [&] { return ens_imex_queued(e->d_mem, e->n, stage, s); })))
       return r;
     if ((r = c2p_phase(e, s, md, u, EA_PRIMS, EA_AUX, EA_PRIMS, EA_AUX, true))) return r;
+    if (stage == 2) break;
     if ((r = phase(e, s, "source", [&] {
-           return ens_source(e->d_mem, it, n, u, EA_AUX, src, grid, s);
+           return ens_source(e->d_mem, it, n, u, EA_AUX, EA_S1, grid, s);
          })))
       return r;
-    if ((r = flux_phase(e, s, md, u, EA_PRIMS, EA_AUX, -1, fl, STAGE_FNET))) return r;
+    if ((r = flux_phase(e, s, md, u, EA_PRIMS, EA_AUX, -1, EA_F1, STAGE_FNET))) return r;
   }
-  if ((r = phase(e, s, "ssp2_combine", [&] { return ens_combine(e->d_mem, it, n, grid, s); })))
+  // F(U2), S(U2) and the combination (SSP2.cc:150-170) fused into the stage-2
+  // flux phase, cons updated in place
+  if ((r = flux_phase(e, s, md, EA_U2, EA_PRIMS, EA_AUX, EA_CONS, EA_CONS, STAGE_SSP2_FINAL)))
     return r;
   return c2p_phase(e, s, md, EA_CONS, EA_PRIMS, EA_AUX, EA_PRIMS, EA_AUX);
 }
@@ -338,10 +340,9 @@ mth_status mth_ensemble_create(const mth_config* cfgs, int n, mth_ensemble** out
     Member& d = e->mem[m];
     const int nc = d.model == MTH_SRMHD ? 9 : 14, np = d.model == MTH_SRMHD ? 8 : 11,
               na = d.model == MTH_SRMHD ? 13 : 17;
-    const int sizes[EA_COUNT] = {nc, np, na, nc, np, na, nc, nc, nc, nc, nc, nc, 2, 2};
+    const int sizes[EA_COUNT] = {nc, np, na, nc, np, na, nc, nc, nc, nc, 2, 2};
     const bool need[EA_COUNT] = {true, true, true,
                                  d.model == MTH_SRMHD, d.model == MTH_SRMHD, d.model == MTH_SRMHD,
-                                 d.model == MTH_SRRMHD, d.model == MTH_SRRMHD,
                                  d.model == MTH_SRRMHD, d.model == MTH_SRRMHD,
                                  d.model == MTH_SRRMHD, d.model == MTH_SRRMHD,
                                  d.model == MTH_SRMHD,

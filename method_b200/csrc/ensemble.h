@@ -18,7 +18,7 @@ namespace mth {
 enum EnsArray : int {
   EA_CONS = 0, EA_PRIMS, EA_AUX,
   EA_P1C, EA_P1P, EA_P1A,            // RK2 predictor state
-  EA_U1, EA_U2, EA_F1, EA_F2, EA_S1, EA_S2,  // SSP2 stages
+  EA_U1, EA_U2, EA_F1, EA_S1,        // SSP2 stages (F(U2), S(U2) stay in registers)
   EA_SOL,                            // SRMHD C2P solution (2 planes)
   EA_ZG,                             // SRMHD learned guess (Z, v^2 planes)
   EA_COUNT
@@ -51,8 +51,6 @@ cudaError_t ens_c2p_retry(const Member* mem, int n_members, int ic, int ip, int 
 cudaError_t ens_imex_queued(const Member* mem, int n_members, int stage, cudaStream_t st);
 cudaError_t ens_source(const Member* mem, const Item* items, int n_items, int ic, int ia,
                        int iout, int grid, cudaStream_t st);
-cudaError_t ens_combine(const Member* mem, const Item* items, int n_items, int grid,
-                        cudaStream_t st);
 cudaError_t ens_dt(Member* mem, int n_members, cudaStream_t st);
 cudaError_t ens_advance(Member* mem, int n_members, cudaStream_t st);
 

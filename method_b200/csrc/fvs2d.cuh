@@ -133,7 +133,7 @@ __device__ __forceinline__ void fvs2d_tile(const Grid& g, const double* __restri
                                            const double* __restrict__ prims,
                                            const double* __restrict__ aux, const double* u0,
                                            double* out, double dt, int mode, int ti, int tj,
-                                           unsigned char* smem_raw) {
+                                           unsigned char* smem_raw, StageTail tail = {}) {
   using S = Fvs2dSmem<M, R, ORDER, TI>;
   constexpr int NC = M::NC, TJ = S::TJ, H = S::H, NT = 32 * TI;
   R* sp = reinterpret_cast<R*>(smem_raw);
@@ -216,6 +216,18 @@ __device__ __forceinline__ void fvs2d_tile(const Grid& g, const double* __restri
 
     // ---------------- stage update ----------------
     const long long cell = cell_id(g, ci, cj, 0);
+    if (mode == STAGE_SSP2_FINAL) {
+      // cons += -0.5 dt (flux1 + flux2 - source1 - source2) in the reference's
+      // order (SSP2.cc:155-166), flux2 = this fnet, source2 = S(stage state)
+      double s2[NC];
+      M::cell_source(cons, aux, g.Ntot, cell, tail.cp, s2);
+#pragma unroll
+      for (int v = 0; v < NC; ++v) {
+        const long long o = (long long)v * g.Ntot + cell;
+        out[o] = u0[o] + -0.5 * dt * (tail.flux1[o] + (double)acc[v] - tail.source1[o] - s2[v]);
+      }
+      return;
+    }
 #pragma unroll
     for (int v = 0; v < NC; ++v) {
       const long long o = (long long)v * g.Ntot + cell;
@@ -235,10 +247,10 @@ template <class M, typename R, int ORDER, int TI>
 __global__ void __launch_bounds__(32 * TI, (fvs2d_min_blocks<M, R, ORDER, TI>()))
     k_fvs2d(Grid g, const double* __restrict__ cons, const double* __restrict__ prims,
             const double* __restrict__ aux, const double* u0, double* out, double dt,
-            int mode) {
+            int mode, StageTail tail) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   fvs2d_tile<M, R, ORDER, TI>(g, cons, prims, aux, u0, out, dt, mode, blockIdx.y, blockIdx.x,
-                              smem_raw);
+                              smem_raw, tail);
 }
 
 }  // namespace mth

@@ -766,7 +766,7 @@ __global__ void __launch_bounds__(128)
 template <class M, int ORDER, int TI>
 cudaError_t fvs2d_instance(const Grid& g, const double* cons, const double* prims,
                            const double* aux, const double* u0, double* out, double dt, int mode,
-                           cudaStream_t st) {
+                           StageTail tail, cudaStream_t st) {
   using S = Fvs2dSmem<M, double, ORDER, TI>;
   auto kern = k_fvs2d<M, double, ORDER, TI>;
   static bool configured = false;
@@ -778,7 +778,7 @@ cudaError_t fvs2d_instance(const Grid& g, const double* cons, const double* prim
   }
   dim3 grid((g.je - g.js + 31) / 32, (g.ie - g.is + TI - 1) / TI);
   dim3 block(32, TI);
-  kern<<<grid, block, S::bytes, st>>>(g, cons, prims, aux, u0, out, dt, mode);
+  kern<<<grid, block, S::bytes, st>>>(g, cons, prims, aux, u0, out, dt, mode, tail);
   return cudaGetLastError();
 }
 
@@ -794,7 +794,8 @@ __global__ void __launch_bounds__(32 * TI)
     const Member& d = mem[w.m];
     const Grid g = d.g;
     fvs2d_tile<M, double, ORDER, TI>(g, d.a[ic], d.a[ip], d.a[ia], iu0 >= 0 ? d.a[iu0] : nullptr,
-                                     d.a[iout], d.dt, mode, w.a, w.b, smem_raw);
+                                     d.a[iout], d.dt, mode, w.a, w.b, smem_raw,
+                                     StageTail{d.a[EA_F1], d.a[EA_S1], g.cp});
     __syncthreads();
   }
 }
@@ -877,26 +878,6 @@ __global__ void __launch_bounds__(128)
   }
 }
 
-// SSP2 combination (SSP2.cc:155-166) of every SRRMHD member, as k_ssp2_combine.
-__global__ void __launch_bounds__(128)
-    k_ens_combine(const Member* __restrict__ mem, const Item* __restrict__ items, int n_items) {
-  for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
-    const Item w = items[it];
-    const Member& d = mem[w.m];
-    const Grid g = d.g;
-    const long long t = w.a + threadIdx.x;
-    if (t >= n_interior(g)) continue;
-    int i, j, k;
-    interior_ijk(g, t, i, j, k);
-    const long long cell = cell_id(g, i, j, k);
-    for (int v = 0; v < 14; ++v) {
-      const long long o = v * g.Ntot + cell;
-      d.a[EA_CONS][o] += -0.5 * d.dt *
-                         (d.a[EA_F1][o] + d.a[EA_F2][o] - d.a[EA_S1][o] - d.a[EA_S2][o]);
-    }
-  }
-}
-
 // Simulation::updateTime's dt for every member (simulation.cc:113-124); the
 // expression is the host's, compiled without contraction.
 __global__ void k_ens_dt(Member* mem, int n) {
@@ -962,13 +943,14 @@ cudaError_t launch_apply_bcs(const Grid& g, double* arr, int nvars, cudaStream_t
 
 cudaError_t launch_fvs2d_fp64(const Grid& g, int model, int order, const double* cons,
                               const double* prims, const double* aux, const double* u0,
-                              double* out, double dt, int mode, cudaStream_t st) {
+                              double* out, double dt, int mode, cudaStream_t st,
+                              StageTail tail) {
   if (model == MODEL_SRMHD) {
-    if (order == 3) return fvs2d_instance<SRMHD, 3, 8>(g, cons, prims, aux, u0, out, dt, mode, st);
-    return fvs2d_instance<SRMHD, 5, 8>(g, cons, prims, aux, u0, out, dt, mode, st);
+    if (order == 3) return fvs2d_instance<SRMHD, 3, 8>(g, cons, prims, aux, u0, out, dt, mode, tail, st);
+    return fvs2d_instance<SRMHD, 5, 8>(g, cons, prims, aux, u0, out, dt, mode, tail, st);
   }
-  if (order == 3) return fvs2d_instance<SRRMHD, 3, 8>(g, cons, prims, aux, u0, out, dt, mode, st);
-  return fvs2d_instance<SRRMHD, 5, 8>(g, cons, prims, aux, u0, out, dt, mode, st);
+  if (order == 3) return fvs2d_instance<SRRMHD, 3, 8>(g, cons, prims, aux, u0, out, dt, mode, tail, st);
+  return fvs2d_instance<SRRMHD, 5, 8>(g, cons, prims, aux, u0, out, dt, mode, tail, st);
 }
 
 cudaError_t launch_fvs_generic(const Grid& g, int model, int order, double* cons, double* prims,
@@ -1212,10 +1194,6 @@ cudaError_t ens_source(const Member* mem, const Item* items, int n, int ic, int 
   return cudaGetLastError();
 }
 
-cudaError_t ens_combine(const Member* mem, const Item* items, int n, int grid, cudaStream_t st) {
-  k_ens_combine<<<grid, 128, 0, st>>>(mem, items, n);
-  return cudaGetLastError();
-}
 
 cudaError_t ens_dt(Member* mem, int n, cudaStream_t st) {
   k_ens_dt<<<(n + 127) / 128, 128, 0, st>>>(mem, n);

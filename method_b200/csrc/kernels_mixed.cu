@@ -661,7 +661,8 @@ __global__ void __launch_bounds__(32 * TI, (fvs2d_min_blocks<M, float, ORDER, TI
     const Member& d = mem[w.m];
     const Grid g = d.g;
     fvs2d_tile<M, float, ORDER, TI>(g, d.a[ic], d.a[ip], d.a[ia], iu0 >= 0 ? d.a[iu0] : nullptr,
-                                    d.a[iout], d.dt, mode, w.a, w.b, smem_raw);
+                                    d.a[iout], d.dt, mode, w.a, w.b, smem_raw,
+                                    StageTail{d.a[EA_F1], d.a[EA_S1], g.cp});
     __syncthreads();
   }
 }
@@ -752,7 +753,7 @@ cudaError_t ens_fvs_fp32_instance(const Member* mem, const Item* items, int n, i
 template <class M, int ORDER, int TI>
 cudaError_t fvs2d_fp32_instance(const Grid& g, const double* cons, const double* prims,
                                 const double* aux, const double* u0, double* out, double dt,
-                                int mode, cudaStream_t st) {
+                                int mode, StageTail tail, cudaStream_t st) {
   using S = Fvs2dSmem<M, float, ORDER, TI>;
   auto kern = k_fvs2d<M, float, ORDER, TI>;
   cudaError_t e =
@@ -760,7 +761,7 @@ cudaError_t fvs2d_fp32_instance(const Grid& g, const double* cons, const double*
   if (e != cudaSuccess) return e;
   dim3 grid((g.je - g.js + 31) / 32, (g.ie - g.is + TI - 1) / TI);
   dim3 block(32, TI);
-  kern<<<grid, block, S::bytes, st>>>(g, cons, prims, aux, u0, out, dt, mode);
+  kern<<<grid, block, S::bytes, st>>>(g, cons, prims, aux, u0, out, dt, mode, tail);
   return cudaGetLastError();
 }
 
@@ -822,15 +823,16 @@ cudaError_t ens_imex_fast(const Member* mem, const Item* items, int n, int stage
 
 cudaError_t launch_fvs2d_fp32(const Grid& g, int model, int order, const double* cons,
                               const double* prims, const double* aux, const double* u0,
-                              double* out, double dt, int mode, cudaStream_t st) {
+                              double* out, double dt, int mode, cudaStream_t st,
+                              StageTail tail) {
   if (model == MODEL_SRMHD) {
     if (order == 3)
-      return fvs2d_fp32_instance<SRMHD, 3, 8>(g, cons, prims, aux, u0, out, dt, mode, st);
-    return fvs2d_fp32_instance<SRMHD, 5, 8>(g, cons, prims, aux, u0, out, dt, mode, st);
+      return fvs2d_fp32_instance<SRMHD, 3, 8>(g, cons, prims, aux, u0, out, dt, mode, tail, st);
+    return fvs2d_fp32_instance<SRMHD, 5, 8>(g, cons, prims, aux, u0, out, dt, mode, tail, st);
   }
   if (order == 3)
-    return fvs2d_fp32_instance<SRRMHD, 3, 8>(g, cons, prims, aux, u0, out, dt, mode, st);
-  return fvs2d_fp32_instance<SRRMHD, 5, 8>(g, cons, prims, aux, u0, out, dt, mode, st);
+    return fvs2d_fp32_instance<SRRMHD, 3, 8>(g, cons, prims, aux, u0, out, dt, mode, tail, st);
+  return fvs2d_fp32_instance<SRRMHD, 5, 8>(g, cons, prims, aux, u0, out, dt, mode, tail, st);
 }
 
 cudaError_t launch_c2p_batch(long long n, double gamma, int method, int guess,

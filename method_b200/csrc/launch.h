@@ -38,7 +38,8 @@ cudaError_t launch_prims_to_all(const Grid& g, int model, const double* prims, d
 cudaError_t launch_apply_bcs(const Grid& g, double* arr, int nvars, cudaStream_t st);
 cudaError_t launch_fvs2d_fp64(const Grid& g, int model, int order, const double* cons,
                               const double* prims, const double* aux, const double* u0,
-                              double* out, double dt, int mode, cudaStream_t st);
+                              double* out, double dt, int mode, cudaStream_t st,
+                              StageTail tail = {});
 // Generic (1D/2D/3D) flux path: materialised ghosts, one pass per direction.
 cudaError_t launch_fvs_generic(const Grid& g, int model, int order, double* cons, double* prims,
                                double* aux, double* fplus, double* fminus, double* frecon,

@@ -53,7 +53,8 @@ void mixed_free(MixedWork* w);
 
 cudaError_t launch_fvs2d_fp32(const Grid& g, int model, int order, const double* cons,
                               const double* prims, const double* aux, const double* u0,
-                              double* out, double dt, int mode, cudaStream_t st);
+                              double* out, double dt, int mode, cudaStream_t st,
+                              StageTail tail = {});
 
 // guess: 0 = previous state, 1 = guess network (falls back to the previous
 // state, then to the reference Powell-hybrid, when Newton does not converge).

@@ -220,6 +220,14 @@ struct SRMHD {
   __device__ __forceinline__ static void flux(const R* c, const R* p, const R* a, int dir, R* f) {
     srmhd::flux<R>(c, p, a, dir, f);
   }
+  // Model::sourceTerm of one cell in FP64 (srmhd.cc:215-250): S_phi = -phi/cp^2.
+  __device__ __forceinline__ static void cell_source(const double* __restrict__ cons,
+                                                     const double*, long long N, long long cell,
+                                                     double cp, double* s) {
+#pragma unroll
+    for (int v = 0; v < NC; ++v) s[v] = 0;
+    s[8] = -cons[8 * N + cell] / (cp * cp);
+  }
 };
 
 }  // namespace mth

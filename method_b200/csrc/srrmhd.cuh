@@ -271,6 +271,18 @@ struct SRRMHD {
   __device__ __forceinline__ static void flux(const R* c, const R* p, const R* a, int dir, R* f) {
     srrmhd::flux<R>(c, p, a, dir, f);
   }
+  // Model::sourceTerm of one cell in FP64 (srrmhd.cc:194-206): reads cons
+  // 11-13 and aux 4-6 only.
+  __device__ __forceinline__ static void cell_source(const double* __restrict__ cons,
+                                                     const double* __restrict__ aux, long long N,
+                                                     long long cell, double cp, double* s) {
+    double c[NC], a[NA];
+#pragma unroll
+    for (int v = 11; v < 14; ++v) c[v] = cons[v * N + cell];
+#pragma unroll
+    for (int v = 4; v < 7; ++v) a[v] = aux[v * N + cell];
+    srrmhd::source(c, a, cp, s);
+  }
 };
 
 cudaError_t launch_prims_to_all_srrmhd(const Grid& g, const double* prims, double* cons,
