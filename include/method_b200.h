@@ -52,6 +52,15 @@ typedef struct {
   int device;                /* CUDA device ordinal */
   int functional_sigma;      /* Data::functionalSigma: conductivity sigma * D^sigma_exp */
   double sigma_exp;          /* Data::gam (simData.h:86; the reference's default is 12) */
+  /* x-slab decomposition (the counterpart of ParallelEnv's split over
+   * nxRanks, Project/CPU/Src/parallelEnv.cc:16-127): when x_slab is set,
+   * this handle holds interior columns [x_offset, x_offset + nx) of a domain
+   * of x_global_nx columns whose bounds are xmin, xmax, and its x halo rows
+   * are filled by the caller (mth_halo_*) instead of by the boundary
+   * conditions.  RK2, RKSplit and SSP2 only. */
+  int x_slab;
+  int x_global_nx;
+  int x_offset;
 } mth_config;
 
 typedef struct {
@@ -125,6 +134,30 @@ mth_status mth_step(mth_handle* h, double dt);
 mth_status mth_update_time(mth_handle* h, int n);
 /* Simulation::evolve without output: updateTime until t >= endTime. */
 mth_status mth_evolve(mth_handle* h);
+/* ---- x-slab decomposition: one domain over several handles (one per GPU).
+ * A step is a sequence of parts that end where the reference applies the
+ * boundary conditions to an intermediate state (TimeIntegrator::finalise):
+ * RK2 / RKSplit 2 (predictor | corrector), SSP2 3 (stage 1 | stage 2 |
+ * combination); SSP3 / SSP2322 1.  After each part the caller exchanges the
+ * Ng-deep x halos of that part's state, which is what ParallelBcs::apply
+ * does through swapGhostBuffers (Project/CPU/Src/parallelBoundaryConds.cc:
+ * 11-30): pack the Ng interior rows next to each x face into a device
+ * buffer of mth_halo_bytes, send them to the neighbour, unpack what the
+ * neighbours sent into the ghost rows; at a physical outflow x face,
+ * mth_halo_outflow fills the ghost rows instead.  part -1 is the handle's
+ * main state (after mth_set_prims / mth_upload).  Buffers are device memory
+ * laid out [cons vars | prims vars | aux vars][Ng rows][Ny*Nz]; every copy
+ * is ordered on the handle's stream. */
+mth_status mth_step_parts(const mth_handle* h, int* n_parts);
+mth_status mth_step_part(mth_handle* h, double dt, int part);
+/* Simulation::updateTime's dt for the next step, and its t += dt, iters++. */
+mth_status mth_next_dt(const mth_handle* h, double* dt);
+mth_status mth_advance_time(mth_handle* h, double dt);
+mth_status mth_halo_bytes(const mth_handle* h, unsigned long long* bytes);
+mth_status mth_halo_pack(mth_handle* h, int part, int side, void* dst);
+mth_status mth_halo_unpack(mth_handle* h, int part, int side, const void* src);
+mth_status mth_halo_outflow(mth_handle* h, int part, int side);
+
 /* Waits for queued work and returns the first device-side error, if any. */
 mth_status mth_sync(mth_handle* h);
 mth_status mth_get_stats(mth_handle* h, mth_stats* s);

@@ -50,7 +50,7 @@ def _dptr(a):
 def _config(nx, ny, nz=0, xmin=0.0, xmax=1.0, ymin=0.0, ymax=1.0, zmin=0.0, zmax=1.0,
             endTime=1.0, cfl=0.5, Ng=4, gamma=5.0 / 3.0, sigma=1e3, cp=0.1, model="srmhd",
             weno=3, bcs="periodic", integrator="rk2", precision="fp64", guess="previous",
-            device=0, functionalSigma=False, gam=12.0):
+            device=0, functionalSigma=False, gam=12.0, x_slab=None):
     """mth_config from the reference Data constructor's arguments plus the
     class choices of a reference main.cc."""
     c = _lib.Config()
@@ -67,6 +67,9 @@ def _config(nx, ny, nz=0, xmin=0.0, xmax=1.0, ymin=0.0, ymax=1.0, zmin=0.0, zmax
     c.device = device
     c.functional_sigma = 1 if functionalSigma else 0
     c.sigma_exp = gam
+    if x_slab is not None:  # (offset, global nx): columns [offset, offset + nx) of the domain
+        c.x_slab = 1
+        c.x_offset, c.x_global_nx = x_slab
     return c
 
 

@@ -19,7 +19,9 @@ STATUS = {0: "MTH_OK", 1: "MTH_ERR_C2P", 2: "MTH_ERR_IMPLICIT", 3: "MTH_ERR_INVA
 SYMBOLS = [
     "mth_create", "mth_destroy", "mth_last_error", "mth_get_dims", "mth_set_prims",
     "mth_upload", "mth_download", "mth_apply_bcs", "mth_prims_to_all", "mth_c2p",
-    "mth_flux_F", "mth_source", "mth_flux_vector", "mth_c2p_cells", "mth_step", "mth_update_time", "mth_evolve", "mth_sync",
+    "mth_flux_F", "mth_source", "mth_flux_vector", "mth_c2p_cells", "mth_step", "mth_update_time", "mth_evolve",
+    "mth_step_parts", "mth_step_part", "mth_next_dt", "mth_advance_time", "mth_halo_bytes",
+    "mth_halo_pack", "mth_halo_unpack", "mth_halo_outflow", "mth_sync",
     "mth_get_stats", "mth_reset_stats", "mth_step_host", "mth_step_host_bytes", "mth_pin_host",
     "mth_unpin_host",
     "mth_set_stream", "mth_profile_step", "mth_mlp_train", "mth_mlp_grad", "mth_mlp_forward",
@@ -55,6 +57,7 @@ class Config(C.Structure):
         ("weno_order", C.c_int), ("bcs", C.c_int), ("integrator", C.c_int),
         ("precision", C.c_int), ("guess", C.c_int), ("device", C.c_int),
         ("functional_sigma", C.c_int), ("sigma_exp", C.c_double),
+        ("x_slab", C.c_int), ("x_global_nx", C.c_int), ("x_offset", C.c_int),
     ]
 
 
@@ -105,6 +108,14 @@ def load():
                                 C.c_double, C.c_int]
     L.mth_step.argtypes = [H, C.c_double]
     L.mth_update_time.argtypes = [H, C.c_int]
+    L.mth_step_parts.argtypes = [H, C.POINTER(C.c_int)]
+    L.mth_step_part.argtypes = [H, C.c_double, C.c_int]
+    L.mth_next_dt.argtypes = [H, D]
+    L.mth_advance_time.argtypes = [H, C.c_double]
+    L.mth_halo_bytes.argtypes = [H, C.POINTER(C.c_ulonglong)]
+    L.mth_halo_pack.argtypes = [H, C.c_int, C.c_int, C.c_void_p]
+    L.mth_halo_unpack.argtypes = [H, C.c_int, C.c_int, C.c_void_p]
+    L.mth_halo_outflow.argtypes = [H, C.c_int, C.c_int]
     L.mth_get_stats.argtypes = [H, C.POINTER(Stats)]
     L.mth_device_state.argtypes = [H, C.POINTER(D), C.POINTER(D), C.POINTER(D)]
     L.mth_save_text.argtypes = [H, C.c_char_p, C.c_char_p, C.c_int]

@@ -45,7 +45,7 @@ struct mth_handle {
   long long steps = 0;
   bool ghosts_dirty = false;
   bool fused = false;
-  std::map<uint64_t, cudaGraphExec_t> graphs;
+  std::map<std::pair<uint64_t, int>, cudaGraphExec_t> graphs;  // (dt, part; -1 = whole step)
   std::string err;
   // eager per-kernel timing (mth_profile_step)
   struct ProfRec {
@@ -222,15 +222,49 @@ cudaError_t enqueue_ssp3(mth_handle* h, double dt) {
   return c2p(h, h->cons, h->prims, s3 ? h->aux : h->taux, h->prims, h->aux);
 }
 
-// One TimeIntegrator::step, enqueued on the handle's stream.
-cudaError_t enqueue_step(mth_handle* h, double dt) {
+// A time step is split into parts at the points where the reference applies
+// the boundary conditions to an intermediate state (TimeIntegrator::finalise
+// after each stage's recovery): RK2 / RKSplit 2 parts, SSP2 3, SSP3 and
+// SSP2322 1.  An x-slab handle (mth_config.x_slab) runs the parts one at a
+// time and its caller exchanges the slab halos of the part's state between
+// them; every other handle runs all parts inside one step graph.
+int n_parts(const mth_handle* h) {
+  const int integ = h->cfg.integrator;
+  if (integ == MTH_RK2 || integ == MTH_RKSPLIT) return 2;
+  if (integ == MTH_SSP2) return 3;
+  return 1;
+}
+
+// The state a part leaves for the next part's flux (cons, prims, aux).
+void part_state(mth_handle* h, int part, double** c, double** p, double** a) {
+  *c = h->cons;
+  *p = h->prims;
+  *a = h->aux;
+  const int integ = h->cfg.integrator;
+  if ((integ == MTH_RK2 || integ == MTH_RKSPLIT) && part == 0) {
+    *c = h->p1cons;
+    *p = h->p1prims;
+    *a = h->p1aux;
+  } else if (integ == MTH_SSP2 && part == 0) {
+    *c = h->u1;
+  } else if (integ == MTH_SSP2 && part == 1) {
+    *c = h->u2;
+  }
+}
+
+cudaError_t enqueue_ssp2_part(mth_handle* h, double dt, int part);
+
+// Part `part` of one TimeIntegrator::step, enqueued on the handle's stream.
+cudaError_t enqueue_part(mth_handle* h, double dt, int part) {
   cudaError_t e;
   const int integ = h->cfg.integrator;
   if (integ == MTH_RK2 || integ == MTH_RKSPLIT) {
-    // RK2::step (RK2.cc:93-100): predictor, finalise(p1), corrector, finalise.
-    if ((e = flux_stage(h, h->cons, h->prims, h->aux, nullptr, h->p1cons, dt, STAGE_EULER)))
-      return e;
-    if ((e = c2p(h, h->p1cons, h->prims, h->aux, h->p1prims, h->p1aux, true))) return e;
+    // RK2::step (RK2.cc:93-100): predictor, finalise(p1) | corrector, finalise.
+    if (part == 0) {
+      if ((e = flux_stage(h, h->cons, h->prims, h->aux, nullptr, h->p1cons, dt, STAGE_EULER)))
+        return e;
+      return c2p(h, h->p1cons, h->prims, h->aux, h->p1prims, h->p1aux, true);
+    }
     if ((e = flux_stage(h, h->p1cons, h->p1prims, h->p1aux, h->cons, h->cons, dt,
                         STAGE_RK2_CORR)))
       return e;
@@ -247,16 +281,44 @@ cudaError_t enqueue_step(mth_handle* h, double dt) {
     return cudaSuccess;
   }
   if (integ == MTH_SSP3 || integ == MTH_SSP2322) return enqueue_ssp3(h, dt);
-  // SSP2::step (SSP2.cc:53-173).
+  return enqueue_ssp2_part(h, dt, part);
+}
+
+// SSP2::step (SSP2.cc:53-173): implicit stage 1, finalise(U1) | F(U1),
+// implicit stage 2, finalise(U2) | F(U2), combination, finalise.
+cudaError_t enqueue_ssp2_part(mth_handle* h, double dt, int part) {
+  cudaError_t e;
   const bool fast = h->cfg.precision == MTH_MIXED;
-  if ((e = timed(h, fast ? "imex_newton_stage1" : "imex_hybrd_stage1", 29, [&] {
-         return fast ? launch_imex_fast(h->g, 1, h->cons, h->aux, nullptr, nullptr, nullptr,
-                                        h->u1, dt, imex_work(h), h->st)
-                     : launch_imex_stage(h->g, 1, h->cons, h->aux, nullptr, nullptr, nullptr,
-                                         h->u1, dt, imex_work(h), h->st);
-       })))
-    return e;
-  if ((e = c2p(h, h->u1, h->prims, h->aux, h->prims, h->aux, true))) return e;
+  if (part == 0) {
+    if ((e = timed(h, fast ? "imex_newton_stage1" : "imex_hybrd_stage1", 29, [&] {
+           return fast ? launch_imex_fast(h->g, 1, h->cons, h->aux, nullptr, nullptr, nullptr,
+                                          h->u1, dt, imex_work(h), h->st)
+                       : launch_imex_stage(h->g, 1, h->cons, h->aux, nullptr, nullptr, nullptr,
+                                           h->u1, dt, imex_work(h), h->st);
+         })))
+      return e;
+    return c2p(h, h->u1, h->prims, h->aux, h->prims, h->aux, true);
+  }
+  if (part == 2) {
+    // flux2 = F(U2), source2 = S(U2) and the combination (SSP2.cc:150-170) in
+    // one pass: the stage-2 flux tile's epilogue updates cons in place
+    if (h->fused) {
+      if ((e = flux_stage(h, h->u2, h->prims, h->aux, h->cons, h->cons, dt, STAGE_SSP2_FINAL)))
+        return e;
+      return c2p(h, h->cons, h->prims, h->aux, h->prims, h->aux);
+    }
+    if ((e = timed(h, "source", 31, [&] {
+           return launch_source(h->g, h->cfg.model, h->u2, h->aux, h->src2, h->st);
+         })))
+      return e;
+    if ((e = flux_stage(h, h->u2, h->prims, h->aux, nullptr, h->flux2, dt, STAGE_FNET))) return e;
+    if ((e = timed(h, "ssp2_combine", 6.0 * h->NC, [&] {
+           return launch_ssp2_combine(h->g, h->NC, h->cons, h->flux1, h->flux2, h->src1, h->src2,
+                                      dt, h->st);
+         })))
+      return e;
+    return c2p(h, h->cons, h->prims, h->aux, h->prims, h->aux);
+  }
   if ((e = timed(h, "source", 31, [&] {
          return launch_source(h->g, h->cfg.model, h->u1, h->aux, h->src1, h->st);
        })))
@@ -269,25 +331,16 @@ cudaError_t enqueue_step(mth_handle* h, double dt) {
                                          h->u2, dt, imex_work(h), h->st);
        })))
     return e;
-  if ((e = c2p(h, h->u2, h->prims, h->aux, h->prims, h->aux, true))) return e;
-  // flux2 = F(U2), source2 = S(U2) and the combination (SSP2.cc:150-170) in
-  // one pass: the stage-2 flux tile's epilogue updates cons in place
-  if (h->fused) {
-    if ((e = flux_stage(h, h->u2, h->prims, h->aux, h->cons, h->cons, dt, STAGE_SSP2_FINAL)))
-      return e;
-    return c2p(h, h->cons, h->prims, h->aux, h->prims, h->aux);
+  return c2p(h, h->u2, h->prims, h->aux, h->prims, h->aux, true);
+}
+
+// One TimeIntegrator::step, enqueued on the handle's stream.
+cudaError_t enqueue_step(mth_handle* h, double dt) {
+  for (int part = 0; part < n_parts(h); ++part) {
+    cudaError_t e = enqueue_part(h, dt, part);
+    if (e != cudaSuccess) return e;
   }
-  if ((e = timed(h, "source", 31, [&] {
-         return launch_source(h->g, h->cfg.model, h->u2, h->aux, h->src2, h->st);
-       })))
-    return e;
-  if ((e = flux_stage(h, h->u2, h->prims, h->aux, nullptr, h->flux2, dt, STAGE_FNET))) return e;
-  if ((e = timed(h, "ssp2_combine", 6.0 * h->NC, [&] {
-         return launch_ssp2_combine(h->g, h->NC, h->cons, h->flux1, h->flux2, h->src1, h->src2,
-                                    dt, h->st);
-       })))
-    return e;
-  return c2p(h, h->cons, h->prims, h->aux, h->prims, h->aux);
+  return cudaSuccess;
 }
 
 uint64_t dt_key(double dt) {
@@ -296,11 +349,14 @@ uint64_t dt_key(double dt) {
   return k;
 }
 
-mth_status launch_step(mth_handle* h, double dt) {
-  auto it = h->graphs.find(dt_key(dt));
+// The whole step (part -1) or one part of it as a CUDA graph, captured once
+// per distinct dt.
+mth_status launch_step(mth_handle* h, double dt, int part = -1) {
+  const std::pair<uint64_t, int> key(dt_key(dt), part);
+  auto it = h->graphs.find(key);
   cudaGraphExec_t exec = nullptr;
   if (it == h->graphs.end()) {
-    if (h->graphs.size() >= 8) {
+    if (h->graphs.size() >= 16) {
       for (auto& kv : h->graphs) cudaGraphExecDestroy(kv.second);
       h->graphs.clear();
     }
@@ -312,20 +368,20 @@ mth_status launch_step(mth_handle* h, double dt) {
       h->st = work;
       return fail(h, MTH_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(e0));
     }
-    cudaError_t e = enqueue_step(h, dt);
+    cudaError_t e = part < 0 ? enqueue_step(h, dt) : enqueue_part(h, dt, part);
     cudaError_t e2 = cudaStreamEndCapture(h->st, &graph);
     h->st = work;
     if (e != cudaSuccess) return fail(h, MTH_ERR_CUDA, std::string("step: ") + cudaGetErrorString(e));
     if (e2 != cudaSuccess) return fail(h, MTH_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(e2));
     CU(h, cudaGraphInstantiate(&exec, graph, 0));
     cudaGraphDestroy(graph);
-    h->graphs[dt_key(dt)] = exec;
+    h->graphs[key] = exec;
   } else {
     exec = it->second;
   }
   CU(h, cudaGraphLaunch(exec, h->st));
   h->ghosts_dirty = true;
-  h->steps++;
+  if (part < 0 || part == n_parts(h) - 1) h->steps++;
   return MTH_OK;
 }
 
@@ -393,15 +449,24 @@ bool grid_from_config(const void* cfg, Grid* out) {
   g.ks = c.Ng; g.ke = g.Nz - c.Ng;
   if (g.dims < 3) { g.ks = 0; g.ke = 1; }
   if (g.dims < 2) { g.js = 0; g.je = 1; }
-  // Periodic ghost copies must come from interior cells.
-  if ((c.bcs == MTH_PERIODIC || c.bcs == MTH_FLOW) && c.nx < c.Ng) { return false; }
+  // Periodic ghost copies must come from interior cells (in x, an x-slab's
+  // halo rows come from its neighbours' interiors instead).
+  if (c.x_slab) {
+    if (c.nx < c.Ng || c.x_global_nx < c.nx || c.x_offset < 0 ||
+        c.x_offset > c.x_global_nx - c.nx)
+      return false;
+  } else if ((c.bcs == MTH_PERIODIC || c.bcs == MTH_FLOW) && c.nx < c.Ng) {
+    return false;
+  }
   if (c.bcs == MTH_PERIODIC && ((g.dims > 1 && c.ny < c.Ng) || (g.dims > 2 && c.nz < c.Ng))) {
     return false;
   }
-  g.bcx = c.bcs == MTH_OUTFLOW ? DIM_OUTFLOW : DIM_PERIODIC;
+  // an x-slab reads its x halo rows as they are: its caller fills them
+  g.bcx = c.x_slab ? DIM_NONE : (c.bcs == MTH_OUTFLOW ? DIM_OUTFLOW : DIM_PERIODIC);
   g.bcy = g.dims > 1 ? (c.bcs == MTH_PERIODIC ? DIM_PERIODIC : DIM_OUTFLOW) : DIM_NONE;
   g.bcz = g.dims > 2 ? (c.bcs == MTH_PERIODIC ? DIM_PERIODIC : DIM_OUTFLOW) : DIM_NONE;
-  g.dx = (c.xmax - c.xmin) / (c.nx);
+  // an x-slab's cell size is the whole domain's (xmin, xmax are its bounds)
+  g.dx = (c.xmax - c.xmin) / (c.x_slab ? c.x_global_nx : c.nx);
   g.dy = (ymax - ymin) / (c.ny);
   g.dz = (zmax - zmin) / (c.nz);
   g.gamma = c.gamma;
@@ -433,7 +498,9 @@ mth_status mth_create(const mth_config* cfg, mth_handle** out) {
       (c.ny == 0 && c.nz != 0) || c.bcs < 0 || c.bcs > 2 || c.integrator < 0 ||
       c.integrator > 4 || (c.integrator >= MTH_SSP2 && c.model != MTH_SRRMHD) ||
       (c.integrator >= MTH_SSP3 && c.guess != 0) ||
-      c.precision < 0 || c.precision > 1 || c.guess < 0 || c.guess > 1) {
+      c.precision < 0 || c.precision > 1 || c.guess < 0 || c.guess > 1 ||
+      (c.x_slab && c.integrator != MTH_RK2 && c.integrator != MTH_RKSPLIT &&
+       c.integrator != MTH_SSP2)) {
     delete h;
     return MTH_ERR_INVALID;
   }
@@ -672,13 +739,119 @@ mth_status mth_c2p_cells(int model, double gamma, double sigma, long long n, con
 
 mth_status mth_step(mth_handle* h, double dt) {
   if (!h || !(dt > 0)) return fail(h, MTH_ERR_INVALID, "dt must be positive");
+  if (h->cfg.x_slab) return fail(h, MTH_ERR_INVALID, "an x-slab steps by parts (mth_step_part)");
   CU(h, cudaSetDevice(h->device));
   h->dt = dt;
   return launch_step(h, dt);
 }
 
+// ---- x-slab decomposition ----------------------------------------------------
+mth_status mth_step_parts(const mth_handle* h, int* n) {
+  if (!h || !n) return MTH_ERR_INVALID;
+  *n = n_parts(h);
+  return MTH_OK;
+}
+
+mth_status mth_step_part(mth_handle* h, double dt, int part) {
+  if (!h || !(dt > 0) || part < 0 || part >= n_parts(h))
+    return fail(h, MTH_ERR_INVALID, "dt must be positive and part in [0, parts)");
+  CU(h, cudaSetDevice(h->device));
+  h->dt = dt;
+  return launch_step(h, dt, part);
+}
+
+mth_status mth_next_dt(const mth_handle* h, double* dt) {
+  if (!h || !dt) return MTH_ERR_INVALID;
+  *dt = next_dt(h);
+  return MTH_OK;
+}
+
+mth_status mth_advance_time(mth_handle* h, double dt) {
+  if (!h) return MTH_ERR_INVALID;
+  h->t += dt;
+  h->iters++;
+  return MTH_OK;
+}
+
+mth_status mth_halo_bytes(const mth_handle* h, unsigned long long* nbytes) {
+  if (!h || !nbytes) return MTH_ERR_INVALID;
+  const Grid& g = h->g;
+  *nbytes = sizeof(double) * (unsigned long long)(h->NC + h->NP + h->NA) * g.Ng * g.Ny * g.Nz;
+  return MTH_OK;
+}
+
+namespace {
+// Copies Ng x-rows of (cons, prims, aux) of a part's state between the grid
+// (rows starting at `row`) and a packed buffer [var][Ng rows][Ny*Nz].
+mth_status halo_copy(mth_handle* h, int part, int row, void* buf, bool to_buf) {
+  double *c, *p, *a;
+  if (part < 0) {
+    c = h->cons;
+    p = h->prims;
+    a = h->aux;
+  } else {
+    part_state(h, part, &c, &p, &a);
+  }
+  const Grid& g = h->g;
+  const size_t plane = sizeof(double) * (size_t)g.Ny * g.Nz;  // one x-row of one variable
+  const size_t block = plane * g.Ng;
+  char* b = static_cast<char*>(buf);
+  const double* arrs[3] = {c, p, a};
+  const int nv[3] = {h->NC, h->NP, h->NA};
+  for (int q = 0; q < 3; ++q) {
+    char* grid_rows = reinterpret_cast<char*>(const_cast<double*>(arrs[q])) + plane * row;
+    const size_t pitch = sizeof(double) * (size_t)g.Ntot;
+    if (to_buf)
+      CU(h, cudaMemcpy2DAsync(b, block, grid_rows, pitch, block, nv[q], cudaMemcpyDeviceToDevice,
+                              h->st));
+    else
+      CU(h, cudaMemcpy2DAsync(grid_rows, pitch, b, block, block, nv[q], cudaMemcpyDeviceToDevice,
+                              h->st));
+    b += block * nv[q];
+  }
+  return MTH_OK;
+}
+}  // namespace
+
+mth_status mth_halo_pack(mth_handle* h, int part, int side, void* dst) {
+  if (!h || !dst || side < 0 || side > 1 || part < -1 || part >= n_parts(h))
+    return MTH_ERR_INVALID;
+  CU(h, cudaSetDevice(h->device));
+  return halo_copy(h, part, side == 0 ? h->g.is : h->g.ie - h->g.Ng, dst, true);
+}
+
+mth_status mth_halo_unpack(mth_handle* h, int part, int side, const void* src) {
+  if (!h || !src || side < 0 || side > 1 || part < -1 || part >= n_parts(h))
+    return MTH_ERR_INVALID;
+  CU(h, cudaSetDevice(h->device));
+  return halo_copy(h, part, side == 0 ? 0 : h->g.ie, const_cast<void*>(src), false);
+}
+
+mth_status mth_halo_outflow(mth_handle* h, int part, int side) {
+  if (!h || side < 0 || side > 1 || part < -1 || part >= n_parts(h)) return MTH_ERR_INVALID;
+  CU(h, cudaSetDevice(h->device));
+  double *c = h->cons, *p = h->prims, *a = h->aux;
+  if (part >= 0) part_state(h, part, &c, &p, &a);
+  const Grid& g = h->g;
+  const size_t plane = sizeof(double) * (size_t)g.Ny * g.Nz;
+  const size_t pitch = sizeof(double) * (size_t)g.Ntot;
+  const int src_row = side == 0 ? g.is : g.ie - 1, first = side == 0 ? 0 : g.ie;
+  double* arrs[3] = {c, p, a};
+  const int nv[3] = {h->NC, h->NP, h->NA};
+  // Outflow::apply (boundaryConds.cc:5-145) in x: every ghost row copies the
+  // boundary's interior row
+  for (int q = 0; q < 3; ++q) {
+    char* base = reinterpret_cast<char*>(arrs[q]);
+    for (int r = 0; r < g.Ng; ++r)
+      CU(h, cudaMemcpy2DAsync(base + plane * (first + r), pitch, base + plane * src_row, pitch,
+                              plane, nv[q], cudaMemcpyDeviceToDevice, h->st));
+  }
+  return MTH_OK;
+}
+
 mth_status mth_update_time(mth_handle* h, int n) {
   if (!h) return MTH_ERR_INVALID;
+  if (h->cfg.x_slab) return fail(h, MTH_ERR_INVALID, "an x-slab steps by parts (mth_step_part)");
   CU(h, cudaSetDevice(h->device));
   for (int s = 0; s < n; ++s) {
     double dt = next_dt(h);
@@ -809,7 +982,7 @@ mth_status mth_step_host_bytes(mth_handle* h, unsigned long long* h2d, unsigned 
 }
 
 mth_status mth_step_host(mth_handle* h, double* cons, double* prims, double* aux, double dt) {
-  if (!h || !cons || !prims || !aux || !(dt > 0)) return MTH_ERR_INVALID;
+  if (!h || !cons || !prims || !aux || !(dt > 0) || h->cfg.x_slab) return MTH_ERR_INVALID;
   CU(h, cudaSetDevice(h->device));
   unsigned pm, am;
   step_inputs(h, pm, am);
@@ -1028,13 +1201,13 @@ mth_status mth_save_text(mth_handle* h, const char* dir, const char* app, int wh
     ymin = -1e20;
     ymax = 1e20;
   }
-  const double dx = (c.xmax - c.xmin) / (c.nx), dy = (ymax - ymin) / (c.ny),
-               dz = (zmax - zmin) / (c.nz);
+  const double dx = g.dx, dy = (ymax - ymin) / (c.ny), dz = (zmax - zmin) / (c.nz);
+  const int x0 = c.x_slab ? c.x_offset : 0;  // an x-slab writes its own columns
   if (which & MTH_SAVE_DOMAIN) {
     const std::string fname = std::string(dir) + "/Domain/domain" + app + ".dat";
     FILE* f = std::fopen(fname.c_str(), "w");
     if (!f) return fail(h, MTH_ERR_INVALID, "could not open " + fname + " for writing");
-    for (int i = 0; i < g.Nx; ++i) std::fprintf(f, "%.16f ", c.xmin + (i + 0 + 0.5 - c.Ng) * dx);
+    for (int i = 0; i < g.Nx; ++i) std::fprintf(f, "%.16f ", c.xmin + (i + x0 + 0.5 - c.Ng) * dx);
     std::fprintf(f, "\n");
     for (int j = 0; j < g.Ny; ++j) std::fprintf(f, "%.16f ", ymin + (j + 0 + 0.5 - c.Ng) * dy);
     std::fprintf(f, "\n");
