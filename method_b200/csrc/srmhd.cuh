@@ -18,7 +18,7 @@ constexpr int NC = 9, NP = 8, NA = 13;
 // p + b^2/2 are formed once per cell instead of once per term.
 __device__ __forceinline__ void flux_fast(const float* c, const float* p, const float* a, int dir,
                                           float* f) {
-  const float iW = __frcp_rn(a[1]);
+  const float iW = __fdividef(1.0f, a[1]);
   const float pt = fmaf(a[8], 0.5f, p[4]);
   if (dir == 0) {
     const float bw = p[5] * iW;

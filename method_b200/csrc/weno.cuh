@@ -81,26 +81,39 @@ __device__ __forceinline__ double weno5_exact(double v0, double v1, double v2, d
 
 // FP32 forms: the upwind (.x) and downwind (.y) reconstructions of one face
 // in FP32x2 arithmetic (sm_100 __ffma2_rn / __fadd2_rn / __fmul2_rn: one
-// instruction for both sides, each lane rounded as the scalar operation);
-// the reciprocals stay scalar.  Linear weights are taken times 3 (WENO3) and
-// times 10 (WENO5), and the WENO5 Jiang-Shu indicators times 4,
-// 13/3 (a - 2b + c)^2 + (.)^2, with eps times 16: none of these scalings
-// changes the normalised weights.
+// instruction for both sides, each lane rounded as the scalar operation).
+// Linear weights are taken times 3 (WENO3) and times 10 (WENO5), and the
+// WENO5 Jiang-Shu indicators times 4, 13/3 (a - 2b + c)^2 + (.)^2, with eps
+// times 16: none of these scalings changes the normalised weights.
+//
+// One reciprocal per side: with q_k = eps + beta_k^2 the weights
+// (d_k / q_k) / sum_j (d_j / q_j) equal d_k P_k / sum_j d_j P_j with P_k the
+// product of the other stencils' q (WENO5; for WENO3 simply the other q), so
+// only the final normalisation divides.  WENO5 first scales the three q by
+// the power of two that brings the largest into [1, 2) (exponent bits only,
+// exact), so the products neither overflow for large flux jumps nor
+// underflow below the largest weight's scale.
 __device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
 
 __device__ __forceinline__ float2 rcp2(float2 q) {
   return make_float2(__fdividef(1.0f, q.x), __fdividef(1.0f, q.y));
 }
 
+// 2^-floor(log2 m) for a positive normal m below 2^126, from the exponent bits.
+__device__ __forceinline__ float pow2_inv(float m) {
+  return __int_as_float(0x7F000000 - (__float_as_int(m) & 0x7F800000));
+}
+
 __device__ __forceinline__ float2 weno3_fast2(float2 v0, float2 v1, float2 v2) {
   const float2 d0 = __ffma2_rn(f2(-1.0f), v0, v1), d1 = __ffma2_rn(f2(-1.0f), v1, v2);
   const float2 b0 = __fmul2_rn(d0, d0), b1 = __fmul2_rn(d1, d1);
-  const float2 a0 = rcp2(__ffma2_rn(b0, b0, f2(1e-16f)));
-  const float2 a1 = __fmul2_rn(f2(2.0f), rcp2(__ffma2_rn(b1, b1, f2(1e-16f))));
+  const float2 q0 = __ffma2_rn(b0, b0, f2(1e-16f)), q1 = __ffma2_rn(b1, b1, f2(1e-16f));
   const float2 s0 = __ffma2_rn(f2(1.5f), v1, __fmul2_rn(f2(-0.5f), v0));
   const float2 s1 = __fmul2_rn(f2(0.5f), __fadd2_rn(v2, v1));
-  const float2 num = __ffma2_rn(a0, s0, __fmul2_rn(a1, s1));
-  return __fmul2_rn(num, rcp2(__fadd2_rn(a0, a1)));
+  // weights 1/q0 : 2/q1  =  q1 : 2 q0
+  const float2 a1 = __fmul2_rn(f2(2.0f), q0);
+  const float2 num = __ffma2_rn(q1, s0, __fmul2_rn(a1, s1));
+  return __fmul2_rn(num, rcp2(__fadd2_rn(q1, a1)));
 }
 
 __device__ __forceinline__ float2 weno5_fast2(float2 v0, float2 v1, float2 v2, float2 v3,
@@ -115,9 +128,18 @@ __device__ __forceinline__ float2 weno5_fast2(float2 v0, float2 v1, float2 v2, f
   const float2 b0 = __ffma2_rn(__fmul2_rn(c13, t0), t0, __fmul2_rn(u0, u0));
   const float2 b1 = __ffma2_rn(__fmul2_rn(c13, t1), t1, __fmul2_rn(u1, u1));
   const float2 b2 = __ffma2_rn(__fmul2_rn(c13, t2), t2, __fmul2_rn(u2, u2));
-  const float2 a0 = rcp2(__ffma2_rn(b0, b0, f2(16e-16f)));
-  const float2 a1 = __fmul2_rn(f2(6.0f), rcp2(__ffma2_rn(b1, b1, f2(16e-16f))));
-  const float2 a2 = __fmul2_rn(f2(3.0f), rcp2(__ffma2_rn(b2, b2, f2(16e-16f))));
+  float2 q0 = __ffma2_rn(b0, b0, f2(16e-16f));
+  float2 q1 = __ffma2_rn(b1, b1, f2(16e-16f));
+  float2 q2 = __ffma2_rn(b2, b2, f2(16e-16f));
+  const float2 sc = make_float2(pow2_inv(fmaxf(fmaxf(q0.x, q1.x), q2.x)),
+                                pow2_inv(fmaxf(fmaxf(q0.y, q1.y), q2.y)));
+  q0 = __fmul2_rn(q0, sc);
+  q1 = __fmul2_rn(q1, sc);
+  q2 = __fmul2_rn(q2, sc);
+  // linear weights 1 : 6 : 3 (x10) over q0 : q1 : q2, times q0 q1 q2
+  const float2 a0 = __fmul2_rn(q1, q2);
+  const float2 a1 = __fmul2_rn(__fmul2_rn(f2(6.0f), q0), q2);
+  const float2 a2 = __fmul2_rn(__fmul2_rn(f2(3.0f), q0), q1);
   // candidate stencils at the face, the 1/6 folded into the coefficients
   const float2 c3 = f2(1.0f / 3.0f), c6 = f2(-1.0f / 6.0f), c56 = f2(5.0f / 6.0f);
   const float2 s0 = __ffma2_rn(f2(11.0f / 6.0f), v2,

@@ -29,6 +29,7 @@ process).
 """
 from __future__ import annotations
 
+import contextlib
 import ctypes as C
 
 import numpy as np
@@ -99,14 +100,17 @@ class ArraySlab:
         for a in self.arrays:
             a[:, first:first + self.Ng] = a[:, src:src + 1]
 
-    def wait(self):
-        pass
+    def on_stream(self):
+        return contextlib.nullcontext()
 
 
 class DeviceSlab:
-    """A slab as a library handle (``Simulation`` created with x_slab)."""
+    """A slab as a library handle (``Simulation`` created with x_slab).  The
+    handle's work, its halo copies and the transport's copies or messages all
+    run on `stream`, a non-default torch stream that the slabs of one process
+    share, so they are ordered without host synchronisation."""
 
-    def __init__(self, sim, torch):
+    def __init__(self, sim, torch, stream):
         self.sim, self.torch = sim, torch
         n = C.c_ulonglong()
         self._check(sim.L.mth_halo_bytes(sim.h, C.byref(n)), "halo_bytes")
@@ -115,8 +119,11 @@ class DeviceSlab:
         self._check(sim.L.mth_step_parts(sim.h, C.byref(parts)), "step_parts")
         self.parts = parts.value
         self.device = torch.device("cuda", sim.cfg.device)
-        self.stream = torch.cuda.current_stream(self.device)
-        sim.set_stream(self.stream.cuda_stream)
+        self.stream = stream
+        sim.set_stream(stream.cuda_stream)
+
+    def on_stream(self):
+        return self.torch.cuda.stream(self.stream)
 
     def _check(self, rc, what):
         if rc != 0:
@@ -134,8 +141,6 @@ class DeviceSlab:
     def outflow(self, part, side):
         self._check(self.sim.L.mth_halo_outflow(self.sim.h, part, side), "outflow")
 
-    def wait(self):
-        self.stream.synchronize()
 
 
 # ---------------------------------------------------------------- transports
@@ -152,24 +157,24 @@ class TorchTransport:
         send, recv = b
         slab.pack(part, 0, send[0])
         slab.pack(part, 1, send[1])
-        if self.world == 1:
-            if self.left is not None:  # periodic: the slab is its own neighbour
-                recv[0][:] = send[1]
-                recv[1][:] = send[0]
-        else:
-            slab.wait()  # packed rows complete before the messages leave
-            ops = []
-            P2P = self.dist.P2POp
-            if self.left is not None:
-                ops.append(P2P(self.dist.isend, send[0], self.left, tag=1))
-            if self.right is not None:
-                ops.append(P2P(self.dist.irecv, recv[1], self.right, tag=1))
-                ops.append(P2P(self.dist.isend, send[1], self.right, tag=0))
-            if self.left is not None:
-                ops.append(P2P(self.dist.irecv, recv[0], self.left, tag=0))
-            if ops:
-                for req in self.dist.batch_isend_irecv(ops):
-                    req.wait()
+        with slab.on_stream():  # messages and copies ordered after the packs
+            if self.world == 1:
+                if self.left is not None:  # periodic: the slab is its own neighbour
+                    recv[0].copy_(send[1])
+                    recv[1].copy_(send[0])
+            else:
+                ops = []
+                P2P = self.dist.P2POp
+                if self.left is not None:
+                    ops.append(P2P(self.dist.isend, send[0], self.left, tag=1))
+                if self.right is not None:
+                    ops.append(P2P(self.dist.irecv, recv[1], self.right, tag=1))
+                    ops.append(P2P(self.dist.isend, send[1], self.right, tag=0))
+                if self.left is not None:
+                    ops.append(P2P(self.dist.irecv, recv[0], self.left, tag=0))
+                if ops:
+                    for req in self.dist.batch_isend_irecv(ops):
+                        req.wait()
         for side, nb in ((0, self.left), (1, self.right)):
             if nb is None:
                 slab.outflow(part, side)
@@ -193,12 +198,14 @@ class LocalTransport:
             if left is None:
                 slab.outflow(part, 0)
             else:
-                recv[0][:] = bufs[left][0][1]  # the left slab's high rows
+                with slab.on_stream():
+                    recv[0].copy_(bufs[left][0][1])  # the left slab's high rows
                 slab.unpack(part, 0, recv[0])
             if right is None:
                 slab.outflow(part, 1)
             else:
-                recv[1][:] = bufs[right][0][0]  # the right slab's low rows
+                with slab.on_stream():
+                    recv[1].copy_(bufs[right][0][0])  # the right slab's low rows
                 slab.unpack(part, 1, recv[1])
 
 
@@ -219,10 +226,11 @@ class SlabDomain:
         self.ranks = list(ranks)
         self.transport = transport
         self.slabs = []
+        self.stream = torch.cuda.Stream(device=device)
         for r in self.ranks:
             off, n = self.extents[r]
             kw = dict(self.cfg, nx=n, x_slab=(off, cfg["nx"]), device=device)
-            self.slabs.append(DeviceSlab(mb.Simulation(**kw), torch))
+            self.slabs.append(DeviceSlab(mb.Simulation(**kw), torch, self.stream))
         self.bufs = [((s.new_buffer(), s.new_buffer()), (s.new_buffer(), s.new_buffer()))
                      for s in self.slabs]
         self.parts = self.slabs[0].parts
