@@ -211,6 +211,7 @@ typedef struct {
   int batch;            /* samples per step (multiple of 128 recommended) */
   float lr;             /* peak learning rate, cosine decay */
   double gamma;         /* adiabatic index */
+  int model;            /* MTH_SRMHD (default) or MTH_SRRMHD: which feature map and pairs */
 } mth_mlp_train_config;
 /* Trains on the device with the project's forward/backward kernels. */
 mth_status mth_mlp_train(const mth_mlp_train_config* cfg, float* params, float* stats,
@@ -227,7 +228,17 @@ mth_status mth_mlp_forward(const float* params, int n, const float* x, float* y,
  * (copies use unified addressing). */
 mth_status mth_mlp_make_pairs(long long n, unsigned long long seed, double gamma, float* feat,
                               float* tgt, double* cons, double* prims, int device);
-/* Installs a trained network in a handle (precision MTH_MIXED, guess MTH_GUESS_MLP). */
+/* The same for SRRMHD: random primitive states (the distributions above,
+ * plus E = -v x B + a departure of 10^U(-3,0) |B|) through SRRMHD primsToAll;
+ * conserved [14][n], primitive [11][n]. */
+mth_status mth_mlp_make_pairs_srrmhd(long long n, unsigned long long seed, double gamma,
+                                     float* feat, float* tgt, double* cons, double* prims,
+                                     int device);
+/* Installs a trained network in a handle (precision MTH_MIXED, guess
+ * MTH_GUESS_MLP); it must have been trained for the handle's model.  SRMHD:
+ * Newton recovery starts from its Z; SRRMHD: the recovery and the implicit
+ * stages' inner recoveries start from its Z (the previous state's Z is the
+ * fallback, then the reference secant / Powell-hybrid solve). */
 mth_status mth_set_mlp(mth_handle* h, const float* params, const float* stats);
 
 /* Batched SRMHD primitive recovery of n independent cells (device arrays,
@@ -339,6 +350,9 @@ mth_status mth_ensemble_download(mth_ensemble* e, int m, double* cons, double* p
  * every primitive recovery from its guess, as mth_set_mlp does for one
  * simulation. */
 mth_status mth_ensemble_set_mlp(mth_ensemble* e, const float* params, const float* stats);
+/* The same for the SRRMHD members: a network trained with model MTH_SRRMHD
+ * seeds their recoveries and the inner recoveries of their implicit stages. */
+mth_status mth_ensemble_set_mlp_srrmhd(mth_ensemble* e, const float* params, const float* stats);
 mth_status mth_ensemble_set_stream(mth_ensemble* e, void* stream);
 /* Times tile heights 4, 8, 16 (rows of 32 cells per flux tile) for each
  * member size class (nx <= 96, <= 192, larger) on the ensemble's first flux

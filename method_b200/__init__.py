@@ -253,13 +253,13 @@ class Simulation:
 
 
 def train_guess(seed=7, n_samples=1 << 19, iterations=4000, batch=8192, lr=3e-3,
-                gamma=4.0 / 3.0, device=0):
-    """Trains the C2P guess network on the GPU on (conserved -> primitive)
-    pairs the solver generates (mth_mlp_train).  Returns (params, stats,
-    final loss) for Simulation.set_mlp / Ensemble.set_mlp."""
+                gamma=4.0 / 3.0, device=0, model="srmhd"):
+    """Trains the C2P guess network of `model` on the GPU on (conserved ->
+    primitive) pairs the solver generates (mth_mlp_train).  Returns (params,
+    stats, final loss) for Simulation.set_mlp / Ensemble.set_mlp."""
     L = _lib.load()
     cfg = _lib.MlpTrainConfig(seed=seed, n_samples=n_samples, iterations=iterations, batch=batch,
-                              lr=lr, gamma=gamma)
+                              lr=lr, gamma=gamma, model=MODELS[model])
     P = np.zeros(_lib.MLP_NPARAM, dtype=np.float32)
     S = np.zeros(_lib.MLP_NSTAT, dtype=np.float32)
     loss = np.zeros(1, dtype=np.float32)
@@ -364,13 +364,14 @@ class Ensemble:
         return [dict(name=out[i].name.decode(), launches=out[i].launches,
                      total_ms=out[i].total_ms) for i in range(min(n.value, 64))]
 
-    def set_mlp(self, params, stats):
-        """Installs a trained C2P guess network (members created with guess='mlp')."""
+    def set_mlp(self, params, stats, model="srmhd"):
+        """Installs a trained C2P guess network for the members of `model`
+        (members created with guess='mlp')."""
         params = np.ascontiguousarray(params, dtype=np.float32)
         stats = np.ascontiguousarray(stats, dtype=np.float32)
         F = C.POINTER(C.c_float)
-        self._check(self.L.mth_ensemble_set_mlp(self.e, params.ctypes.data_as(F),
-                                                stats.ctypes.data_as(F)), "set_mlp")
+        fn = self.L.mth_ensemble_set_mlp if model == "srmhd" else self.L.mth_ensemble_set_mlp_srrmhd
+        self._check(fn(self.e, params.ctypes.data_as(F), stats.ctypes.data_as(F)), "set_mlp")
 
     def set_stream(self, stream_ptr):
         self._check(self.L.mth_ensemble_set_stream(self.e, stream_ptr), "set_stream")

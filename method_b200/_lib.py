@@ -25,11 +25,11 @@ SYMBOLS = [
     "mth_get_stats", "mth_reset_stats", "mth_step_host", "mth_step_host_bytes", "mth_pin_host",
     "mth_unpin_host",
     "mth_set_stream", "mth_profile_step", "mth_mlp_train", "mth_mlp_grad", "mth_mlp_forward",
-    "mth_mlp_make_pairs", "mth_set_mlp", "mth_c2p_batch", "mth_c2p_ctx_create", "mth_c2p_ctx_destroy",
+    "mth_mlp_make_pairs", "mth_mlp_make_pairs_srrmhd", "mth_set_mlp", "mth_c2p_batch", "mth_c2p_ctx_create", "mth_c2p_ctx_destroy",
     "mth_c2p_ctx_set_mlp", "mth_c2p_ctx_run", "mth_c2p_ctx_stats", "mth_c2p_srmhd_noalloc",
     "mth_save_text", "mth_device_state", "mth_ensemble_create", "mth_ensemble_destroy",
     "mth_ensemble_last_error", "mth_ensemble_set_prims", "mth_ensemble_download",
-    "mth_ensemble_set_mlp", "mth_ensemble_set_stream", "mth_ensemble_autotune", "mth_ensemble_step",
+    "mth_ensemble_set_mlp", "mth_ensemble_set_mlp_srrmhd", "mth_ensemble_set_stream", "mth_ensemble_autotune", "mth_ensemble_step",
     "mth_ensemble_profile", "mth_ensemble_sync", "mth_ensemble_stats", "mth_ensemble_info",
 ]
 
@@ -39,7 +39,7 @@ MLP_NSTAT = 20
 
 class MlpTrainConfig(C.Structure):
     _fields_ = [("seed", C.c_ulonglong), ("n_samples", C.c_longlong), ("iterations", C.c_int),
-                ("batch", C.c_int), ("lr", C.c_float), ("gamma", C.c_double)]
+                ("batch", C.c_int), ("lr", C.c_float), ("gamma", C.c_double), ("model", C.c_int)]
 
 
 class C2PBatchStats(C.Structure):
@@ -131,6 +131,8 @@ def load():
     L.mth_mlp_grad.argtypes = [F, C.c_int, F, F, F, F, C.c_int]
     L.mth_mlp_forward.argtypes = [F, C.c_int, F, F, C.c_int]
     L.mth_mlp_make_pairs.argtypes = [C.c_longlong, C.c_ulonglong, C.c_double, F, F, D, D, C.c_int]
+    L.mth_mlp_make_pairs_srrmhd.argtypes = [C.c_longlong, C.c_ulonglong, C.c_double, F, F, D, D,
+                                            C.c_int]
     L.mth_set_mlp.argtypes = [H, F, F]
     L.mth_c2p_batch.argtypes = [C.c_double, C.c_longlong, C.c_void_p, C.c_void_p, C.c_void_p,
                                 C.c_int, C.c_int, F, F, C.c_void_p, C.POINTER(C2PBatchStats)]
@@ -151,6 +153,7 @@ def load():
     L.mth_ensemble_set_prims.argtypes = [E, C.c_int, D]
     L.mth_ensemble_download.argtypes = [E, C.c_int, D, D, D]
     L.mth_ensemble_set_mlp.argtypes = [E, F, F]
+    L.mth_ensemble_set_mlp_srrmhd.argtypes = [E, F, F]
     L.mth_ensemble_set_stream.argtypes = [E, C.c_void_p]
     L.mth_ensemble_autotune.argtypes = [E, C.c_int, C.POINTER(C.c_int)]
     L.mth_ensemble_step.argtypes = [E, C.c_int]

@@ -103,6 +103,12 @@ cudaError_t timed(mth_handle* h, const char* name, double doubles_per_cell,
 
 C2PWork c2p_work(mth_handle* h) { return C2PWork{h->fail_list, h->fail_count, h->counters}; }
 C2PWork imex_work(mth_handle* h) { return C2PWork{h->fail_list, h->fail_count, h->counters + 4}; }
+// The guess network of an SRRMHD handle with MTH_GUESS_MLP, for its implicit stages.
+const MixedWork* mlp_work(const mth_handle* h) {
+  return (h->cfg.model == MTH_SRRMHD && h->cfg.guess == MTH_GUESS_MLP && h->mixed.has_mlp)
+             ? &h->mixed
+             : nullptr;
+}
 
 size_t bytes(const mth_handle* h, int nv) { return sizeof(double) * (size_t)nv * h->g.Ntot; }
 
@@ -292,7 +298,7 @@ cudaError_t enqueue_ssp2_part(mth_handle* h, double dt, int part) {
   if (part == 0) {
     if ((e = timed(h, fast ? "imex_newton_stage1" : "imex_hybrd_stage1", 29, [&] {
            return fast ? launch_imex_fast(h->g, 1, h->cons, h->aux, nullptr, nullptr, nullptr,
-                                          h->u1, dt, imex_work(h), h->st)
+                                          h->u1, dt, imex_work(h), h->st, mlp_work(h))
                        : launch_imex_stage(h->g, 1, h->cons, h->aux, nullptr, nullptr, nullptr,
                                            h->u1, dt, imex_work(h), h->st);
          })))
@@ -326,7 +332,7 @@ cudaError_t enqueue_ssp2_part(mth_handle* h, double dt, int part) {
   if ((e = flux_stage(h, h->u1, h->prims, h->aux, nullptr, h->flux1, dt, STAGE_FNET))) return e;
   if ((e = timed(h, fast ? "imex_newton_stage2" : "imex_hybrd_stage2", 71, [&] {
          return fast ? launch_imex_fast(h->g, 2, h->cons, h->aux, h->u1, h->flux1, h->src1,
-                                        h->u2, dt, imex_work(h), h->st)
+                                        h->u2, dt, imex_work(h), h->st, mlp_work(h))
                      : launch_imex_stage(h->g, 2, h->cons, h->aux, h->u1, h->flux1, h->src1,
                                          h->u2, dt, imex_work(h), h->st);
        })))

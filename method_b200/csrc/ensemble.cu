@@ -60,10 +60,13 @@ struct mth_ensemble {
   int grid_cells = 148 * 8;
   int grid_mlp = 148 * 2;
   bool has_model[2] = {false, false};
-  int guess = MTH_GUESS_PREVIOUS;  // MTH_GUESS_MLP: SRMHD members use the network
-  float* mlp_params = nullptr;     // device, MLP_NPARAM
+  int guess = MTH_GUESS_PREVIOUS;  // MTH_GUESS_MLP: members use their model's network
+  float* mlp_params = nullptr;     // device, MLP_NPARAM: SRMHD network
   float* mlp_stats = nullptr;      // device, MLP_NSTAT
   bool has_mlp = false;
+  float* mlp_params_r = nullptr;   // SRRMHD network
+  float* mlp_stats_r = nullptr;
+  bool has_mlp_r = false;
   cudaStream_t own = nullptr, st = nullptr;
   cudaStream_t side = nullptr;  // second branch of the captured step
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
@@ -176,6 +179,12 @@ cudaError_t flux_phase(mth_ensemble* e, cudaStream_t s, int md, int ic, int ip, 
   return cudaSuccess;
 }
 
+// 1 when members of model `md` start their solves from the learned guess.
+int net_mode(const mth_ensemble* e, int md) {
+  if (e->guess != MTH_GUESS_MLP) return 0;
+  return (md == MODEL_SRMHD ? e->has_mlp : e->has_mlp_r) ? 1 : 0;
+}
+
 // lean: an intermediate recovered state (RK2 predictor, SSP2 stage) that only
 // the next flux, source and implicit solve read (mixed form: only their
 // inputs are written).
@@ -185,11 +194,13 @@ cudaError_t c2p_phase(mth_ensemble* e, cudaStream_t s, int md, int ic, int ipg, 
   if (!n) return cudaSuccess;
   const int grid = std::max(1, std::min(n, e->grid_cells));
   if (e->precision == MTH_MIXED) {
-    const int gm = (md == MODEL_SRMHD && e->guess == MTH_GUESS_MLP && e->has_mlp) ? 1 : 0;
+    const int gm = net_mode(e, md);
     if (gm) {
       cudaError_t r = phase(e, s, "mlp_zguess", [&] {
-        return ens_mlp_zguess(e->d_mem, e->d_cells[md], n, ic, e->mlp_params, e->mlp_stats,
-                              e->grid_mlp, s);
+        return ens_mlp_zguess(e->d_mem, e->d_cells[md], n, ic,
+                              md == MODEL_SRMHD ? e->mlp_params : e->mlp_params_r,
+                              md == MODEL_SRMHD ? e->mlp_stats : e->mlp_stats_r, e->grid_mlp, s,
+                              md);
       });
       if (r != cudaSuccess) return r;
     }
@@ -223,10 +234,22 @@ cudaError_t srrmhd_ssp2(mth_ensemble* e, cudaStream_t s) {
   const int grid = std::max(1, std::min(n, e->grid_cells));
   Item* it = e->d_cells[md];
   cudaError_t r;
+  const int gm = net_mode(e, md);
   for (int stage = 1; stage <= 2; ++stage) {
     const int u = stage == 1 ? EA_U1 : EA_U2;
+    if (gm) {  // the network's Z for the stage's first iterate (its explicit part)
+      if (stage == 2 && (r = phase(e, s, "imex_explicit_part", [&] {
+                           return ens_imex_explicit_part2(e->d_mem, it, n, grid, s);
+                         })))
+        return r;
+      if ((r = phase(e, s, "mlp_zguess", [&] {
+             return ens_mlp_zguess(e->d_mem, it, n, stage == 1 ? EA_CONS : EA_U2, e->mlp_params_r,
+                                   e->mlp_stats_r, e->grid_mlp, s, MODEL_SRRMHD);
+           })))
+        return r;
+    }
     if ((r = phase(e, s, "imex_newton", [&] {
-           return ens_imex_fast(e->d_mem, it, n, stage, grid, s);
+           return ens_imex_fast(e->d_mem, it, n, stage, grid, s, gm);
          })))
       return r;
     if ((r = phase(e, s, "imex_queued", [&] { return ens_imex_queued(e->d_mem, e->n, stage, s); })))
@@ -346,7 +369,7 @@ mth_status mth_ensemble_create(const mth_config* cfgs, int n, mth_ensemble** out
                                  d.model == MTH_SRRMHD, d.model == MTH_SRRMHD,
                                  d.model == MTH_SRRMHD, d.model == MTH_SRRMHD,
                                  d.model == MTH_SRMHD,
-                                 d.model == MTH_SRMHD && e->guess == MTH_GUESS_MLP};
+                                 e->guess == MTH_GUESS_MLP};
     for (int a = 0; a < EA_COUNT; ++a) {
       d.a[a] = nullptr;
       if (need[a] && (r = dalloc(e, (void**)&d.a[a], nbytes(d.g, sizes[a])))) return bail(r);
@@ -358,6 +381,8 @@ mth_status mth_ensemble_create(const mth_config* cfgs, int n, mth_ensemble** out
   if ((r = dalloc(e, (void**)&e->d_mem, sizeof(Member) * n))) return bail(r);
   if ((r = dalloc(e, (void**)&e->mlp_params, sizeof(float) * MLP_NPARAM))) return bail(r);
   if ((r = dalloc(e, (void**)&e->mlp_stats, sizeof(float) * 32))) return bail(r);
+  if ((r = dalloc(e, (void**)&e->mlp_params_r, sizeof(float) * MLP_NPARAM))) return bail(r);
+  if ((r = dalloc(e, (void**)&e->mlp_stats_r, sizeof(float) * 32))) return bail(r);
   if ((r = cudaMemcpyAsync(e->d_mem, e->mem.data(), sizeof(Member) * n, cudaMemcpyHostToDevice,
                            e->st)))
     return bail(r);
@@ -449,18 +474,28 @@ mth_status mth_ensemble_download(mth_ensemble* e, int m, double* cons, double* p
   return MTH_OK;
 }
 
-mth_status mth_ensemble_set_mlp(mth_ensemble* e, const float* params, const float* stats) {
+namespace {
+mth_status set_network(mth_ensemble* e, int md, const float* params, const float* stats) {
   if (!e || !params || !stats || e->guess != MTH_GUESS_MLP) return MTH_ERR_INVALID;
   ECU(e, cudaSetDevice(e->device));
-  ECU(e, cudaMemcpyAsync(e->mlp_params, params, sizeof(float) * MLP_NPARAM,
-                         cudaMemcpyHostToDevice, e->st));
-  ECU(e, cudaMemcpyAsync(e->mlp_stats, stats, sizeof(float) * MLP_NSTAT, cudaMemcpyHostToDevice,
-                         e->st));
+  float* P = md == MODEL_SRMHD ? e->mlp_params : e->mlp_params_r;
+  float* S = md == MODEL_SRMHD ? e->mlp_stats : e->mlp_stats_r;
+  ECU(e, cudaMemcpyAsync(P, params, sizeof(float) * MLP_NPARAM, cudaMemcpyHostToDevice, e->st));
+  ECU(e, cudaMemcpyAsync(S, stats, sizeof(float) * MLP_NSTAT, cudaMemcpyHostToDevice, e->st));
   ECU(e, cudaStreamSynchronize(e->st));
-  e->has_mlp = true;
+  (md == MODEL_SRMHD ? e->has_mlp : e->has_mlp_r) = true;
   if (e->graph) cudaGraphExecDestroy(e->graph);
   e->graph = nullptr;
   return MTH_OK;
+}
+}  // namespace
+
+mth_status mth_ensemble_set_mlp(mth_ensemble* e, const float* params, const float* stats) {
+  return set_network(e, MODEL_SRMHD, params, stats);
+}
+
+mth_status mth_ensemble_set_mlp_srrmhd(mth_ensemble* e, const float* params, const float* stats) {
+  return set_network(e, MODEL_SRRMHD, params, stats);
 }
 
 mth_status mth_ensemble_set_stream(mth_ensemble* e, void* stream) {

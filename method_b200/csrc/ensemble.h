@@ -20,7 +20,7 @@ enum EnsArray : int {
   EA_P1C, EA_P1P, EA_P1A,            // RK2 predictor state
   EA_U1, EA_U2, EA_F1, EA_S1,        // SSP2 stages (F(U2), S(U2) stay in registers)
   EA_SOL,                            // SRMHD C2P solution (2 planes)
-  EA_ZG,                             // SRMHD learned guess (Z, v^2 planes)
+  EA_ZG,                             // learned guess (Z, v^2 planes)
   EA_COUNT
 };
 
@@ -58,18 +58,23 @@ cudaError_t ens_advance(Member* mem, int n_members, cudaStream_t st);
 cudaError_t ens_fvs_fp32(const Member* mem, const Item* items, int n_items, int model, int order,
                          int TI, int ic, int ip, int ia, int iu0, int iout, int mode, int grid,
                          cudaStream_t st);
-// guess_mode 1: SRMHD members start Newton from the learned guess in EA_ZG.
+// guess_mode 1: members start Newton from the learned guess in EA_ZG.
 // lean: write only what the stage's flux, source and next implicit solve read
 // (SRMHD: prims 1-7, aux 1 and 4-8, no solution; SRRMHD: prims 1-4, aux 4-8
 // and 10), for the intermediate recovered states of RK2 and SSP2.
 cudaError_t ens_c2p_newton(const Member* mem, const Item* items, int n_items, int model,
                            int guess_mode, int ic, int ipg, int iag, int ip, int ia, bool lean,
                            int grid, cudaStream_t st);
+// guess_mode 1: the inner recoveries start from the learned guess in EA_ZG.
 cudaError_t ens_imex_fast(const Member* mem, const Item* items, int n_items, int stage, int grid,
-                          cudaStream_t st);
-// ---- guess network (mlp.cu): EA_ZG of the SRMHD members from state `ic`.
+                          cudaStream_t st, int guess_mode = 0);
+// Stage 2's explicit part of every SRRMHD member into EA_U2 (the network's input).
+cudaError_t ens_imex_explicit_part2(const Member* mem, const Item* items, int n_items, int grid,
+                                    cudaStream_t st);
+// ---- guess network (mlp.cu): EA_ZG of one model's members from state `ic`.
 cudaError_t ens_mlp_zguess(const Member* mem, const Item* items, int n_items, int ic,
-                           const float* params, const float* stats, int grid, cudaStream_t st);
+                           const float* params, const float* stats, int grid, cudaStream_t st,
+                           int model = 0);
 
 constexpr int ENS_CHUNK = 128;  // cells per cell-phase work item (= CTA size)
 

@@ -308,7 +308,8 @@ __device__ __forceinline__ void c2p_srrmhd_newton_cell(const Grid& g, long long 
                                                        const double* __restrict__ cons,
                                                        const double* aux_guess, double* prims,
                                                        double* aux, NewtonTally& tl,
-                                                       long long* counters) {
+                                                       long long* counters,
+                                                       const double* zseed = nullptr) {
   const long long N = g.Ntot;
   double c[14], p[11], a[17];
 #pragma unroll
@@ -323,9 +324,14 @@ __device__ __forceinline__ void c2p_srrmhd_newton_cell(const Grid& g, long long 
   a[14] = c[3] - (c[8] * c[6] - c[9] * c[5]);
   a[15] = a[12] * a[12] + a[13] * a[13] + a[14] * a[14];
   a[16] = c[4] - 0.5 * (a[7] + a[8]);
-  double Z = aux_guess[10 * N + cell];
+  double Z = zseed ? zseed[cell] : aux_guess[10 * N + cell];
   int it = 0;
   bool ok = newton_srrmhd(a[15], c[0], a[16], gm, Z, it);
+  if (!ok && zseed) {  // the network's Z failed: the previous state's, as without it
+    tl.fb_prev += 1;
+    Z = aux_guess[10 * N + cell];
+    ok = newton_srrmhd(a[15], c[0], a[16], gm, Z, it);
+  }
   bool bad = false;
   if (!ok) {
     tl.fb_hybrd += 1;
@@ -375,14 +381,14 @@ __device__ __forceinline__ void c2p_srrmhd_newton_cell(const Grid& g, long long 
 template <bool LEAN>
 __global__ void __launch_bounds__(128, kNewtonMinBlocks)
     k_c2p_newton_srrmhd(Grid g, const double* __restrict__ cons, const double* aux_guess,
-                        double* prims, double* aux, C2PWork w) {
+                        double* prims, double* aux, C2PWork w, const double* zseed) {
   long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   NewtonTally tl;
   if (t < n_interior(g)) {
     int i, j, k;
     interior_ijk(g, t, i, j, k);
     c2p_srrmhd_newton_cell<LEAN>(g, cell_id(g, i, j, k), cons, aux_guess, prims, aux, tl,
-                                 w.counters);
+                                 w.counters, zseed);
   }
   tally_flush(tl, t < n_interior(g), w.counters);
 }
@@ -521,7 +527,7 @@ __device__ __forceinline__ bool imex_fast_form(const Grid& g, long long cell,
                                                const double* __restrict__ source1,
                                                const double* __restrict__ source2,
                                                double* __restrict__ out, double* zout, double dt,
-                                               int& its) {
+                                               int& its, const double* zseed = nullptr) {
   const long long N = g.Ntot;
   double c[14], x[14];
 #pragma unroll
@@ -539,11 +545,17 @@ __device__ __forceinline__ bool imex_fast_form(const Grid& g, long long cell,
   const double a = FORM <= 3 ? dt * kGam : 0.5 * dt, cp2 = g.cp * g.cp, sg = sigma_of(g, c[0]);
   x[12] = c[12] / (1 + a / cp2);
   x[11] = (c[11] + a * c[13]) / (1 + a / cp2);
-  double Z = aux_guess[10 * N + cell];
+  // the inner recovery's Z: the network's guess for the stage's first
+  // iterate when given (the previous state's Z is its fallback), else that Z
+  double Z = zseed ? zseed[cell] : aux_guess[10 * N + cell];
   bool ok = false;
   for (int it = 0; it < 50; ++it) {
     double v[3], W;
-    if (!srrmhd_prims_newton(x, g.gamma, Z, v, W, its)) break;
+    if (!srrmhd_prims_newton(x, g.gamma, Z, v, W, its)) {
+      if (it > 0 || !zseed) break;
+      Z = aux_guess[10 * N + cell];
+      if (!srrmhd_prims_newton(x, g.gamma, Z, v, W, its)) break;
+    }
     const double q = x[13];
     const double vE = v[0] * x[8] + v[1] * x[9] + v[2] * x[10];
     const double vxB0 = v[1] * x[7] - v[2] * x[6];
@@ -587,9 +599,30 @@ __device__ __forceinline__ bool imex_fast_cell(const Grid& g, long long cell,
                                                const double* __restrict__ aux_guess,
                                                const double* __restrict__ flux1,
                                                const double* __restrict__ source1,
-                                               double* __restrict__ out, double dt, int& its) {
+                                               double* __restrict__ out, double dt, int& its,
+                                               const double* zseed = nullptr) {
   return imex_fast_form<STAGE>(g, cell, cons, aux_guess, flux1, nullptr, source1, nullptr, out,
-                               nullptr, dt, its);
+                               nullptr, dt, its, zseed);
+}
+
+// The first iterate of SSP2 implicit stage STAGE (the stage's explicit part
+// c, SSP2.cc:194-264) of every interior cell, into `out`: the state the
+// guess network reads for that stage (stage 1's is U^n itself).
+template <int STAGE>
+__global__ void __launch_bounds__(128)
+    k_imex_explicit_part(Grid g, const double* __restrict__ cons,
+                         const double* __restrict__ flux1, const double* __restrict__ source1,
+                         double* __restrict__ out, double dt) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= n_interior(g)) return;
+  int i, j, k;
+  interior_ijk(g, t, i, j, k);
+  const long long cell = cell_id(g, i, j, k);
+#pragma unroll
+  for (int v = 0; v < 14; ++v) {
+    const long long o = v * g.Ntot + cell;
+    out[o] = STAGE == 1 ? cons[o] : cons[o] - dt * (flux1[o] - kOm2Gam * source1[o]);
+  }
 }
 
 // SSP3 / SSP2322 stages in the mixed form; failures queued for the exact solve.
@@ -626,7 +659,7 @@ __global__ void __launch_bounds__(128, kNewtonMinBlocks)
     k_imex_fast(Grid g, const double* __restrict__ cons, const double* __restrict__ aux_guess,
                 const double* __restrict__ u1, const double* __restrict__ flux1,
                 const double* __restrict__ source1, double* __restrict__ out, double dt,
-                C2PWork w) {
+                C2PWork w, const double* zseed) {
   (void)u1;
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   long long its_total = 0;
@@ -635,7 +668,8 @@ __global__ void __launch_bounds__(128, kNewtonMinBlocks)
     interior_ijk(g, t, i, j, k);
     const long long cell = cell_id(g, i, j, k);
     int its = 0;
-    if (!imex_fast_cell<STAGE>(g, cell, cons, aux_guess, flux1, source1, out, dt, its)) {
+    if (!imex_fast_cell<STAGE>(g, cell, cons, aux_guess, flux1, source1, out, dt, its,
+                               zseed)) {
       const int slot = atomicAdd(w.fail_count, 1);
       w.fail_list[slot] = (int)cell;
     }
@@ -689,15 +723,38 @@ __global__ void __launch_bounds__(128, kNewtonMinBlocks)
                                     d.a[ia], d.a[EA_SOL], guess_mode ? d.a[EA_ZG] : nullptr, tl);
       else
         c2p_srrmhd_newton_cell<LEAN>(g, cell, d.a[ic], d.a[iag], d.a[ip], d.a[ia], tl,
-                                     d.counters);
+                                     d.counters, guess_mode ? d.a[EA_ZG] : nullptr);
     }
     tally_flush(tl, act, d.counters);
   }
 }
 
+// SSP2 stage STAGE's explicit part of every SRRMHD member into EA_U2 (the
+// state the guess network reads for stage 2; stage 1 reads EA_CONS).
+__global__ void __launch_bounds__(128)
+    k_ens_imex_explicit_part2(const Member* __restrict__ mem, const Item* __restrict__ items,
+                              int n_items) {
+  for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
+    const Item w = items[it];
+    const Member& d = mem[w.m];
+    const Grid g = d.g;
+    const long long t = w.a + threadIdx.x;
+    if (t >= n_interior(g)) continue;
+    int i, j, k;
+    interior_ijk(g, t, i, j, k);
+    const long long cell = cell_id(g, i, j, k);
+#pragma unroll
+    for (int v = 0; v < 14; ++v) {
+      const long long o = v * g.Ntot + cell;
+      d.a[EA_U2][o] = d.a[EA_CONS][o] - d.dt * (d.a[EA_F1][o] - kOm2Gam * d.a[EA_S1][o]);
+    }
+  }
+}
+
 template <int STAGE>
 __global__ void __launch_bounds__(128, kNewtonMinBlocks)
-    k_ens_imex_fast(const Member* __restrict__ mem, const Item* __restrict__ items, int n_items) {
+    k_ens_imex_fast(const Member* __restrict__ mem, const Item* __restrict__ items, int n_items,
+                    int guess_mode) {
   for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
     const Item w = items[it];
     const Member& d = mem[w.m];
@@ -712,7 +769,7 @@ __global__ void __launch_bounds__(128, kNewtonMinBlocks)
       const long long cell = cell_id(g, i, j, k);
       const bool ok = imex_fast_cell<STAGE>(g, cell, d.a[EA_CONS], d.a[EA_AUX], d.a[EA_F1],
                                             d.a[EA_S1], d.a[STAGE == 1 ? EA_U1 : EA_U2], d.dt,
-                                            its);
+                                            its, guess_mode ? d.a[EA_ZG] : nullptr);
       its_total = its;
       if (!ok) {  // queued for the reference solve (ens_imex_queued)
         const int slot = atomicAdd(d.fail_count, 1);
@@ -803,20 +860,26 @@ cudaError_t ens_c2p_newton(const Member* mem, const Item* items, int n, int mode
     k_ens_c2p_newton<MODEL_SRMHD, false><<<grid, 128, 0, st>>>(mem, items, n, guess_mode, ic, ipg,
                                                                iag, ip, ia);
   else if (lean)
-    k_ens_c2p_newton<MODEL_SRRMHD, true><<<grid, 128, 0, st>>>(mem, items, n, 0, ic, ipg, iag, ip,
-                                                               ia);
+    k_ens_c2p_newton<MODEL_SRRMHD, true><<<grid, 128, 0, st>>>(mem, items, n, guess_mode, ic,
+                                                               ipg, iag, ip, ia);
   else
-    k_ens_c2p_newton<MODEL_SRRMHD, false><<<grid, 128, 0, st>>>(mem, items, n, 0, ic, ipg, iag, ip,
-                                                                ia);
+    k_ens_c2p_newton<MODEL_SRRMHD, false><<<grid, 128, 0, st>>>(mem, items, n, guess_mode, ic,
+                                                                ipg, iag, ip, ia);
+  return cudaGetLastError();
+}
+
+cudaError_t ens_imex_explicit_part2(const Member* mem, const Item* items, int n, int grid,
+                                    cudaStream_t st) {
+  k_ens_imex_explicit_part2<<<grid, 128, 0, st>>>(mem, items, n);
   return cudaGetLastError();
 }
 
 cudaError_t ens_imex_fast(const Member* mem, const Item* items, int n, int stage, int grid,
-                          cudaStream_t st) {
+                          cudaStream_t st, int guess_mode) {
   if (stage == 1)
-    k_ens_imex_fast<1><<<grid, 128, 0, st>>>(mem, items, n);
+    k_ens_imex_fast<1><<<grid, 128, 0, st>>>(mem, items, n, guess_mode);
   else
-    k_ens_imex_fast<2><<<grid, 128, 0, st>>>(mem, items, n);
+    k_ens_imex_fast<2><<<grid, 128, 0, st>>>(mem, items, n, guess_mode);
   return cudaGetLastError();
 }
 
@@ -863,10 +926,18 @@ cudaError_t launch_c2p_mixed(const Grid& g, int model, int guess, const double* 
       k_c2p_newton_srmhd<false><<<blocks, 128, 0, st>>>(g, gm, cons, prims_guess, aux_guess, prims,
                                                         aux, solution, w, mw.zguess);
   } else {
+    const double* zseed = nullptr;
+    if (guess == 1 && mw.has_mlp) {
+      cudaError_t e = mlp::launch_zguess(g, nI, false, cons, mw.mlp_params, mw.feat_stats,
+                                         mw.zguess, st, MODEL_SRRMHD);
+      if (e != cudaSuccess) return e;
+      zseed = mw.zguess;
+    }
     if (lean)
-      k_c2p_newton_srrmhd<true><<<blocks, 128, 0, st>>>(g, cons, aux_guess, prims, aux, w);
+      k_c2p_newton_srrmhd<true><<<blocks, 128, 0, st>>>(g, cons, aux_guess, prims, aux, w, zseed);
     else
-      k_c2p_newton_srrmhd<false><<<blocks, 128, 0, st>>>(g, cons, aux_guess, prims, aux, w);
+      k_c2p_newton_srrmhd<false><<<blocks, 128, 0, st>>>(g, cons, aux_guess, prims, aux, w,
+                                                         zseed);
   }
   return cudaGetLastError();
 }
@@ -874,13 +945,27 @@ cudaError_t launch_c2p_mixed(const Grid& g, int model, int guess, const double* 
 cudaError_t launch_imex_fast(const Grid& g, int stage, const double* cons,
                              const double* aux_guess, const double* u1, const double* flux1,
                              const double* source1, double* out, double dt, C2PWork w,
-                             cudaStream_t st) {
+                             cudaStream_t st, const MixedWork* mw) {
   const long long nI = (long long)(g.ie - g.is) * (g.je - g.js) * (g.ke - g.ks);
   const int blocks = (int)((nI + 127) / 128);
+  const double* zseed = nullptr;
+  if (mw && mw->has_mlp) {
+    // the network's Z for the stage's first iterate, its explicit part: U^n
+    // itself for stage 1; for stage 2 staged in `out` (which the stage then
+    // overwrites)
+    if (stage == 2)
+      k_imex_explicit_part<2><<<blocks, 128, 0, st>>>(g, cons, flux1, source1, out, dt);
+    cudaError_t e = mlp::launch_zguess(g, nI, false, stage == 1 ? cons : out, mw->mlp_params,
+                                       mw->feat_stats, mw->zguess, st, MODEL_SRRMHD);
+    if (e != cudaSuccess) return e;
+    zseed = mw->zguess;
+  }
   if (stage == 1)
-    k_imex_fast<1><<<blocks, 128, 0, st>>>(g, cons, aux_guess, u1, flux1, source1, out, dt, w);
+    k_imex_fast<1><<<blocks, 128, 0, st>>>(g, cons, aux_guess, u1, flux1, source1, out, dt, w,
+                                           zseed);
   else
-    k_imex_fast<2><<<blocks, 128, 0, st>>>(g, cons, aux_guess, u1, flux1, source1, out, dt, w);
+    k_imex_fast<2><<<blocks, 128, 0, st>>>(g, cons, aux_guess, u1, flux1, source1, out, dt, w,
+                                           zseed);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   // cells the fast solve could not converge: the reference stage solve

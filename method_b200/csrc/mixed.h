@@ -23,8 +23,10 @@ struct MixedWork {
 namespace mlp {
 size_t smem_bytes();
 cudaError_t configure();
+// model 0: SRMHD features of cons (9 vars); 1: SRRMHD (14 vars).
 cudaError_t launch_zguess(const Grid& g, long long n_cells, bool batch, const double* cons,
-                          const float* P, const float* st, double* zguess, cudaStream_t s);
+                          const float* P, const float* st, double* zguess, cudaStream_t s,
+                          int model = 0);
 }  // namespace mlp
 
 // SSP2 implicit stage of the mixed form (closed-form psi/phi, Newton on E).
@@ -35,10 +37,12 @@ cudaError_t launch_imex_fast_form(const Grid& g, int form, const double* cons,
                                   const double* flux1, const double* flux2,
                                   const double* source1, const double* source2, double* out,
                                   double* zout, double dt, C2PWork w, cudaStream_t st);
+// mw (may be null): with a guess network installed, the inner recoveries
+// start from its Z for the stage's first iterate.
 cudaError_t launch_imex_fast(const Grid& g, int stage, const double* cons,
                              const double* aux_guess, const double* u1, const double* flux1,
                              const double* source1, double* out, double dt, C2PWork w,
-                             cudaStream_t st);
+                             cudaStream_t st, const MixedWork* mw = nullptr);
 
 // Batched primitive recovery of independent cells (variable-major, stride n).
 // method: 0 Powell hybrid (reference), 1 Newton; guess: 0 previous state,

@@ -15,6 +15,7 @@
 #include "mixed.h"
 #include "mlp.cuh"
 #include "srmhd.cuh"
+#include "srrmhd.cuh"
 
 namespace mth {
 namespace mlp {
@@ -346,17 +347,18 @@ __global__ void __launch_bounds__(256) k_mlp_forward(const float* __restrict__ P
 }
 
 // One lane's cell: standardised features into the warp's x row; returns D.
+template <int MODEL>
 __device__ __forceinline__ double stage_features(InferSmem& s, int warp, int lane,
                                                  const double* __restrict__ cons, long long N,
                                                  long long cell) {
   float f[IN] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
   double D = 1.0;
   if (cell >= 0) {
-    double c[9];
+    double c[Net<MODEL>::NC];
 #pragma unroll
-    for (int v = 0; v < 9; ++v) c[v] = cons[v * N + cell];
+    for (int v = 0; v < Net<MODEL>::NC; ++v) c[v] = cons[v * N + cell];
     D = c[0];
-    features_srmhd(c, f);
+    Net<MODEL>::features(c, f);
   }
 #pragma unroll
   for (int k = 0; k < IN; ++k) s.x[warp][lane][k] = (f[k] - s.stats[k]) * s.stats[IN + k];
@@ -377,6 +379,7 @@ __device__ __forceinline__ void write_guess(const InferSmem& s, int warp, int la
 // Guess of Z = rho h W^2 and v^2 for every interior cell of a grid, or for
 // the n cells of a variable-major batch (batch = 1).  zguess holds two
 // planes: Z, then v^2, each with the stride of the cons array.
+template <int MODEL>
 __global__ void __launch_bounds__(256) k_mlp_zguess(Grid g, long long n_cells, int batch,
                                                      const double* __restrict__ cons,
                                                      const float* __restrict__ P,
@@ -401,7 +404,7 @@ __global__ void __launch_bounds__(256) k_mlp_zguess(Grid g, long long n_cells, i
         cell = cell_id(g, i, j, k);
       }
     }
-    const double D = stage_features(s, warp, lane, cons, N, cell);
+    const double D = stage_features<MODEL>(s, warp, lane, cons, N, cell);
     __syncwarp();
     warp_infer(s, s.x[warp], s.y[warp]);
     __syncwarp();
@@ -410,8 +413,9 @@ __global__ void __launch_bounds__(256) k_mlp_zguess(Grid g, long long n_cells, i
   }
 }
 
-// Ensembles: the guess for the cells of every SRMHD member into the member's
-// EA_ZG planes.  A 128-cell work item is four 32-row warp chunks.
+// Ensembles: the guess for the cells of every member of one model into the
+// member's EA_ZG planes.  A 128-cell work item is four 32-row warp chunks.
+template <int MODEL>
 __global__ void __launch_bounds__(256) k_ens_mlp_zguess(const Member* __restrict__ mem,
                                                         const Item* __restrict__ items,
                                                         int n_items, int ic,
@@ -436,7 +440,7 @@ __global__ void __launch_bounds__(256) k_ens_mlp_zguess(const Member* __restrict
       interior_ijk(g, t, i, j, k);
       cell = cell_id(g, i, j, k);
     }
-    const double D = stage_features(s, warp, lane, d.a[ic], g.Ntot, cell);
+    const double D = stage_features<MODEL>(s, warp, lane, d.a[ic], g.Ntot, cell);
     __syncwarp();
     warp_infer(s, s.x[warp], s.y[warp]);
     __syncwarp();
@@ -486,7 +490,10 @@ __device__ __forceinline__ double u01(unsigned long long seed, unsigned long lon
 // b^2/rho log-uniform, isotropic directions) mapped to conserved variables
 // by the model's primsToAll; features of the conserved state, targets
 // log10(Z/D) and v^2 of the generating state.
-__global__ void k_make_pairs(long long n, unsigned long long seed, double gamma,
+// SRRMHD (model 1): the same primitive draws plus an electric field
+// E = -v x B + delta, |delta| = 10^U(-3, 0) |B| in an isotropic direction (a
+// resistive departure from ideal MHD), through the SRRMHD primsToAll.
+__global__ void k_make_pairs(long long n, unsigned long long seed, double gamma, int model,
                              float* __restrict__ feat, float* __restrict__ tgt,
                              double* __restrict__ cons_out, double* __restrict__ prims_out) {
   const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -503,21 +510,43 @@ __global__ void k_make_pairs(long long n, unsigned long long seed, double gamma,
   const double vmag = sqrt(1.0 - 1.0 / (W * W));
   const double vb = (vh[0] * bh[0] + vh[1] * bh[1] + vh[2] * bh[2]) * vmag;
   const double Bmag = sqrt(sig * rho * W * W / (1.0 + W * W * vb * vb));
-  double p[8] = {rho, vh[0] * vmag, vh[1] * vmag, vh[2] * vmag, prs, bh[0] * Bmag, bh[1] * Bmag,
-                 bh[2] * Bmag};
-  double c[9], a[13];
-  srmhd::prims_to_all(p, gamma, c, a);
+  double p[11] = {rho, vh[0] * vmag, vh[1] * vmag, vh[2] * vmag, prs, bh[0] * Bmag,
+                  bh[1] * Bmag, bh[2] * Bmag, 0.0, 0.0, 0.0};
   float f[IN];
-  features_srmhd(c, f);
+  double Z, v2;
+  if (model == 0) {
+    double c[9], a[13];
+    srmhd::prims_to_all(p, gamma, c, a);
+    features_srmhd(c, f);
+    Z = p[0] * a[0] * a[1] * a[1];
+    v2 = a[9];
+    if (cons_out)
+      for (int v = 0; v < 9; ++v) cons_out[v * n + q] = c[v];
+    if (prims_out)
+      for (int v = 0; v < 8; ++v) prims_out[v * n + q] = p[v];
+    tgt[q * OUT + 0] = (float)log10(Z / c[0]);
+  } else {
+    const double ce = 2.0 * u01(seed, b + 8) - 1.0, pe = 6.283185307179586 * u01(seed, b + 9);
+    const double se = sqrt(fmax(0.0, 1.0 - ce * ce));
+    const double dmag = pow(10.0, -3.0 + 3.0 * u01(seed, b + 10)) * Bmag;
+    const double dh[3] = {se * cos(pe), se * sin(pe), ce};
+    p[8] = -(p[2] * p[7] - p[3] * p[6]) + dmag * dh[0];
+    p[9] = -(p[3] * p[5] - p[1] * p[7]) + dmag * dh[1];
+    p[10] = -(p[1] * p[6] - p[2] * p[5]) + dmag * dh[2];
+    double c[14], a[17];
+    srrmhd::prims_to_all(p, gamma, 0.0, 0.0, 0, false, 0.0, c, a);
+    features_srrmhd(c, f);
+    Z = a[10];
+    v2 = a[9];
+    if (cons_out)
+      for (int v = 0; v < 14; ++v) cons_out[v * n + q] = c[v];
+    if (prims_out)
+      for (int v = 0; v < 11; ++v) prims_out[v * n + q] = p[v];
+    tgt[q * OUT + 0] = (float)log10(Z / c[0]);
+  }
 #pragma unroll
   for (int k = 0; k < IN; ++k) feat[q * IN + k] = f[k];
-  const double Z = p[0] * a[0] * a[1] * a[1];
-  tgt[q * OUT + 0] = (float)log10(Z / c[0]);
-  tgt[q * OUT + 1] = (float)a[9];
-  if (cons_out)
-    for (int v = 0; v < 9; ++v) cons_out[v * n + q] = c[v];
-  if (prims_out)
-    for (int v = 0; v < 8; ++v) prims_out[v * n + q] = p[v];
+  tgt[q * OUT + 1] = (float)v2;
 }
 
 __global__ void k_standardise(long long n, float* __restrict__ feat, float* __restrict__ tgt,
@@ -544,9 +573,13 @@ cudaError_t configure() {
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, bi);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_mlp_zguess, cudaFuncAttributeMaxDynamicSharedMemorySize, bi);
+    e = cudaFuncSetAttribute(k_mlp_zguess<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, bi);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_ens_mlp_zguess, cudaFuncAttributeMaxDynamicSharedMemorySize, bi);
+    e = cudaFuncSetAttribute(k_mlp_zguess<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bi);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_ens_mlp_zguess<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, bi);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_ens_mlp_zguess<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bi);
   return e;
 }
 
@@ -563,21 +596,31 @@ cudaError_t launch_forward(const float* P, int n, const float* x, float* y, cuda
 }
 
 cudaError_t launch_zguess(const Grid& g, long long n_cells, bool batch, const double* cons,
-                          const float* P, const float* st, double* zguess, cudaStream_t s) {
-  k_mlp_zguess<<<infer_grid((const void*)k_mlp_zguess, n_cells), 256, sizeof(InferSmem), s>>>(
-      g, n_cells, batch ? 1 : 0, cons, P, st, zguess);
+                          const float* P, const float* st, double* zguess, cudaStream_t s,
+                          int model) {
+  if (model == 0)
+    k_mlp_zguess<0><<<infer_grid((const void*)k_mlp_zguess<0>, n_cells), 256, sizeof(InferSmem),
+                      s>>>(g, n_cells, batch ? 1 : 0, cons, P, st, zguess);
+  else
+    k_mlp_zguess<1><<<infer_grid((const void*)k_mlp_zguess<1>, n_cells), 256, sizeof(InferSmem),
+                      s>>>(g, n_cells, batch ? 1 : 0, cons, P, st, zguess);
   return cudaGetLastError();
 }
 
 }  // namespace mlp
 
 cudaError_t ens_mlp_zguess(const Member* mem, const Item* items, int n_items, int ic,
-                           const float* params, const float* stats, int grid, cudaStream_t st) {
+                           const float* params, const float* stats, int grid, cudaStream_t st,
+                           int model) {
   (void)grid;
-  const int blocks = mlp::infer_grid((const void*)mlp::k_ens_mlp_zguess,
+  const int blocks = mlp::infer_grid((const void*)mlp::k_ens_mlp_zguess<0>,
                                      (long long)n_items * ENS_CHUNK);
-  mlp::k_ens_mlp_zguess<<<blocks, 256, sizeof(mlp::InferSmem), st>>>(mem, items, n_items, ic,
-                                                                     params, stats);
+  if (model == 0)
+    mlp::k_ens_mlp_zguess<0><<<blocks, 256, sizeof(mlp::InferSmem), st>>>(mem, items, n_items,
+                                                                          ic, params, stats);
+  else
+    mlp::k_ens_mlp_zguess<1><<<blocks, 256, sizeof(mlp::InferSmem), st>>>(mem, items, n_items,
+                                                                          ic, params, stats);
   return cudaGetLastError();
 }
 
@@ -589,9 +632,11 @@ cudaError_t launch_adam(float* P, float* m, float* v, const float* grad, float l
   return cudaGetLastError();
 }
 
-cudaError_t launch_make_pairs(long long n, unsigned long long seed, double gamma, float* feat,
-                              float* tgt, double* cons, double* prims, cudaStream_t st) {
-  k_make_pairs<<<(int)((n + 255) / 256), 256, 0, st>>>(n, seed, gamma, feat, tgt, cons, prims);
+cudaError_t launch_make_pairs(long long n, unsigned long long seed, double gamma, int model,
+                              float* feat, float* tgt, double* cons, double* prims,
+                              cudaStream_t st) {
+  k_make_pairs<<<(int)((n + 255) / 256), 256, 0, st>>>(n, seed, gamma, model, feat, tgt, cons,
+                                                       prims);
   return cudaGetLastError();
 }
 
@@ -650,7 +695,7 @@ void init_params(std::vector<float>& P, unsigned long long seed) {
 extern "C" mth_status mth_mlp_train(const mth_mlp_train_config* c, float* params, float* stats,
                                     float* final_loss, int device) {
   if (!c || !params || !stats || c->n_samples < mlp::ROWS || c->batch < mlp::ROWS ||
-      c->batch > c->n_samples || c->iterations <= 0)
+      c->batch > c->n_samples || c->iterations <= 0 || c->model < 0 || c->model > 1)
     return MTH_ERR_INVALID;
   MLP_CU(cudaSetDevice(device));
   MLP_CU(mlp::configure());
@@ -666,8 +711,8 @@ extern "C" mth_status mth_mlp_train(const mth_mlp_train_config* c, float* params
   MLP_CU(cudaMalloc(&st.p, sizeof(float) * mlp::NSTAT));
   cudaStream_t s;
   MLP_CU(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
-  MLP_CU(mlp::launch_make_pairs(n, c->seed, c->gamma, feat.as<float>(), tgt.as<float>(), nullptr,
-                                nullptr, s));
+  MLP_CU(mlp::launch_make_pairs(n, c->seed, c->gamma, c->model, feat.as<float>(),
+                                tgt.as<float>(), nullptr, nullptr, s));
   // normalisation statistics on the host
   std::vector<float> hf(n * mlp::IN), ht(n * mlp::OUT);
   MLP_CU(cudaMemcpyAsync(hf.data(), feat.p, sizeof(float) * hf.size(), cudaMemcpyDeviceToHost, s));
@@ -771,21 +816,35 @@ extern "C" mth_status mth_mlp_forward(const float* params, int n, const float* x
   return MTH_OK;
 }
 
-extern "C" mth_status mth_mlp_make_pairs(long long n, unsigned long long seed, double gamma,
-                                         float* feat, float* tgt, double* cons, double* prims,
-                                         int device) {
+namespace {
+mth_status make_pairs(int model, long long n, unsigned long long seed, double gamma, float* feat,
+                      float* tgt, double* cons, double* prims, int device) {
   if (n <= 0 || !feat || !tgt) return MTH_ERR_INVALID;
+  const int nc = model == 0 ? 9 : 14, np = model == 0 ? 8 : 11;
   MLP_CU(cudaSetDevice(device));
   DevBuf df, dt, dc, dp;
   MLP_CU(cudaMalloc(&df.p, sizeof(float) * n * mlp::IN));
   MLP_CU(cudaMalloc(&dt.p, sizeof(float) * n * mlp::OUT));
-  if (cons) MLP_CU(cudaMalloc(&dc.p, sizeof(double) * n * 9));
-  if (prims) MLP_CU(cudaMalloc(&dp.p, sizeof(double) * n * 8));
-  MLP_CU(mlp::launch_make_pairs(n, seed, gamma, df.as<float>(), dt.as<float>(), dc.as<double>(),
-                                dp.as<double>(), 0));
+  if (cons) MLP_CU(cudaMalloc(&dc.p, sizeof(double) * n * nc));
+  if (prims) MLP_CU(cudaMalloc(&dp.p, sizeof(double) * n * np));
+  MLP_CU(mlp::launch_make_pairs(n, seed, gamma, model, df.as<float>(), dt.as<float>(),
+                                dc.as<double>(), dp.as<double>(), 0));
   MLP_CU(cudaMemcpy(feat, df.p, sizeof(float) * n * mlp::IN, cudaMemcpyDefault));
   MLP_CU(cudaMemcpy(tgt, dt.p, sizeof(float) * n * mlp::OUT, cudaMemcpyDefault));
-  if (cons) MLP_CU(cudaMemcpy(cons, dc.p, sizeof(double) * n * 9, cudaMemcpyDefault));
-  if (prims) MLP_CU(cudaMemcpy(prims, dp.p, sizeof(double) * n * 8, cudaMemcpyDefault));
+  if (cons) MLP_CU(cudaMemcpy(cons, dc.p, sizeof(double) * n * nc, cudaMemcpyDefault));
+  if (prims) MLP_CU(cudaMemcpy(prims, dp.p, sizeof(double) * n * np, cudaMemcpyDefault));
   return MTH_OK;
+}
+}  // namespace
+
+extern "C" mth_status mth_mlp_make_pairs(long long n, unsigned long long seed, double gamma,
+                                         float* feat, float* tgt, double* cons, double* prims,
+                                         int device) {
+  return make_pairs(0, n, seed, gamma, feat, tgt, cons, prims, device);
+}
+
+extern "C" mth_status mth_mlp_make_pairs_srrmhd(long long n, unsigned long long seed,
+                                                double gamma, float* feat, float* tgt,
+                                                double* cons, double* prims, int device) {
+  return make_pairs(1, n, seed, gamma, feat, tgt, cons, prims, device);
 }

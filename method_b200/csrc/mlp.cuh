@@ -58,6 +58,51 @@ __device__ __forceinline__ void features_srmhd(const double* c, float* f) {
   f[7] = log10f((float)(S2 / (E * E)) + 1e-30f);
 }
 
+// Features of an SRRMHD conserved state (D, S, tau, B, E, psi, phi, q): its
+// primitive recovery depends on S-bar = S - E x B and tau-bar = tau -
+// (B^2 + E^2)/2 only (srrmhd.cc:256-301), so the map uses those:
+//   f0 = log10(tau-bar/D)        f4 = log10(S-bar^2 / (tau-bar + D)^2)
+//   f1 = log10(S-bar^2/D^2)      f5 = S-bar^2 / (tau-bar + D)^2
+//   f2 = log10(1 + tau-bar/D)    f6 = D / (tau-bar + D)
+//   f3 = |S-bar| / (tau-bar + D) f7 = 0
+// Outputs as for SRMHD: log10(Z/D) with Z = rho h W^2, and v^2.
+__device__ __forceinline__ void features_srrmhd(const double* c, float* f) {
+  const double D = c[0];
+  const double sx = c[1] - (c[9] * c[7] - c[10] * c[6]);
+  const double sy = c[2] - (c[10] * c[5] - c[8] * c[7]);
+  const double sz = c[3] - (c[8] * c[6] - c[9] * c[5]);
+  const double S2 = sx * sx + sy * sy + sz * sz;
+  const double tb = c[4] - 0.5 * (c[5] * c[5] + c[6] * c[6] + c[7] * c[7] + c[8] * c[8] +
+                                  c[9] * c[9] + c[10] * c[10]);
+  const double E = tb + D;
+  f[0] = log10f(fmaxf((float)(tb / D), 1e-30f));
+  f[1] = log10f((float)(S2 / (D * D)) + 1e-30f);
+  f[2] = log10f(1.f + fmaxf((float)(tb / D), 0.f));
+  f[3] = (float)(sqrt(S2) / E);
+  f[4] = log10f((float)(S2 / (E * E)) + 1e-30f);
+  f[5] = (float)(S2 / (E * E));
+  f[6] = (float)(D / E);
+  f[7] = 0.f;
+}
+
+// Conserved variables per model and the feature map of a model.
+template <int MODEL>
+struct Net;
+template <>
+struct Net<0> {
+  static constexpr int NC = 9;
+  __device__ __forceinline__ static void features(const double* c, float* f) {
+    features_srmhd(c, f);
+  }
+};
+template <>
+struct Net<1> {
+  static constexpr int NC = 14;
+  __device__ __forceinline__ static void features(const double* c, float* f) {
+    features_srrmhd(c, f);
+  }
+};
+
 __device__ __forceinline__ uint32_t pack_bf16(__nv_bfloat16 lo, __nv_bfloat16 hi) {
   uint32_t l = (uint32_t)__bfloat16_as_ushort(lo), h = (uint32_t)__bfloat16_as_ushort(hi);
   return l | (h << 16);
