@@ -188,7 +188,7 @@ def cpu_ensemble(initial):
                       "zone-updates/s on a 64x128 member)"}
 
 
-def run_ensemble(mb, initial, torch, ranks, K, W, guess):
+def run_ensemble(mb, initial, torch, ranks, K, W, guess, guess_r=None):
     """The ensemble workload, members split over ranks by cost (LPT)."""
     from method_b200.ranks import lpt_partition
     mem = initial.kh_ensemble(ENS_MEMBERS, seed=2024)
@@ -203,6 +203,8 @@ def run_ensemble(mb, initial, torch, ranks, K, W, guess):
     ens = mb.Ensemble(cfgs)
     if guess:
         ens.set_mlp(guess[0], guess[1])
+        if guess_r:
+            ens.set_mlp(guess_r[0], guess_r[1], model="srrmhd")
     for k, i in enumerate(mine):
         ens.set_prims(k, initial.kelvin_helmholtz(**mem[i][1]))
     ti = ens.autotune(reps=2)
@@ -407,9 +409,10 @@ def timed_steps(sim, torch, device, dt, K, W, barrier, max_over_ranks):
     return max_over_ranks(e0.elapsed_time(e1))
 
 
-def run_sheet(mb, initial, torch, ranks, K, W, peak, cpu):
-    """Config 3: SSP2 on the resistive current sheet, plain and mixed forms,
-    the reference CPU build's SSP2::step beside them (rank 0, N = 1)."""
+def run_sheet(mb, initial, torch, ranks, K, W, peak, cpu, guess_r=None):
+    """Config 3: SSP2 on the resistive current sheet, plain and mixed forms
+    (and the mixed form seeded by the SRRMHD guess network when given), the
+    reference CPU build's SSP2::step beside them (rank 0, N = 1)."""
     sigma = initial.sigma_for_seed(SHEET_SEED)
     cfg = sheet_cfg(sigma)
     nx, ny = SHEET_N
@@ -417,8 +420,12 @@ def run_sheet(mb, initial, torch, ranks, K, W, peak, cpu):
     p0 = initial.current_sheet(nx, ny, seed=SHEET_SEED)
     dt = 0.4 * min(1.0 / nx, 2.0 / ny) / np.sqrt(2.0)  # steady-state CFL dt
     out, states = {}, {}
-    for form, prec in (("plain", "fp64"), ("mixed", "mixed")):
-        sim = mb.Simulation(precision=prec, device=ranks.local, **cfg)
+    forms = [("plain", "fp64"), ("mixed", "mixed")] + ([("mixed_mlp", "mixed")] if guess_r else [])
+    for form, prec in forms:
+        sim = mb.Simulation(precision=prec, device=ranks.local,
+                            guess="mlp" if form == "mixed_mlp" else "previous", **cfg)
+        if form == "mixed_mlp":
+            sim.set_mlp(*guess_r)
         sim.set_prims(p0)
         kk = max(2, K // 5) if form == "plain" else K
         ms = timed_steps(sim, torch, ranks.local, dt, kk, W, ranks.barrier, ranks.max)
@@ -432,7 +439,9 @@ def run_sheet(mb, initial, torch, ranks, K, W, peak, cpu):
             "steps": kk, "implicit_failed": st["implicit_failed"],
             "implicit_iters_per_cell": st["implicit_evals"] / max(st["implicit_cells"], 1),
             "implicit_fallbacks": st["implicit_fallbacks"], "c2p_unconverged":
-                st["c2p_unconverged"], "roofline": roof,
+                st["c2p_unconverged"],
+            "c2p_newton_iters_per_cell": st["c2p_evals"] / max(st["c2p_cells"], 1),
+            "c2p_fallbacks": st["c2p_fallbacks"], "roofline": roof,
             "step_roofline": {"bytes_per_zone_update": SHEET_BYTES, "achieved_gbs": round(
                 SHEET_BYTES * cells / (ms / kk * 1e-3) / 1e9, 1), "peak": peak,
                 "frac": round(SHEET_BYTES * cells / (ms / kk * 1e-3) / 1e9 / peak, 4)},
@@ -456,6 +465,7 @@ def run_sheet(mb, initial, torch, ranks, K, W, peak, cpu):
         l1[name] = {"l1_rel": float(d.sum() / np.abs(b).sum()), "max_abs": float(d.max())}
     res = {"workload": SHEET_WORKLOAD, "seed": SHEET_SEED, "sigma": sigma, "dt": dt,
            "unit": "zone-updates/s", "plain": out["plain"], "mixed": out["mixed"],
+           "mixed_mlp": out.get("mixed_mlp"),
            "speedup_mixed_vs_plain": out["mixed"]["value"] / out["plain"]["value"],
            "l1_mixed_vs_fp64": {"steps": W + out["plain"]["steps"], **l1}}
     if cpu:
@@ -724,6 +734,13 @@ def main():
         train = {"loss": loss, "seconds": round(time.perf_counter() - t0, 2),
                  "samples": 1 << 19, "iterations": 4000, "batch": 8192}
         guess = (P, S)
+    guess_r = None
+    if not args.no_ensemble or not args.no_sheet:
+        t0 = time.perf_counter()
+        Pr, Sr, loss_r = mb.train_guess(device=local, model="srrmhd")
+        guess_r = (Pr, Sr)
+        if train is not None:
+            train["srrmhd"] = {"loss": loss_r, "seconds": round(time.perf_counter() - t0, 2)}
     ensemble = None
     with clocks:
         for form in forms:
@@ -747,10 +764,14 @@ def main():
             ke, we = max(1, min(K, 20)), max(W, 3)
             ensemble = run_ensemble(mb, initial, torch, ranks, ke, we, None)
             if guess:
-                e_mlp = run_ensemble(mb, initial, torch, ranks, ke, we, guess)
+                e_mlp = run_ensemble(mb, initial, torch, ranks, ke, we, guess, guess_r)
                 ensemble["with_learned_guess"] = {
                     k: e_mlp[k] for k in ("value", "ms_per_step", "c2p_newton_iters_per_cell",
-                                          "c2p_unconverged", "c2p_fallbacks")}
+                                          "implicit_iters_per_cell", "c2p_unconverged",
+                                          "c2p_fallbacks", "implicit_fallbacks",
+                                          "implicit_failed")}
+                ensemble["with_learned_guess"]["networks"] = "SRMHD and SRRMHD members" \
+                    if guess_r else "SRMHD members"
         c2p_batch = None
         want_cpu = rank == 0 and world == 1 and not args.no_cpu
         if not args.no_c2p_batch:
@@ -758,7 +779,7 @@ def main():
         sheet = None
         if not args.no_sheet:
             sheet = run_sheet(mb, initial, torch, ranks, max(K // 5, 5), max(W, 3), peak,
-                              cpu=False)
+                              cpu=False, guess_r=guess_r)
         kh = None
         if not args.no_kh:
             kh = run_kh_full(mb, initial, torch, ranks, peak, cpu=False)
