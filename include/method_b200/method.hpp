@@ -173,6 +173,19 @@ class Weno5 : public WenoBase {
  public:
   explicit Weno5(Data* data) : WenoBase(data, 5) {}
 };
+// Higher orders (weno.h:346-624): the same Jiang-Shu scheme on 7, 9, 11 points.
+class Weno7 : public WenoBase {
+ public:
+  explicit Weno7(Data* data) : WenoBase(data, 7) {}
+};
+class Weno9 : public WenoBase {
+ public:
+  explicit Weno9(Data* data) : WenoBase(data, 9) {}
+};
+class Weno11 : public WenoBase {
+ public:
+  explicit Weno11(Data* data) : WenoBase(data, 11) {}
+};
 
 // ------------------------------------------------------------ flux methods
 class FluxMethod {

@@ -499,7 +499,9 @@ mth_status mth_create(const mth_config* cfg, mth_handle** out) {
     delete h;
     return MTH_ERR_INVALID;
   }
-  if (c.sigma < 0.0 || (c.weno_order != 3 && c.weno_order != 5) ||
+  if (c.sigma < 0.0 ||
+      (c.weno_order != 3 && c.weno_order != 5 && c.weno_order != 7 && c.weno_order != 9 &&
+       c.weno_order != 11) ||
       c.Ng < (c.weno_order + 1) / 2 + 1 || c.nx <= 0 || c.ny < 0 || c.nz < 0 ||
       (c.ny == 0 && c.nz != 0) || c.bcs < 0 || c.bcs > 2 || c.integrator < 0 ||
       c.integrator > 4 || (c.integrator >= MTH_SSP2 && c.model != MTH_SRRMHD) ||

@@ -20,14 +20,43 @@
 #pragma once
 #include "common.cuh"
 #include "weno.cuh"
+#include "weno_hi.cuh"
 
 namespace mth {
+
+// The upwind point reconstruction of order ORDER (3 .. 11) on the values
+// v[q * stride], q = 0 .. ORDER-1, walking forwards (dir = +1) or backwards.
+template <int ORDER, typename R>
+__device__ __forceinline__ R weno_point(const R* v, int stride) {
+#define V(q) v[(q) * stride]
+  if constexpr (sizeof(R) == 8) {
+    if constexpr (ORDER == 7) return weno7_exact(V(0), V(1), V(2), V(3), V(4), V(5), V(6));
+    if constexpr (ORDER == 9)
+      return weno9_exact(V(0), V(1), V(2), V(3), V(4), V(5), V(6), V(7), V(8));
+    if constexpr (ORDER == 11)
+      return weno11_exact(V(0), V(1), V(2), V(3), V(4), V(5), V(6), V(7), V(8), V(9), V(10));
+  } else {
+    if constexpr (ORDER == 7) return weno7_fast(V(0), V(1), V(2), V(3), V(4), V(5), V(6));
+    if constexpr (ORDER == 9)
+      return weno9_fast(V(0), V(1), V(2), V(3), V(4), V(5), V(6), V(7), V(8));
+    if constexpr (ORDER == 11)
+      return weno11_fast(V(0), V(1), V(2), V(3), V(4), V(5), V(6), V(7), V(8), V(9), V(10));
+  }
+#undef V
+  return R(0);
+}
 
 template <int ORDER, typename R>
 __device__ __forceinline__ R weno_face(const R* p, const R* m, int stride, int base) {
   // p, m point at the first stencil cell of the region column; `base` is the
   // region index of cell i-H for face i (face between cells i-1 and i).
-  if constexpr (ORDER == 3) {
+  if constexpr (ORDER >= 7) {
+    // upwind cells i-H .. i-H+ORDER-1; downwind cells i+H-1 down to i+H-ORDER
+    // (weno.cc:239-482): the region indices base .. base+ORDER-1 and
+    // base+ORDER down to base+1
+    return weno_point<ORDER, R>(p + base * stride, stride) +
+           weno_point<ORDER, R>(m + (base + ORDER) * stride, -stride);
+  } else if constexpr (ORDER == 3) {
     // upwind cells i-2, i-1, i ; downwind cells i+1, i, i-1 (weno.cc:123-164)
     if constexpr (sizeof(R) == 8) {
       return weno3_exact(p[(base + 0) * stride], p[(base + 1) * stride], p[(base + 2) * stride]) +
@@ -56,9 +85,10 @@ __device__ __forceinline__ R weno_face(const R* p, const R* m, int stride, int b
   }
 }
 
+// Halo of a face reconstruction: the reference's WENO shift (order + 1) / 2.
 template <int ORDER>
 struct Halo {
-  static constexpr int H = (ORDER == 3) ? 2 : 3;
+  static constexpr int H = (ORDER + 1) / 2;
 };
 
 template <class M, typename R, int ORDER, int TI>
@@ -159,7 +189,7 @@ __device__ __forceinline__ void fvs2d_tile(const Grid& g, const double* __restri
     const R* P = sp + v * S::RX + lane;
     const R* Mm = sm + v * S::RX + lane;
     // face i0+fi: cell i-H sits at region row fi
-    sr[e] = weno_face<ORDER, R>(P, Mm, TJ, fi + H - (ORDER == 3 ? 2 : 3));
+    sr[e] = weno_face<ORDER, R>(P, Mm, TJ, fi);
     fi += TI;
     if (fi > TI) {
       fi -= TI + 1;
@@ -193,7 +223,7 @@ __device__ __forceinline__ void fvs2d_tile(const Grid& g, const double* __restri
     for (int e = tid; e < NC * S::FY; e += NT) {
       const R* P = sp + v * S::RY + r * WY;
       const R* Mm = sm + v * S::RY + r * WY;
-      sr[e] = weno_face<ORDER, R>(P, Mm, 1, fj + H - (ORDER == 3 ? 2 : 3));
+      sr[e] = weno_face<ORDER, R>(P, Mm, 1, fj);
       fj += FS;
       r += RS;
       if (fj > TJ) {

@@ -98,10 +98,25 @@ __global__ void k_weno_dir(Grid g, int nc, int order, int dir, const double* __r
       if (order == 3) {
         up = weno3_exact(P[-2 * stride], P[-1 * stride], P[0]);
         dn = weno3_exact(Mm[1 * stride], Mm[0], Mm[-1 * stride]);
-      } else {
+      } else if (order == 5) {
         up = weno5_exact(P[-3 * stride], P[-2 * stride], P[-1 * stride], P[0], P[1 * stride]);
         dn = weno5_exact(Mm[2 * stride], Mm[1 * stride], Mm[0], Mm[-1 * stride],
                          Mm[-2 * stride]);
+      } else {
+        // upwind i-shift .. i-shift+order-1, downwind i+shift-1 .. i+shift-order
+        const int s = (int)stride;
+        const double* U = P - shift * stride;
+        const double* Dn = Mm + (shift - 1) * stride;
+        if (order == 7) {
+          up = weno_point<7, double>(U, s);
+          dn = weno_point<7, double>(Dn, -s);
+        } else if (order == 9) {
+          up = weno_point<9, double>(U, s);
+          dn = weno_point<9, double>(Dn, -s);
+        } else {
+          up = weno_point<11, double>(U, s);
+          dn = weno_point<11, double>(Dn, -s);
+        }
       }
       r = up + dn;
     } else {
@@ -945,12 +960,24 @@ cudaError_t launch_fvs2d_fp64(const Grid& g, int model, int order, const double*
                               const double* prims, const double* aux, const double* u0,
                               double* out, double dt, int mode, cudaStream_t st,
                               StageTail tail) {
+#define FVS64(MM, O) return fvs2d_instance<MM, O, 8>(g, cons, prims, aux, u0, out, dt, mode, tail, st)
   if (model == MODEL_SRMHD) {
-    if (order == 3) return fvs2d_instance<SRMHD, 3, 8>(g, cons, prims, aux, u0, out, dt, mode, tail, st);
-    return fvs2d_instance<SRMHD, 5, 8>(g, cons, prims, aux, u0, out, dt, mode, tail, st);
+    switch (order) {
+      case 3: FVS64(SRMHD, 3);
+      case 5: FVS64(SRMHD, 5);
+      case 7: FVS64(SRMHD, 7);
+      case 9: FVS64(SRMHD, 9);
+      default: FVS64(SRMHD, 11);
+    }
   }
-  if (order == 3) return fvs2d_instance<SRRMHD, 3, 8>(g, cons, prims, aux, u0, out, dt, mode, tail, st);
-  return fvs2d_instance<SRRMHD, 5, 8>(g, cons, prims, aux, u0, out, dt, mode, tail, st);
+  switch (order) {
+    case 3: FVS64(SRRMHD, 3);
+    case 5: FVS64(SRRMHD, 5);
+    case 7: FVS64(SRRMHD, 7);
+    case 9: FVS64(SRRMHD, 9);
+    default: FVS64(SRRMHD, 11);
+  }
+#undef FVS64
 }
 
 cudaError_t launch_fvs_generic(const Grid& g, int model, int order, double* cons, double* prims,

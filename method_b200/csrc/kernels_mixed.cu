@@ -888,14 +888,25 @@ cudaError_t launch_fvs2d_fp32(const Grid& g, int model, int order, const double*
                               const double* prims, const double* aux, const double* u0,
                               double* out, double dt, int mode, cudaStream_t st,
                               StageTail tail) {
+#define FVS32(MM, O) \
+  return fvs2d_fp32_instance<MM, O, 8>(g, cons, prims, aux, u0, out, dt, mode, tail, st)
   if (model == MODEL_SRMHD) {
-    if (order == 3)
-      return fvs2d_fp32_instance<SRMHD, 3, 8>(g, cons, prims, aux, u0, out, dt, mode, tail, st);
-    return fvs2d_fp32_instance<SRMHD, 5, 8>(g, cons, prims, aux, u0, out, dt, mode, tail, st);
+    switch (order) {
+      case 3: FVS32(SRMHD, 3);
+      case 5: FVS32(SRMHD, 5);
+      case 7: FVS32(SRMHD, 7);
+      case 9: FVS32(SRMHD, 9);
+      default: FVS32(SRMHD, 11);
+    }
   }
-  if (order == 3)
-    return fvs2d_fp32_instance<SRRMHD, 3, 8>(g, cons, prims, aux, u0, out, dt, mode, tail, st);
-  return fvs2d_fp32_instance<SRRMHD, 5, 8>(g, cons, prims, aux, u0, out, dt, mode, tail, st);
+  switch (order) {
+    case 3: FVS32(SRRMHD, 3);
+    case 5: FVS32(SRRMHD, 5);
+    case 7: FVS32(SRRMHD, 7);
+    case 9: FVS32(SRRMHD, 9);
+    default: FVS32(SRRMHD, 11);
+  }
+#undef FVS32
 }
 
 cudaError_t launch_c2p_batch(long long n, double gamma, int method, int guess,

@@ -37,7 +37,7 @@ typedef struct {
   double endTime, cfl;
   int Ng;
   double gamma, sigma, cp;
-  int weno;       /* 3 or 5 */
+  int weno;       /* 3, 5, 7, 9 or 11 */
   int bcs;        /* 0 outflow, 1 periodic, 2 flow */
   int integrator; /* 0 RK2, 1 RKSplit, 2 SSP2, 3 SSP3, 4 SSP2322 */
   int functional_sigma; /* Data::functionalSigma */
@@ -804,6 +804,21 @@ void orc_apply_bcs(void* h, double* cons, double* prims, double* aux) {
   bc_arr(s, aux, s->NA);
 }
 
+/* WENO7 / WENO9 / WENO11 point kernels (wenoUpwinds.cc:86-482), generated
+ * by method_b200/gen_weno.py from the Jiang-Shu scheme in exact arithmetic. */
+#include "weno_hi.h"
+
+/* The upwind point kernel of order 3 .. 11 on v[0 .. order-1]. */
+static double weno_point(int order, const double* v) {
+  switch (order) {
+    case 3: return orc_weno3_upwind(v[0], v[1], v[2]);
+    case 5: return orc_weno5_upwind(v[0], v[1], v[2], v[3], v[4]);
+    case 7: return orc_weno7(v[0], v[1], v[2], v[3], v[4], v[5], v[6]);
+    case 9: return orc_weno9(v[0], v[1], v[2], v[3], v[4], v[5], v[6], v[7], v[8]);
+    default: return orc_weno11(v[0], v[1], v[2], v[3], v[4], v[5], v[6], v[7], v[8], v[9], v[10]);
+  }
+}
+
 /* ------------------------------------------------------------------------ */
 /* FVS::F (fluxVectorSplitting.cc:4-131) with WENO sweeps (weno.cc).         */
 
@@ -840,12 +855,15 @@ static void flux_reconstruction(orc_sim* s, const double* cons, int dir, double*
           size_t o = IDX(s, v, i, j, k);
           const double *P = s->fplus + o, *M = s->fminus + o;
           if (idx < shift || idx >= N - shift) continue;
-          if (s->c.weno == 3) {
-            s->fprec[o] = orc_weno3_upwind(P[-2 * (long)stride], P[-(long)stride], P[0]);
-            s->fmrec[o] = orc_weno3_upwind(M[stride], M[0], M[-(long)stride]);
-          } else {
-            s->fprec[o] = orc_weno5_upwind(P[-3 * (long)stride], P[-2 * (long)stride], P[-(long)stride], P[0], P[stride]);
-            s->fmrec[o] = orc_weno5_upwind(M[2 * stride], M[stride], M[0], M[-(long)stride], M[-2 * (long)stride]);
+          {
+            /* upwind cells i-shift .. i-shift+order-1, downwind i+shift-1 .. i+shift-order */
+            double vu[11], vd[11];
+            for (int m = 0; m < s->c.weno; m++) {
+              vu[m] = P[(long)(m - shift) * (long)stride];
+              vd[m] = M[(long)(shift - 1 - m) * (long)stride];
+            }
+            s->fprec[o] = weno_point(s->c.weno, vu);
+            s->fmrec[o] = weno_point(s->c.weno, vd);
           }
         }
   for (size_t q = 0; q < n; q++) frecon[q] = s->fprec[q] + s->fmrec[q];
@@ -1198,7 +1216,11 @@ void* orc_create(const orc_config* c, const double* prims) {
   s->ks = c->Ng; s->ke = s->Nz - c->Ng;
   if (s->dims < 3) { s->ks = 0; s->ke = 1; }
   if (s->dims < 2) { s->js = 0; s->je = 1; }
-  if (c->sigma < 0.0 || c->Ng < (c->weno + 1) / 2 + 1) { free(s); return NULL; }
+  if (c->sigma < 0.0 || c->Ng < (c->weno + 1) / 2 + 1 ||
+      (c->weno != 3 && c->weno != 5 && c->weno != 7 && c->weno != 9 && c->weno != 11)) {
+    free(s);
+    return NULL;
+  }
   s->dx = (c->xmax - c->xmin) / (c->nx);
   s->dy = (ymax - ymin) / (c->ny);
   s->dz = (zmax - zmin) / (c->nz);

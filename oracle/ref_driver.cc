@@ -115,7 +115,10 @@ void* mref_create(const mref_config* c, const double* prims) {
     if (c->model == 0) r->model = new SRMHD(r->data);
     else r->model = new SRRMHD(r->data);
     if (c->weno == 3) r->weno = new Weno3(r->data);
-    else r->weno = new Weno5(r->data);
+    else if (c->weno == 5) r->weno = new Weno5(r->data);
+    else if (c->weno == 7) r->weno = new Weno7(r->data);
+    else if (c->weno == 9) r->weno = new Weno9(r->data);
+    else r->weno = new Weno11(r->data);
     r->flux = new FVS(r->data, r->weno, r->model);
     if (c->bcs == 0) r->bcs = r->outflow = new Outflow(r->data);
     else if (c->bcs == 1) r->bcs = r->periodic = new Periodic(r->data);

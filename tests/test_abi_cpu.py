@@ -38,8 +38,10 @@ def test_invalid_configuration_rejected_on_host():
             mb.Simulation(nx=16, ny=16, model="srmhd", integrator=integ)
     with pytest.raises(ValueError):  # a 3D grid needs ny > 0 (simData.cc:66-84)
         mb.Simulation(nx=16, ny=0, nz=8)
-    with pytest.raises(ValueError):  # WENO order 3 or 5
-        mb.Simulation(nx=16, ny=16, weno=7)
+    with pytest.raises(ValueError):  # WENO orders 3, 5, 7, 9, 11 (weno.h)
+        mb.Simulation(nx=16, ny=16, Ng=8, weno=6)
+    with pytest.raises(ValueError):  # WENO7 needs Ng >= 5
+        mb.Simulation(nx=16, ny=16, Ng=4, weno=7)
     with pytest.raises(KeyError):  # no such boundary class
         mb.Simulation(nx=16, ny=16, bcs="reflective")
 

@@ -148,6 +148,17 @@ LIVE = {
                            ymax=1.0, endTime=3.0, cfl=0.4, Ng=4, gamma=4.0 / 3.0, sigma=1e3,
                            weno=3, bcs="periodic", integrator="ssp2322"),
                       lambda: initial.current_sheet(16, 32, seed=11), 2),
+    # WENO7 / WENO9 / WENO11 (weno.cc:239-482), Ng = shift + 1
+    "kh_weno7": (dict(model="srmhd", nx=32, ny=64, xmin=-0.5, xmax=0.5, ymin=-1.0, ymax=1.0,
+                      endTime=3.0, cfl=0.4, Ng=5, gamma=4.0 / 3.0, weno=7, bcs="flow",
+                      integrator="rk2"), lambda: initial.kelvin_helmholtz(32, 64, Ng=5, seed=4), 6),
+    "ot_weno9": (dict(model="srmhd", nx=32, ny=32, xmin=0, xmax=1, ymin=0, ymax=1, endTime=3.0,
+                      cfl=0.4, Ng=6, gamma=4.0 / 3.0, weno=9, bcs="periodic", integrator="rk2"),
+                 lambda: initial.orszag_tang(32, Ng=6), 4),
+    "sheet_weno11_ssp2": (dict(model="srrmhd", nx=24, ny=48, xmin=-0.5, xmax=0.5, ymin=-1.0,
+                               ymax=1.0, endTime=3.0, cfl=0.4, Ng=7, gamma=4.0 / 3.0, sigma=1e3,
+                               weno=11, bcs="outflow", integrator="ssp2"),
+                          lambda: initial.current_sheet(24, 48, Ng=7, seed=14), 2),
     # Data::functionalSigma: conductivity sigma * D^gam per cell (simData.cc:114-127)
     "sheet_ssp2_functional_sigma": (dict(model="srrmhd", nx=24, ny=48, xmin=-0.5, xmax=0.5,
                                          ymin=-1.0, ymax=1.0, endTime=3.0, cfl=0.4, Ng=4,
