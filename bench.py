@@ -208,6 +208,7 @@ def run_ensemble(mb, initial, torch, ranks, K, W, guess, guess_r=None):
     for k, i in enumerate(mine):
         ens.set_prims(k, initial.kelvin_helmholtz(**mem[i][1]))
     ti = ens.autotune(reps=2)
+    tuning = ens.tuning()
     stream = torch.cuda.Stream(device=ranks.local)
     ens.set_stream(stream.cuda_stream)
     ens.step(W, sync=False)
@@ -235,7 +236,8 @@ def run_ensemble(mb, initial, torch, ranks, K, W, guess, guess_r=None):
     return {"value": total * K / (ms * 1e-3), "unit": "zone-updates/s", "ms_per_step": ms / K,
             "steps": K, "warmup": W, "members": ENS_MEMBERS, "resistive_members": n_res,
             "members_this_rank": len(mine), "interior_cells_total": int(total),
-            "tile_heights_by_class": ti, "guess": "mlp" if guess else "previous",
+            "tile_heights_by_class": ti, "autotune": tuning,
+            "guess": "mlp" if guess else "previous",
             "c2p_newton_iters_per_cell": agg["c2p_evals"] / max(agg["c2p_cells"], 1),
             "implicit_iters_per_cell": agg["implicit_evals"] / max(agg["implicit_cells"], 1),
             **{k: agg[k] for k in ("c2p_unconverged", "c2p_fallbacks", "implicit_fallbacks",

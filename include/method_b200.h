@@ -354,12 +354,24 @@ mth_status mth_ensemble_set_mlp(mth_ensemble* e, const float* params, const floa
  * seeds their recoveries and the inner recoveries of their implicit stages. */
 mth_status mth_ensemble_set_mlp_srrmhd(mth_ensemble* e, const float* params, const float* stats);
 mth_status mth_ensemble_set_stream(mth_ensemble* e, void* stream);
-/* Times tile heights 4, 8, 16 (rows of 32 cells per flux tile) for each
- * member size class (nx <= 96, <= 192, larger) on the ensemble's first flux
- * phase, `reps` timed launches each, and keeps the fastest; the choice is
- * returned in ti3 (may be NULL).  Runs flux kernels on the current state but
- * changes no member's state. */
+/* Autotuner, on the ensemble's own members: for each member size class
+ * (nx <= 96, <= 192, larger) it times the flux phase at tile heights 4, 8,
+ * 16 (rows of 32 cells) x persistent grids (one CTA per tile, 4 or 2 CTAs per
+ * SM), and the recovery phases at 4, 8, 16 CTAs per SM, `reps` timed
+ * launches each, and keeps the fastest; the tile heights are returned in ti3
+ * (may be NULL).  Runs kernels on the current state but changes no member's
+ * state. */
 mth_status mth_ensemble_autotune(mth_ensemble* e, int reps, int* ti3);
+/* What the autotuner chose, and the summed phase times (ms per repetition)
+ * of the default choice (tile height 8, one CTA per tile, 8 CTAs per SM)
+ * against the chosen one. */
+typedef struct {
+  int tile_height[3];  /* per size class */
+  int flux_ctas[3];    /* flux-phase grid per size class; 0 = one CTA per tile */
+  int cell_ctas;       /* grid of the cell phases */
+  float default_ms, tuned_ms;
+} mth_tuning_report;
+mth_status mth_ensemble_tuning(const mth_ensemble* e, mth_tuning_report* t);
 /* Enqueues n_steps ensemble steps (asynchronous; see mth_ensemble_sync). */
 mth_status mth_ensemble_step(mth_ensemble* e, int n_steps);
 /* Per-phase timing of `reps` ensemble steps run eagerly (one phase at a time,

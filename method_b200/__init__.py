@@ -342,10 +342,18 @@ class Ensemble:
         return c, p, a
 
     def autotune(self, reps=3):
-        """Picks the flux tile height per member size class; returns the three choices."""
+        """Tunes the flux tile height and grid per member size class and the
+        cell phases' grid; returns the three tile heights."""
         ti = (C.c_int * 3)()
         self._check(self.L.mth_ensemble_autotune(self.e, int(reps), ti), "autotune")
         return list(ti)
+
+    def tuning(self):
+        """The autotuner's choice and its measured gain (dict)."""
+        t = _lib.EnsembleTuning()
+        self._check(self.L.mth_ensemble_tuning(self.e, C.byref(t)), "tuning")
+        return {"tile_height": list(t.tile_height), "flux_ctas": list(t.flux_ctas),
+                "cell_ctas": t.cell_ctas, "default_ms": t.default_ms, "tuned_ms": t.tuned_ms}
 
     def step(self, n=1, sync=True):
         self._check(self.L.mth_ensemble_step(self.e, int(n)), "step")

@@ -29,7 +29,7 @@ SYMBOLS = [
     "mth_c2p_ctx_set_mlp", "mth_c2p_ctx_run", "mth_c2p_ctx_stats", "mth_c2p_srmhd_noalloc",
     "mth_save_text", "mth_device_state", "mth_ensemble_create", "mth_ensemble_destroy",
     "mth_ensemble_last_error", "mth_ensemble_set_prims", "mth_ensemble_download",
-    "mth_ensemble_set_mlp", "mth_ensemble_set_mlp_srrmhd", "mth_ensemble_set_stream", "mth_ensemble_autotune", "mth_ensemble_step",
+    "mth_ensemble_set_mlp", "mth_ensemble_set_mlp_srrmhd", "mth_ensemble_set_stream", "mth_ensemble_autotune", "mth_ensemble_tuning", "mth_ensemble_step",
     "mth_ensemble_profile", "mth_ensemble_sync", "mth_ensemble_stats", "mth_ensemble_info",
 ]
 
@@ -69,6 +69,11 @@ class Stats(C.Structure):
         ("steps", C.c_longlong), ("t", C.c_double), ("dt", C.c_double), ("iters", C.c_int),
         ("c2p_fallbacks", C.c_longlong), ("implicit_fallbacks", C.c_longlong),
     ]
+
+
+class EnsembleTuning(C.Structure):
+    _fields_ = [("tile_height", C.c_int * 3), ("flux_ctas", C.c_int * 3), ("cell_ctas", C.c_int),
+                ("default_ms", C.c_float), ("tuned_ms", C.c_float)]
 
 
 class KernelTime(C.Structure):
@@ -156,6 +161,7 @@ def load():
     L.mth_ensemble_set_mlp_srrmhd.argtypes = [E, F, F]
     L.mth_ensemble_set_stream.argtypes = [E, C.c_void_p]
     L.mth_ensemble_autotune.argtypes = [E, C.c_int, C.POINTER(C.c_int)]
+    L.mth_ensemble_tuning.argtypes = [E, C.POINTER(EnsembleTuning)]
     L.mth_ensemble_step.argtypes = [E, C.c_int]
     L.mth_ensemble_profile.argtypes = [E, C.c_int, C.POINTER(KernelTime), C.c_int,
                                        C.POINTER(C.c_int)]

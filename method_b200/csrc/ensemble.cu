@@ -57,7 +57,10 @@ struct mth_ensemble {
   Item* d_cells[2] = {};
   int n_cells[2] = {};
   int ti[kClasses] = {8, 8, 8};
+  int fgrid[kClasses] = {0, 0, 0};  // flux-phase CTAs per class (0: one per item, capped)
+  int sms = 148;
   int grid_cells = 148 * 8;
+  float tune_default_ms = 0.f, tune_best_ms = 0.f;  // autotuner's measured phase sums
   int grid_mlp = 148 * 2;
   bool has_model[2] = {false, false};
   int guess = MTH_GUESS_PREVIOUS;  // MTH_GUESS_MLP: members use their model's network
@@ -130,9 +133,12 @@ cudaError_t build_flux_items(mth_ensemble* e) {
   return cudaSuccess;
 }
 
-int flux_grid(const mth_ensemble* e, int n_items) {
-  (void)e;
-  return std::max(1, n_items);  // the launcher caps it at the resident capacity
+// CTAs of a flux phase of size class c: one per work item unless the
+// autotuner chose fewer persistent CTAs; the launcher caps it at the
+// resident capacity.
+int flux_grid(const mth_ensemble* e, int n_items, int c) {
+  const int g = e->fgrid[c] > 0 ? std::min(e->fgrid[c], n_items) : n_items;
+  return std::max(1, g);
 }
 
 template <class F>
@@ -170,9 +176,9 @@ cudaError_t flux_phase(mth_ensemble* e, cudaStream_t s, int md, int ic, int ip, 
     const bool mixed = e->precision == MTH_MIXED;
     cudaError_t r = phase(e, s, names[mixed][md][c], [&] {
       return mixed ? ens_fvs_fp32(e->d_mem, e->d_flux[md][c], n, md, e->order, e->ti[c], ic, ip,
-                                  ia, iu0, iout, mode, flux_grid(e, n), s)
+                                  ia, iu0, iout, mode, flux_grid(e, n, c), s)
                    : ens_fvs_fp64(e->d_mem, e->d_flux[md][c], n, md, e->order, e->ti[c], ic, ip,
-                                  ia, iu0, iout, mode, flux_grid(e, n), s);
+                                  ia, iu0, iout, mode, flux_grid(e, n, c), s);
     });
     if (r != cudaSuccess) return r;
   }
@@ -405,6 +411,7 @@ mth_status mth_ensemble_create(const mth_config* cfgs, int n, mth_ensemble** out
   }
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->device);
+  e->sms = sms;
   e->grid_cells = sms * 8;
   e->grid_mlp = sms * 2;
   if ((r = build_flux_items(e))) return bail(r);
@@ -508,6 +515,59 @@ mth_status mth_ensemble_set_stream(mth_ensemble* e, void* stream) {
 
 // Times each candidate tile height per size class on the ensemble's own
 // first flux phase and keeps the fastest; returns the choice in ti_out[3].
+namespace {
+// Event time of `reps` launches of one flux phase (after one warm-up launch).
+cudaError_t time_flux(mth_ensemble* e, int c, int T, int grid, int reps, cudaEvent_t a,
+                      cudaEvent_t b, float* ms_out) {
+  float total = 0.f;
+  for (int md = 0; md < 2; ++md) {
+    if (!e->n_flux[md][c]) continue;
+    const int iout = md == MODEL_SRMHD ? EA_P1C : EA_F1;
+    const int mode = md == MODEL_SRMHD ? STAGE_EULER : STAGE_FNET;
+    const int n = e->n_flux[md][c];
+    const int g = grid > 0 ? std::min(grid, n) : n;
+    for (int rep = 0; rep <= reps; ++rep) {
+      cudaError_t r = cudaEventRecord(a, e->st);
+      if (r != cudaSuccess) return r;
+      r = (e->precision == MTH_MIXED)
+              ? ens_fvs_fp32(e->d_mem, e->d_flux[md][c], n, md, e->order, T, EA_CONS, EA_PRIMS,
+                             EA_AUX, -1, iout, mode, g, e->st)
+              : ens_fvs_fp64(e->d_mem, e->d_flux[md][c], n, md, e->order, T, EA_CONS, EA_PRIMS,
+                             EA_AUX, -1, iout, mode, g, e->st);
+      if (r != cudaSuccess) return r;
+      if ((r = cudaEventRecord(b, e->st)) || (r = cudaEventSynchronize(b))) return r;
+      float ms = 0.f;
+      if ((r = cudaEventElapsedTime(&ms, a, b))) return r;
+      if (rep > 0) total += ms;
+    }
+  }
+  *ms_out = total;
+  return cudaSuccess;
+}
+
+// Event time of `reps` primitive-recovery phases of every model at the
+// current cell-phase grid (mixed form): each member's state is recovered into
+// its stage scratch arrays (SRMHD: the RK2 predictor's prims / aux; SRRMHD:
+// U2 / U1, which hold what the lean recovery writes), so no state changes.
+cudaError_t time_cells(mth_ensemble* e, int reps, cudaEvent_t a, cudaEvent_t b, float* ms_out) {
+  float total = 0.f;
+  for (int rep = 0; rep <= reps; ++rep) {
+    cudaError_t r = cudaEventRecord(a, e->st);
+    if (r != cudaSuccess) return r;
+    if ((r = c2p_phase(e, e->st, MODEL_SRMHD, EA_CONS, EA_PRIMS, EA_AUX, EA_P1P, EA_P1A, true)))
+      return r;
+    if ((r = c2p_phase(e, e->st, MODEL_SRRMHD, EA_CONS, EA_PRIMS, EA_AUX, EA_U2, EA_U1, true)))
+      return r;
+    if ((r = cudaEventRecord(b, e->st)) || (r = cudaEventSynchronize(b))) return r;
+    float ms = 0.f;
+    if ((r = cudaEventElapsedTime(&ms, a, b))) return r;
+    if (rep > 0) total += ms;
+  }
+  *ms_out = total;
+  return cudaSuccess;
+}
+}  // namespace
+
 mth_status mth_ensemble_autotune(mth_ensemble* e, int reps, int* ti_out) {
   if (!e || reps <= 0) return MTH_ERR_INVALID;
   ECU(e, cudaSetDevice(e->device));
@@ -515,52 +575,84 @@ mth_status mth_ensemble_autotune(mth_ensemble* e, int reps, int* ti_out) {
   cudaEvent_t a, b;
   ECU(e, cudaEventCreate(&a));
   ECU(e, cudaEventCreate(&b));
+  float def_total = 0.f, best_total = 0.f;
+  // flux phases: tile height x persistent grid, per member size class
+  const int grids[3] = {0, e->sms * 4, e->sms * 2};
   for (int c = 0; c < kClasses; ++c) {
     bool any = false;
     for (int m = 0; m < e->n; ++m) any |= size_class(e->cfg[m].nx) == c;
     if (!any) continue;
-    float best = 1e30f;
-    int best_ti = e->ti[c];
+    float best = 1e30f, def = 0.f;
+    int best_ti = 8, best_grid = 0;
     for (int T : kTiles) {
       e->ti[c] = T;
       ECU(e, build_flux_items(e));
-      float total = 0.f;
-      for (int md = 0; md < 2; ++md) {
-        if (!e->n_flux[md][c]) continue;
-        const int iout = md == MODEL_SRMHD ? EA_P1C : EA_F1;
-        const int mode = md == MODEL_SRMHD ? STAGE_EULER : STAGE_FNET;
-        for (int rep = 0; rep <= reps; ++rep) {  // first repetition warms up
-          ECU(e, cudaEventRecord(a, e->st));
-          const int n = e->n_flux[md][c];
-          cudaError_t r = (e->precision == MTH_MIXED)
-                              ? ens_fvs_fp32(e->d_mem, e->d_flux[md][c], n, md, e->order, T,
-                                             EA_CONS, EA_PRIMS, EA_AUX, -1, iout, mode,
-                                             flux_grid(e, n), e->st)
-                              : ens_fvs_fp64(e->d_mem, e->d_flux[md][c], n, md, e->order, T,
-                                             EA_CONS, EA_PRIMS, EA_AUX, -1, iout, mode,
-                                             flux_grid(e, n), e->st);
-          ECU(e, r);
-          ECU(e, cudaEventRecord(b, e->st));
-          ECU(e, cudaEventSynchronize(b));
-          float ms = 0.f;
-          ECU(e, cudaEventElapsedTime(&ms, a, b));
-          if (rep > 0) total += ms;
+      for (int G : grids) {
+        float ms = 0.f;
+        ECU(e, time_flux(e, c, T, G, reps, a, b, &ms));
+        if (T == 8 && G == 0) def = ms;
+        if (ms < best) {
+          best = ms;
+          best_ti = T;
+          best_grid = G;
         }
-      }
-      if (total < best) {
-        best = total;
-        best_ti = T;
       }
     }
     e->ti[c] = best_ti;
+    e->fgrid[c] = best_grid;
+    def_total += def;
+    best_total += best;
   }
+  ECU(e, build_flux_items(e));
+  // cell phases (recoveries, implicit stages): CTAs per SM of the persistent
+  // grid, timed on the mixed form's recoveries; the members' statistics are
+  // restored afterwards
+  if (e->precision == MTH_MIXED) {
+    std::vector<long long> saved(16 * (size_t)e->n);
+    for (int m = 0; m < e->n; ++m)
+      ECU(e, cudaMemcpyAsync(&saved[16 * (size_t)m], e->mem[m].counters, 16 * sizeof(long long),
+                             cudaMemcpyDeviceToHost, e->st));
+    ECU(e, cudaStreamSynchronize(e->st));
+    float best = 1e30f, def = 0.f;
+    int best_g = e->sms * 8;
+    for (int per_sm : {8, 4, 16}) {
+      e->grid_cells = e->sms * per_sm;
+      float ms = 0.f;
+      ECU(e, time_cells(e, reps, a, b, &ms));
+      if (per_sm == 8) def = ms;
+      if (ms < best) {
+        best = ms;
+        best_g = e->grid_cells;
+      }
+    }
+    e->grid_cells = best_g;
+    def_total += def;
+    best_total += best;
+    for (int m = 0; m < e->n; ++m)
+      ECU(e, cudaMemcpyAsync(e->mem[m].counters, &saved[16 * (size_t)m], 16 * sizeof(long long),
+                             cudaMemcpyHostToDevice, e->st));
+    ECU(e, cudaStreamSynchronize(e->st));
+  }
+  e->tune_default_ms = def_total / reps;
+  e->tune_best_ms = best_total / reps;
   cudaEventDestroy(a);
   cudaEventDestroy(b);
-  ECU(e, build_flux_items(e));
   if (e->graph) cudaGraphExecDestroy(e->graph);
   e->graph = nullptr;
   if (ti_out)
     for (int c = 0; c < kClasses; ++c) ti_out[c] = e->ti[c];
+  return MTH_OK;
+}
+
+mth_status mth_ensemble_tuning(const mth_ensemble* e, mth_tuning_report* t) {
+  if (!e || !t) return MTH_ERR_INVALID;
+  for (int c = 0; c < kClasses; ++c) {
+    t->tile_height[c] = e->ti[c];
+    t->flux_ctas[c] = e->fgrid[c];
+  }
+  t->cell_ctas = e->grid_cells;
+  t->default_ms = e->tune_default_ms;
+  t->tuned_ms = e->tune_best_ms;
   return MTH_OK;
 }
 
