@@ -142,20 +142,57 @@ def emit_function(r, qual="__device__ __forceinline__ double", name=None):
     return "\n".join(L)
 
 
+def indicator_ldl(r, k):
+    """beta_k as sum_i D_i z_i^2 with z = L^T dv over the stencil's first
+    differences dv_j = v(k+j+1) - v(k+j) (P = L D L^T, L unit lower
+    triangular, exact): the form evaluated in FP32 without the cancellation
+    of the expanded quadratic form."""
+    c = r - 1
+    Q = _indicator(list(range(k, k + r)), c)
+    m = r - 1
+    # v = v_k 1 + T dv, T[q][j] = 1 for j < q; Q annihilates constants
+    T = [[Fr(int(j < q)) for j in range(m)] for q in range(r)]
+    P = [[sum(T[a][i] * Q[a][b] * T[b][j] for a in range(r) for b in range(r))
+          for j in range(m)] for i in range(m)]
+    Lm = [[Fr(int(i == j)) for j in range(m)] for i in range(m)]
+    Dg = [Fr(0)] * m
+    for j in range(m):
+        Dg[j] = P[j][j] - sum(Lm[j][t] ** 2 * Dg[t] for t in range(j))
+        for i in range(j + 1, m):
+            Lm[i][j] = (P[i][j] - sum(Lm[i][t] * Lm[j][t] * Dg[t] for t in range(j))) / Dg[j]
+    return Lm, Dg
+
+
 def emit_fast(r):
     """FP32 form for the mixed-precision flux path: the same weights, FMA
-    allowed, one approximate reciprocal per indicator and for the sum."""
+    allowed, indicators from first differences in L D L^T form, one
+    approximate reciprocal per indicator and for the sum."""
     betas, cands, d = scheme(r)
     n = 2 * r - 1
+    m = r - 1
     args = ", ".join(f"float v{q}" for q in range(n))
     L = [f"__device__ __forceinline__ float weno{n}_fast({args}) {{"]
+    for q in range(n - 1):
+        L.append(f"  const float d{q} = v{q + 1} - v{q};")
     for k in range(r):
-        expr = " + ".join(f"{lit(coef)}f * v{a} * v{b}" for coef, a, b in betas[k])
-        L.append(f"  const float b{k} = {expr};")
+        Lm, Dg = indicator_ldl(r, k)
+        zs = []
+        for i in range(m):
+            terms = [f"d{k + i}"] + [f"{lit(Lm[j][i])}f * d{k + j}" for j in range(i + 1, m)
+                                     if Lm[j][i] != 0]
+            L.append(f"  const float z{k}_{i} = {' + '.join(terms)};")
+            zs.append(f"{lit(Dg[i])}f * z{k}_{i} * z{k}_{i}")
+        L.append(f"  const float b{k} = {' + '.join(zs)};")
         L.append(f"  const float a{k} = {lit(d[k])}f * __fdividef(1.0f, 1e-16f + b{k} * b{k});")
+    # candidates anchored at the centre cell (in every stencil; the weights
+    # sum to one): v_c + sum_q c_q (v_q - v_c), small corrections to v_c
+    cc = r - 1
+    for q in range(n):
+        if q != cc:
+            L.append(f"  const float e{q} = v{q} - v{cc};")
     for k in range(r):
-        expr = " + ".join(f"{lit(coef)}f * v{q}" for coef, q in cands[k])
-        L.append(f"  const float s{k} = {expr};")
+        expr = " + ".join(f"{lit(coef)}f * e{q}" for coef, q in cands[k] if q != cc)
+        L.append(f"  const float s{k} = v{cc} + ({expr});")
     num = " + ".join(f"a{k} * s{k}" for k in range(r))
     den = " + ".join(f"a{k}" for k in range(r))
     L.append(f"  return ({num}) * __fdividef(1.0f, {den});")
