@@ -4,6 +4,7 @@
 // the work arrays of the chosen TimeIntegrator, and a CUDA stream.  A time
 // step is captured once per distinct dt into a CUDA graph and replayed, so the
 // host enters the device once per step.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdint>
@@ -57,6 +58,10 @@ struct mth_handle {
   bool profiling = false;
   std::vector<ProfRec> prof;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // pipelined host-array step: copy streams and per-row-block events
+  cudaStream_t up_st = nullptr, down_st = nullptr;
+  std::vector<cudaEvent_t> ev_up, ev_fin;
+  cudaEvent_t ev_start = nullptr, ev_end = nullptr, ev_done = nullptr;
 };
 
 namespace {
@@ -132,15 +137,16 @@ cudaError_t c2p_raw(mth_handle* h, const double* cons, const double* pg, const d
   return launch_c2p_srrmhd(h->g, cons, ag, prims, aux, c2p_work(h), h->st);
 }
 
-// FVS::F of (c, p, a) combined with a stage update into `out`.
+// FVS::F of (c, p, a) combined with a stage update into `out`; the mixed
+// form's fused tile may be restricted to tile rows [ti0, ti0 + nti).
 cudaError_t flux_stage_raw(mth_handle* h, double* c, double* p, double* a, const double* u0,
-                       double* out, double dt, int mode) {
+                       double* out, double dt, int mode, int ti0 = 0, int nti = -1) {
   const Grid& g = h->g;
   const StageTail tail{h->flux1, h->src1, g.cp};
   if (h->fused) {
     if (h->cfg.precision == MTH_MIXED)
       return launch_fvs2d_fp32(g, h->cfg.model, h->cfg.weno_order, c, p, a, u0, out, dt, mode,
-                               h->st, tail);
+                               h->st, tail, ti0, nti);
     return launch_fvs2d_fp64(g, h->cfg.model, h->cfg.weno_order, c, p, a, u0, out, dt, mode,
                              h->st, tail);
   }
@@ -585,6 +591,12 @@ mth_status mth_destroy(mth_handle* h) {
   mixed_free(&h->mixed);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
+  for (cudaEvent_t ev : h->ev_up) cudaEventDestroy(ev);
+  for (cudaEvent_t ev : h->ev_fin) cudaEventDestroy(ev);
+  for (cudaEvent_t ev : {h->ev_start, h->ev_end, h->ev_done})
+    if (ev) cudaEventDestroy(ev);
+  if (h->up_st) cudaStreamDestroy(h->up_st);
+  if (h->down_st) cudaStreamDestroy(h->down_st);
   if (h->own_st) cudaStreamDestroy(h->own_st);
   delete h;
   return MTH_OK;
@@ -989,15 +1001,163 @@ mth_status mth_step_host_bytes(mth_handle* h, unsigned long long* h2d, unsigned 
   return MTH_OK;
 }
 
+namespace {
+// Copies x-rows [a, b) of the variables in `mask` between a host array and
+// the device array of the same layout, one strided copy per run of
+// consecutive variables.
+cudaError_t copy_rows(const mth_handle* h, double* dst, const double* src, unsigned mask, int nv,
+                      int a, int b, cudaMemcpyKind kind, cudaStream_t st) {
+  const size_t plane = (size_t)h->g.Ny * h->g.Nz, pitch = sizeof(double) * (size_t)h->g.Ntot;
+  for (int v = 0; v < nv;) {
+    if (!(mask >> v & 1u)) {
+      ++v;
+      continue;
+    }
+    int e = v;
+    while (e < nv && (mask >> e & 1u)) ++e;
+    const size_t off = (size_t)v * h->g.Ntot + (size_t)a * plane;
+    cudaError_t r = cudaMemcpy2DAsync(dst + off, pitch, src + off, pitch,
+                                      sizeof(double) * plane * (b - a), e - v, kind, st);
+    if (r != cudaSuccess) return r;
+    v = e;
+  }
+  return cudaSuccess;
+}
+
+constexpr int kPipeRows = 64;  // interior x-rows per block of the pipelined host step
+
+bool pipelined(const mth_handle* h) {
+  return h->fused && h->cfg.precision == MTH_MIXED && h->cfg.guess == MTH_GUESS_PREVIOUS &&
+         h->cfg.integrator == MTH_RK2 && (h->g.ie - h->g.is) >= 4 * kPipeRows;
+}
+
+// TimeIntegrator::step on host arrays for the mixed RK2 form, pipelined over
+// blocks of x-rows so that host->device copies, the two stages and
+// device->host copies overlap: block k's predictor runs once blocks k-1..k+1
+// are on the device, its corrector once their predictor states are
+// recovered, and its final rows leave for the host while later blocks are
+// still arriving.  Every kernel is the whole-grid step's, on a row range;
+// the results are those of mth_step.
+mth_status step_host_pipelined(mth_handle* h, double* cons, double* prims, double* aux,
+                               double dt, unsigned pm, unsigned am) {
+  const Grid& g = h->g;
+  const int nrow = g.ie - g.is, B = (nrow + kPipeRows - 1) / kPipeRows;
+  const long long nj = (long long)(g.je - g.js) * (g.ke - g.ks);
+  if (!h->up_st) {
+    CU(h, cudaStreamCreateWithFlags(&h->up_st, cudaStreamNonBlocking));
+    CU(h, cudaStreamCreateWithFlags(&h->down_st, cudaStreamNonBlocking));
+    for (cudaEvent_t* ev : {&h->ev_start, &h->ev_end, &h->ev_done})
+      CU(h, cudaEventCreateWithFlags(ev, cudaEventDisableTiming));
+  }
+  while ((int)h->ev_up.size() < B) {
+    cudaEvent_t a, b;
+    CU(h, cudaEventCreateWithFlags(&a, cudaEventDisableTiming));
+    CU(h, cudaEventCreateWithFlags(&b, cudaEventDisableTiming));
+    h->ev_up.push_back(a);
+    h->ev_fin.push_back(b);
+  }
+  const unsigned all_c = (1u << h->NC) - 1, all_p = (1u << h->NP) - 1, all_a = (1u << h->NA) - 1;
+  auto r0 = [&](int k) { return g.is + k * kPipeRows; };
+  auto r1 = [&](int k) { return std::min(g.is + (k + 1) * kPipeRows, g.ie); };
+  // uploads, block by block, after the handle's earlier work
+  CU(h, cudaEventRecord(h->ev_start, h->st));
+  CU(h, cudaStreamWaitEvent(h->up_st, h->ev_start, 0));
+  CU(h, cudaStreamWaitEvent(h->down_st, h->ev_start, 0));
+  for (int k = 0; k < B; ++k) {
+    CU(h, copy_rows(h, h->cons, cons, all_c, h->NC, r0(k), r1(k), cudaMemcpyHostToDevice,
+                    h->up_st));
+    CU(h, copy_rows(h, h->prims, prims, pm, h->NP, r0(k), r1(k), cudaMemcpyHostToDevice,
+                    h->up_st));
+    CU(h, copy_rows(h, h->aux, aux, am, h->NA, r0(k), r1(k), cudaMemcpyHostToDevice, h->up_st));
+    CU(h, cudaEventRecord(h->ev_up[k], h->up_st));
+  }
+  auto tiles = [&](int k, int* ti0, int* nti) {
+    *ti0 = (r0(k) - g.is) / 8;
+    *nti = (r1(k) - r0(k) + 7) / 8;
+  };
+  auto pred = [&](int k) -> cudaError_t {
+    cudaError_t e;
+    for (int q : {(k + B - 1) % B, k, (k + 1) % B})
+      if ((e = cudaStreamWaitEvent(h->st, h->ev_up[q], 0))) return e;
+    int ti0, nti;
+    tiles(k, &ti0, &nti);
+    if ((e = flux_stage_raw(h, h->cons, h->prims, h->aux, nullptr, h->p1cons, dt, STAGE_EULER,
+                            ti0, nti)))
+      return e;
+    return launch_c2p_mixed(g, h->cfg.model, h->cfg.guess, h->p1cons, h->prims, h->aux,
+                            h->p1prims, h->p1aux, h->solution, c2p_work(h), h->mixed, true, h->st,
+                            (r0(k) - g.is) * nj, (r1(k) - r0(k)) * nj);
+  };
+  auto corr = [&](int k) -> cudaError_t {
+    cudaError_t e;
+    int ti0, nti;
+    tiles(k, &ti0, &nti);
+    if ((e = flux_stage_raw(h, h->p1cons, h->p1prims, h->p1aux, h->cons, h->cons, dt,
+                            STAGE_RK2_CORR, ti0, nti)))
+      return e;
+    if ((e = launch_c2p_mixed(g, h->cfg.model, h->cfg.guess, h->cons, h->prims, h->aux, h->prims,
+                              h->aux, h->solution, c2p_work(h), h->mixed, false, h->st,
+                              (r0(k) - g.is) * nj, (r1(k) - r0(k)) * nj)))
+      return e;
+    // finalise: the rows' own ghost cells (y and z), then the rows go home
+    for (auto arr : {std::make_pair(h->cons, h->NC), std::make_pair(h->prims, h->NP),
+                     std::make_pair(h->aux, h->NA)})
+      if ((e = launch_apply_bcs_rows(g, arr.first, arr.second, r0(k), r1(k), h->st))) return e;
+    if ((e = cudaEventRecord(h->ev_fin[k], h->st))) return e;
+    if ((e = cudaStreamWaitEvent(h->down_st, h->ev_fin[k], 0))) return e;
+    if ((e = copy_rows(h, cons, h->cons, all_c, h->NC, r0(k), r1(k), cudaMemcpyDeviceToHost,
+                       h->down_st)) ||
+        (e = copy_rows(h, prims, h->prims, all_p, h->NP, r0(k), r1(k), cudaMemcpyDeviceToHost,
+                       h->down_st)))
+      return e;
+    return copy_rows(h, aux, h->aux, all_a, h->NA, r0(k), r1(k), cudaMemcpyDeviceToHost,
+                     h->down_st);
+  };
+  // block order: predictors from block 1 on, each corrector as soon as its
+  // neighbours' predictors are done, block 0 (whose halo wraps to the last
+  // block) once the last block has arrived
+  CU(h, pred(1));
+  CU(h, pred(2));
+  for (int k = 3; k < B; ++k) {
+    CU(h, pred(k));
+    CU(h, corr(k - 1));
+  }
+  CU(h, pred(0));
+  CU(h, corr(B - 1));
+  CU(h, corr(0));
+  CU(h, corr(1));
+  // the x ghost rows (the boundary conditions across x, corners included)
+  for (auto arr : {std::make_pair(h->cons, h->NC), std::make_pair(h->prims, h->NP),
+                   std::make_pair(h->aux, h->NA)}) {
+    CU(h, launch_apply_bcs_rows(g, arr.first, arr.second, 0, g.is, h->st));
+    CU(h, launch_apply_bcs_rows(g, arr.first, arr.second, g.ie, g.Nx, h->st));
+  }
+  CU(h, cudaEventRecord(h->ev_end, h->st));
+  CU(h, cudaStreamWaitEvent(h->down_st, h->ev_end, 0));
+  for (int side = 0; side < 2; ++side) {
+    const int a = side == 0 ? 0 : g.ie, b = side == 0 ? g.is : g.Nx;
+    CU(h, copy_rows(h, cons, h->cons, all_c, h->NC, a, b, cudaMemcpyDeviceToHost, h->down_st));
+    CU(h, copy_rows(h, prims, h->prims, all_p, h->NP, a, b, cudaMemcpyDeviceToHost, h->down_st));
+    CU(h, copy_rows(h, aux, h->aux, all_a, h->NA, a, b, cudaMemcpyDeviceToHost, h->down_st));
+  }
+  CU(h, cudaEventRecord(h->ev_done, h->down_st));
+  CU(h, cudaStreamWaitEvent(h->st, h->ev_done, 0));
+  h->ghosts_dirty = false;
+  h->steps++;
+  return read_status(h);
+}
+}  // namespace
+
 mth_status mth_step_host(mth_handle* h, double* cons, double* prims, double* aux, double dt) {
   if (!h || !cons || !prims || !aux || !(dt > 0) || h->cfg.x_slab) return MTH_ERR_INVALID;
   CU(h, cudaSetDevice(h->device));
   unsigned pm, am;
   step_inputs(h, pm, am);
+  h->dt = dt;
+  if (pipelined(h)) return step_host_pipelined(h, cons, prims, aux, dt, pm, am);
   CU(h, cudaMemcpyAsync(h->cons, cons, bytes(h, h->NC), cudaMemcpyHostToDevice, h->st));
   CU(h, upload_vars(h, h->prims, prims, pm, h->NP));
   CU(h, upload_vars(h, h->aux, aux, am, h->NA));
-  h->dt = dt;
   mth_status s = launch_step(h, dt);
   if (s != MTH_OK) return s;
   // the reference leaves its arrays with boundary conditions applied (finalise)

@@ -277,10 +277,10 @@ template <class M, typename R, int ORDER, int TI>
 __global__ void __launch_bounds__(32 * TI, (fvs2d_min_blocks<M, R, ORDER, TI>()))
     k_fvs2d(Grid g, const double* __restrict__ cons, const double* __restrict__ prims,
             const double* __restrict__ aux, const double* u0, double* out, double dt,
-            int mode, StageTail tail) {
+            int mode, StageTail tail, int ti0) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  fvs2d_tile<M, R, ORDER, TI>(g, cons, prims, aux, u0, out, dt, mode, blockIdx.y, blockIdx.x,
-                              smem_raw, tail);
+  fvs2d_tile<M, R, ORDER, TI>(g, cons, prims, aux, u0, out, dt, mode, ti0 + blockIdx.y,
+                              blockIdx.x, smem_raw, tail);
 }
 
 }  // namespace mth

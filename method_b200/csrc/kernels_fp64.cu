@@ -793,7 +793,7 @@ cudaError_t fvs2d_instance(const Grid& g, const double* cons, const double* prim
   }
   dim3 grid((g.je - g.js + 31) / 32, (g.ie - g.is + TI - 1) / TI);
   dim3 block(32, TI);
-  kern<<<grid, block, S::bytes, st>>>(g, cons, prims, aux, u0, out, dt, mode, tail);
+  kern<<<grid, block, S::bytes, st>>>(g, cons, prims, aux, u0, out, dt, mode, tail, 0);
   return cudaGetLastError();
 }
 
@@ -953,6 +953,30 @@ cudaError_t launch_prims_to_all(const Grid& g, int model, const double* prims, d
 
 cudaError_t launch_apply_bcs(const Grid& g, double* arr, int nvars, cudaStream_t st) {
   k_apply_bcs<<<blocks_for(g.Ntot), kThreads, 0, st>>>(g, arr, nvars);
+  return cudaGetLastError();
+}
+
+// The ghost cells of x-rows [r0, r1) only (k_apply_bcs on a row range).
+__global__ void k_apply_bcs_rows(Grid g, double* __restrict__ arr, int nvars, int r0, int r1) {
+  const long long plane = (long long)g.Ny * g.Nz;
+  const long long cell = r0 * plane + blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (cell >= r1 * plane) return;
+  const int k = (int)(cell % g.Nz);
+  const long long t = cell / g.Nz;
+  const int j = (int)(t % g.Ny);
+  const int i = (int)(t / g.Ny);
+  const bool ghost = (i < g.is || i >= g.ie) || (g.dims > 1 && (j < g.js || j >= g.je)) ||
+                     (g.dims > 2 && (k < g.ks || k >= g.ke));
+  if (!ghost) return;
+  const long long src = mapped_cell(g, i, j, k);
+  for (int v = 0; v < nvars; ++v) arr[v * g.Ntot + cell] = arr[v * g.Ntot + src];
+}
+
+cudaError_t launch_apply_bcs_rows(const Grid& g, double* arr, int nvars, int r0, int r1,
+                                  cudaStream_t st) {
+  const long long n = (long long)(r1 - r0) * g.Ny * g.Nz;
+  if (n <= 0) return cudaSuccess;
+  k_apply_bcs_rows<<<blocks_for(n), kThreads, 0, st>>>(g, arr, nvars, r0, r1);
   return cudaGetLastError();
 }
 

@@ -286,17 +286,16 @@ __global__ void __launch_bounds__(128, kNewtonMinBlocks)
     k_c2p_newton_srmhd(Grid g, int guess_mode, const double* __restrict__ cons,
                        const double* prims_guess, const double* aux_guess, double* prims,
                        double* aux, double* __restrict__ solution, C2PWork w,
-                       const double* __restrict__ zguess) {
-  long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+                       const double* __restrict__ zguess, long long t0, long long t_end) {
+  const long long t = t0 + blockIdx.x * (long long)blockDim.x + threadIdx.x;
   NewtonTally tl;
-  if (t < n_interior(g)) {
+  if (t < t_end) {
     int i, j, k;
     interior_ijk(g, t, i, j, k);
     c2p_srmhd_newton_cell<LEAN>(g, cell_id(g, i, j, k), guess_mode, cons, prims_guess, aux_guess,
-                                prims,
-                          aux, solution, zguess, tl);
+                                prims, aux, solution, zguess, tl);
   }
-  tally_flush(tl, t < n_interior(g), w.counters);
+  tally_flush(tl, t < t_end, w.counters);
 }
 
 // Mixed-form SRRMHD recovery of one cell (Newton in Z, secant fallback).
@@ -381,16 +380,17 @@ __device__ __forceinline__ void c2p_srrmhd_newton_cell(const Grid& g, long long 
 template <bool LEAN>
 __global__ void __launch_bounds__(128, kNewtonMinBlocks)
     k_c2p_newton_srrmhd(Grid g, const double* __restrict__ cons, const double* aux_guess,
-                        double* prims, double* aux, C2PWork w, const double* zseed) {
-  long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+                        double* prims, double* aux, C2PWork w, const double* zseed, long long t0,
+                        long long t_end) {
+  const long long t = t0 + blockIdx.x * (long long)blockDim.x + threadIdx.x;
   NewtonTally tl;
-  if (t < n_interior(g)) {
+  if (t < t_end) {
     int i, j, k;
     interior_ijk(g, t, i, j, k);
     c2p_srrmhd_newton_cell<LEAN>(g, cell_id(g, i, j, k), cons, aux_guess, prims, aux, tl,
                                  w.counters, zseed);
   }
-  tally_flush(tl, t < n_interior(g), w.counters);
+  tally_flush(tl, t < t_end, w.counters);
 }
 
 // Batched SRMHD primitive recovery for independent cells.
@@ -810,15 +810,18 @@ cudaError_t ens_fvs_fp32_instance(const Member* mem, const Item* items, int n, i
 template <class M, int ORDER, int TI>
 cudaError_t fvs2d_fp32_instance(const Grid& g, const double* cons, const double* prims,
                                 const double* aux, const double* u0, double* out, double dt,
-                                int mode, StageTail tail, cudaStream_t st) {
+                                int mode, StageTail tail, cudaStream_t st, int ti0, int nti) {
   using S = Fvs2dSmem<M, float, ORDER, TI>;
   auto kern = k_fvs2d<M, float, ORDER, TI>;
   cudaError_t e =
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::bytes);
   if (e != cudaSuccess) return e;
-  dim3 grid((g.je - g.js + 31) / 32, (g.ie - g.is + TI - 1) / TI);
+  const int rows = (g.ie - g.is + TI - 1) / TI;
+  if (nti < 0) nti = rows - ti0;
+  if (nti <= 0) return cudaSuccess;
+  dim3 grid((g.je - g.js + 31) / 32, nti);
   dim3 block(32, TI);
-  kern<<<grid, block, S::bytes, st>>>(g, cons, prims, aux, u0, out, dt, mode, tail);
+  kern<<<grid, block, S::bytes, st>>>(g, cons, prims, aux, u0, out, dt, mode, tail, ti0);
   return cudaGetLastError();
 }
 
@@ -887,9 +890,9 @@ cudaError_t ens_imex_fast(const Member* mem, const Item* items, int n, int stage
 cudaError_t launch_fvs2d_fp32(const Grid& g, int model, int order, const double* cons,
                               const double* prims, const double* aux, const double* u0,
                               double* out, double dt, int mode, cudaStream_t st,
-                              StageTail tail) {
+                              StageTail tail, int ti0, int nti) {
 #define FVS32(MM, O) \
-  return fvs2d_fp32_instance<MM, O, 8>(g, cons, prims, aux, u0, out, dt, mode, tail, st)
+  return fvs2d_fp32_instance<MM, O, 8>(g, cons, prims, aux, u0, out, dt, mode, tail, st, ti0, nti)
   if (model == MODEL_SRMHD) {
     switch (order) {
       case 3: FVS32(SRMHD, 3);
@@ -920,9 +923,12 @@ cudaError_t launch_c2p_batch(long long n, double gamma, int method, int guess,
 cudaError_t launch_c2p_mixed(const Grid& g, int model, int guess, const double* cons,
                              const double* prims_guess, const double* aux_guess, double* prims,
                              double* aux, double* solution, C2PWork w, const MixedWork& mw,
-                             bool lean, cudaStream_t st) {
+                             bool lean, cudaStream_t st, long long t0, long long nt) {
   const long long nI = (long long)(g.ie - g.is) * (g.je - g.js) * (g.ke - g.ks);
-  const int blocks = (int)((nI + 127) / 128);
+  if (nt < 0) nt = nI - t0;
+  const long long t_end = t0 + nt;
+  const int blocks = (int)((nt + 127) / 128);
+  if (nt <= 0) return cudaSuccess;
   if (model == MODEL_SRMHD && guess == 1 && mw.has_mlp) {
     cudaError_t e = mlp::launch_zguess(g, nI, false, cons, mw.mlp_params, mw.feat_stats,
                                        mw.zguess, st);
@@ -932,10 +938,10 @@ cudaError_t launch_c2p_mixed(const Grid& g, int model, int guess, const double* 
     const int gm = (guess == 1 && mw.has_mlp) ? 1 : 0;
     if (lean)
       k_c2p_newton_srmhd<true><<<blocks, 128, 0, st>>>(g, gm, cons, prims_guess, aux_guess, prims,
-                                                       aux, solution, w, mw.zguess);
+                                                       aux, solution, w, mw.zguess, t0, t_end);
     else
       k_c2p_newton_srmhd<false><<<blocks, 128, 0, st>>>(g, gm, cons, prims_guess, aux_guess, prims,
-                                                        aux, solution, w, mw.zguess);
+                                                        aux, solution, w, mw.zguess, t0, t_end);
   } else {
     const double* zseed = nullptr;
     if (guess == 1 && mw.has_mlp) {
@@ -945,10 +951,11 @@ cudaError_t launch_c2p_mixed(const Grid& g, int model, int guess, const double* 
       zseed = mw.zguess;
     }
     if (lean)
-      k_c2p_newton_srrmhd<true><<<blocks, 128, 0, st>>>(g, cons, aux_guess, prims, aux, w, zseed);
+      k_c2p_newton_srrmhd<true><<<blocks, 128, 0, st>>>(g, cons, aux_guess, prims, aux, w, zseed,
+                                                        t0, t_end);
     else
       k_c2p_newton_srrmhd<false><<<blocks, 128, 0, st>>>(g, cons, aux_guess, prims, aux, w,
-                                                         zseed);
+                                                         zseed, t0, t_end);
   }
   return cudaGetLastError();
 }

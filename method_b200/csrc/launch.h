@@ -36,6 +36,9 @@ cudaError_t format_body(const Grid& g, const double* arr, int nvars, std::string
 cudaError_t launch_prims_to_all(const Grid& g, int model, const double* prims, double* cons,
                                 double* aux, cudaStream_t st);
 cudaError_t launch_apply_bcs(const Grid& g, double* arr, int nvars, cudaStream_t st);
+// Bcs::apply for the ghost cells of x-rows [r0, r1) (ghost-inclusive indices).
+cudaError_t launch_apply_bcs_rows(const Grid& g, double* arr, int nvars, int r0, int r1,
+                                  cudaStream_t st);
 cudaError_t launch_fvs2d_fp64(const Grid& g, int model, int order, const double* cons,
                               const double* prims, const double* aux, const double* u0,
                               double* out, double dt, int mode, cudaStream_t st,

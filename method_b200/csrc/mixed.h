@@ -55,19 +55,22 @@ cudaError_t launch_c2p_batch(long long n, double gamma, int method, int guess,
 cudaError_t mixed_init(MixedWork* w, const Grid& g, int model, cudaStream_t st);
 void mixed_free(MixedWork* w);
 
+// ti0, nti: the tile rows (of 8 interior rows) to update; all by default.
 cudaError_t launch_fvs2d_fp32(const Grid& g, int model, int order, const double* cons,
                               const double* prims, const double* aux, const double* u0,
                               double* out, double dt, int mode, cudaStream_t st,
-                              StageTail tail = {});
+                              StageTail tail = {}, int ti0 = 0, int nti = -1);
 
 // guess: 0 = previous state, 1 = guess network (falls back to the previous
 // state, then to the reference Powell-hybrid, when Newton does not converge).
 // lean: write only what the flux tile, the source and the next implicit solve
 // read back (SRMHD: prims 1-7, aux 1 and 4-8, no solution; SRRMHD: prims 1-4,
 // aux 4-8 and 10), for an intermediate recovered state.
+// t0, nt: the range of interior cells (k fastest, then j, then i) to
+// recover; all by default.
 cudaError_t launch_c2p_mixed(const Grid& g, int model, int guess, const double* cons,
                              const double* prims_guess, const double* aux_guess, double* prims,
                              double* aux, double* solution, C2PWork w, const MixedWork& mw,
-                             bool lean, cudaStream_t st);
+                             bool lean, cudaStream_t st, long long t0 = 0, long long nt = -1);
 
 }  // namespace mth

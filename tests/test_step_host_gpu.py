@@ -35,6 +35,20 @@ def _cases():
         for integ in ("ssp2", "rk2"):
             yield (f"srrmhd-{integ}-{prec}", dict(SHEET, integrator=integ, precision=prec), sh0,
                    sh1, 2e-3)
+    # mixed RK2 grids of 256 interior x-rows and more take the pipelined path
+    # (blocks of 64 rows; a partial last block; periodic, flow and outflow x)
+    yield ("srmhd-rk2-mixed-pipelined-periodic", dict(OT, nx=320, precision="mixed"),
+           lambda: initial.orszag_tang(320, Ng=4)[:, :, :72],
+           lambda: initial.kelvin_helmholtz(320, 64, Ng=4, seed=6), 1e-3)
+    kh = dict(OT, nx=300, xmin=-0.5, xmax=0.5, ymin=-1.0, ymax=1.0, bcs="flow",
+              precision="mixed", weno=3)
+    yield ("srmhd-rk2-mixed-pipelined-flow", kh,
+           lambda: initial.kelvin_helmholtz(300, 64, Ng=4, seed=7),
+           lambda: initial.kelvin_helmholtz(300, 64, Ng=4, seed=8), 1e-3)
+    yield ("srrmhd-rk2-mixed-pipelined-outflow", dict(SHEET, nx=256, integrator="rk2",
+                                                      precision="mixed"),
+           lambda: initial.current_sheet(256, 64, seed=9),
+           lambda: initial.current_sheet(256, 64, seed=10), 2e-4)
 
 
 @pytest.mark.parametrize("name,cfg,init,other,dt", [pytest.param(*c, id=c[0]) for c in _cases()])
@@ -53,7 +67,9 @@ def test_step_host_matches_device_steps(name, cfg, init, other, dt):
     h2d, d2h = C.c_ulonglong(), C.c_ulonglong()
     assert host.L.mth_step_host_bytes(host.h, C.byref(h2d), C.byref(d2h)) == 0
     per = hc[0].nbytes
-    nc, np_, na = UPLOADED.get(name, (hc.shape[0], hp.shape[0], ha.shape[0]))
+    nc, np_, na = UPLOADED.get(name.replace("-pipelined-periodic", "").replace(
+        "-pipelined-flow", "").replace("-pipelined-outflow", ""),
+        (hc.shape[0], hp.shape[0], ha.shape[0]))
     assert h2d.value == per * (nc + np_ + na), name
     assert d2h.value == hc.nbytes + hp.nbytes + ha.nbytes, name
     for _ in range(2):
