@@ -621,6 +621,25 @@ def ncu_record(kernel):
         return json.load(f).get(kernel) or {}
 
 
+def fp64_pipe_roofline(inst_per_cell, cells, launch_ms, clk):
+    """The FP64 pipe's roofline of a kernel whose FP64 work bounds it: thread
+    instructions (DADD + DMUL + DFMA, counted by ncu per interior cell) per
+    launch over the CUDA-event launch time, against 64 FP64 thread
+    instructions per SM per clock (ncu's peak_sustained of
+    sm__sass_thread_inst_executed_op_dfma_pred_on on B200) x SMs x the median
+    SM clock sampled during the timed region."""
+    import torch
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    mhz = (clk or {}).get("sm_mhz") or (clk or {}).get("sm_max_mhz")
+    if not mhz:
+        return None
+    achieved = inst_per_cell * cells / (launch_ms * 1e-3) / 1e9
+    peak = 64 * sms * mhz * 1e6 / 1e9
+    return {"unit": "G thread-inst/s", "inst_per_cell": inst_per_cell,
+            "achieved": round(achieved, 1), "peak": round(peak, 1),
+            "frac": round(achieved / peak, 4), "sm_mhz": mhz}
+
+
 def ncu_traffic(kernel):
     """DRAM bytes per launch of `kernel` from the committed ncu summary, or None."""
     return ncu_record(kernel).get("dram_bytes_per_launch_full_size")
@@ -802,6 +821,9 @@ def main():
         roof["ncu_pipes"] = {k: rec[k] for k in ("fp64_pipe_active_pct", "fma_pipe_active_pct",
                                                  "issue_active_pct", "warps_active_pct")
                              if k in rec} or None
+        if rec.get("fp64_thread_inst_per_cell"):
+            roof["fp64_pipe"] = fp64_pipe_roofline(rec["fp64_thread_inst_per_cell"], cells,
+                                                   roof["avg_launch_ms"], clk)
         launches_per_step = sum(k["launches"] for k in ks) / 3.0
         r.update(roof=roof, kernels=ks, launches_per_step=launches_per_step)
         st = r["stats"]

@@ -101,4 +101,17 @@ __host__ __device__ inline long long mapped_cell(const Grid& g, int i, int j, in
                  map_dim(k, g.nz, g.Ng, g.bcz));
 }
 
+#ifdef __CUDACC__
+// Read-only input load: through the non-coherent path (`__ldg`, which the
+// compiler keeps even when the value is unused), or as a plain load that it
+// may drop when nothing uses the value.
+template <bool LDG>
+__device__ __forceinline__ double ld_in(const double* __restrict__ p) {
+  if constexpr (LDG)
+    return __ldg(p);
+  else
+    return *p;
+}
+#endif
+
 }  // namespace mth

@@ -156,6 +156,42 @@ __device__ __forceinline__ R face_diff(R right, R left, R d) {
   }
 }
 
+// The stage's output for one interior cell from its flux difference `acc`
+// (fnet of FVS::F): fnet itself, the Euler step U - dt fnet, the RK2
+// corrector 1/2 (U^n + U^1 - dt fnet), or SSP2's final combination
+// cons += -0.5 dt (flux1 + flux2 - source1 - source2) in the reference's
+// order (SSP2.cc:155-166) with flux2 = fnet and source2 = S(stage state).
+template <class M, typename R>
+__device__ __forceinline__ void stage_update(const Grid& g, const double* __restrict__ cons,
+                                             const double* __restrict__ aux, const double* u0,
+                                             double* out, double dt, int mode,
+                                             const StageTail& tail, long long cell,
+                                             const R* acc) {
+  constexpr int NC = M::NC;
+  if (mode == STAGE_SSP2_FINAL) {
+    double s2[NC];
+    M::cell_source(cons, aux, g.Ntot, cell, tail.cp, s2);
+#pragma unroll
+    for (int v = 0; v < NC; ++v) {
+      const long long o = (long long)v * g.Ntot + cell;
+      out[o] = u0[o] + -0.5 * dt * (tail.flux1[o] + (double)acc[v] - tail.source1[o] - s2[v]);
+    }
+    return;
+  }
+#pragma unroll
+  for (int v = 0; v < NC; ++v) {
+    const long long o = (long long)v * g.Ntot + cell;
+    const double fn = (double)acc[v];
+    if (mode == STAGE_FNET) {
+      out[o] = fn;
+    } else if (mode == STAGE_EULER) {
+      out[o] = cons[o] - dt * fn;
+    } else {
+      out[o] = 0.5 * (u0[o] + cons[o] - dt * fn);
+    }
+  }
+}
+
 // One TI x 32 tile (tile row ti, tile column tj) of the fused stage; the
 // whole CTA participates and `smem_raw` holds Fvs2dSmem::bytes.
 template <class M, typename R, int ORDER, int TI>
@@ -244,32 +280,7 @@ __device__ __forceinline__ void fvs2d_tile(const Grid& g, const double* __restri
       acc[v] = acc[v] + face_diff<R>(sr[v * S::FY + ty * (TJ + 1) + lane + 1],
                                      sr[v * S::FY + ty * (TJ + 1) + lane], dy);
 
-    // ---------------- stage update ----------------
-    const long long cell = cell_id(g, ci, cj, 0);
-    if (mode == STAGE_SSP2_FINAL) {
-      // cons += -0.5 dt (flux1 + flux2 - source1 - source2) in the reference's
-      // order (SSP2.cc:155-166), flux2 = this fnet, source2 = S(stage state)
-      double s2[NC];
-      M::cell_source(cons, aux, g.Ntot, cell, tail.cp, s2);
-#pragma unroll
-      for (int v = 0; v < NC; ++v) {
-        const long long o = (long long)v * g.Ntot + cell;
-        out[o] = u0[o] + -0.5 * dt * (tail.flux1[o] + (double)acc[v] - tail.source1[o] - s2[v]);
-      }
-      return;
-    }
-#pragma unroll
-    for (int v = 0; v < NC; ++v) {
-      const long long o = (long long)v * g.Ntot + cell;
-      const double fn = (double)acc[v];
-      if (mode == STAGE_FNET) {
-        out[o] = fn;
-      } else if (mode == STAGE_EULER) {
-        out[o] = cons[o] - dt * fn;
-      } else {
-        out[o] = 0.5 * (u0[o] + cons[o] - dt * fn);
-      }
-    }
+    stage_update<M, R>(g, cons, aux, u0, out, dt, mode, tail, cell_id(g, ci, cj, 0), acc);
   }
 }
 

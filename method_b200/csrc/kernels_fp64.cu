@@ -9,6 +9,7 @@
 #include "common.cuh"
 #include "ensemble.h"
 #include "fvs2d.cuh"
+#include "fvs2d_group.cuh"
 #include "launch.h"
 #include "minpack.cuh"
 #include "srmhd.cuh"
@@ -778,22 +779,46 @@ __global__ void __launch_bounds__(128)
   for (int v = 0; v < 17; ++v) aux[v * n + q] = a[v];
 }
 
+// The plain tile runs in passes of kFp64Group variables (fvs2d_group.cuh)
+// with registers sized for kFp64Blocks CTAs per SM: WENO3/5 4 CTAs (64
+// registers, a few spilled; OT 1024^2 WENO5 0.550 ms per launch against
+// 0.600 at 3 CTAs and 0.66 for the one-pass tile), WENO7 3, WENO9/11 2.
+// Grids of fewer than two tiles per SM keep the one-pass tile: there the
+// passes only lengthen each CTA (KH 64 x 128: 0.145 against 0.131 ms per
+// step).  Both forms give the same bits.
+template <class M>
+constexpr int kFp64Group = M::NC == 9 ? 3 : 5;
+template <int ORDER>
+constexpr int kFp64Blocks = ORDER <= 5 ? 4 : ORDER <= 7 ? 3 : 2;
+
+int device_sm_count() {
+  int dev = 0, sms = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
+  return sms;
+}
+
 template <class M, int ORDER, int TI>
 cudaError_t fvs2d_instance(const Grid& g, const double* cons, const double* prims,
                            const double* aux, const double* u0, double* out, double dt, int mode,
                            StageTail tail, cudaStream_t st) {
-  using S = Fvs2dSmem<M, double, ORDER, TI>;
-  auto kern = k_fvs2d<M, double, ORDER, TI>;
-  static bool configured = false;
-  if (!configured) {
+  dim3 grid((g.je - g.js + 31) / 32, (g.ie - g.is + TI - 1) / TI);
+  dim3 block(32, TI);
+  if ((long long)grid.x * grid.y >= 2LL * device_sm_count()) {
+    using S = Fvs2dGroupSmem<M, ORDER, TI, kFp64Group<M>>;
+    auto kern = k_fvs2d_group<M, ORDER, TI, kFp64Group<M>, kFp64Blocks<ORDER>>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)S::bytes);
     if (e != cudaSuccess) return e;
-    configured = true;
+    kern<<<grid, block, S::bytes, st>>>(g, cons, prims, aux, u0, out, dt, mode, tail);
+  } else {
+    using S = Fvs2dSmem<M, double, ORDER, TI>;
+    auto kern = k_fvs2d<M, double, ORDER, TI>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)S::bytes);
+    if (e != cudaSuccess) return e;
+    kern<<<grid, block, S::bytes, st>>>(g, cons, prims, aux, u0, out, dt, mode, tail, 0);
   }
-  dim3 grid((g.je - g.js + 31) / 32, (g.ie - g.is + TI - 1) / TI);
-  dim3 block(32, TI);
-  kern<<<grid, block, S::bytes, st>>>(g, cons, prims, aux, u0, out, dt, mode, tail, 0);
   return cudaGetLastError();
 }
 

@@ -34,7 +34,7 @@ struct HybrdResult {
 // Euclidean norm with MINPACK's three-range accumulation (enorm.cc), the
 // dwarf / giant limits of the reference's double build.
 template <int M>
-__device__ __forceinline__ double hy_enorm(const double* x) {
+__device__ __forceinline__ double hy_enorm_ranges(const double* x) {
   const double rdwarf = 1.82691291192569e-153;
   const double rgiant = 1.34078079299426e+153;
   double s1 = 0., s2 = 0., s3 = 0., x1max = 0., x3max = 0.;
@@ -70,6 +70,44 @@ __device__ __forceinline__ double hy_enorm(const double* x) {
     return sqrt(x3max * ((s2 / x3max) + (x3max * s3)));
   }
   return x3max * sqrt(s3);
+}
+
+// enorm's arguments by value, so that its out-of-line form keeps the
+// caller's vector in registers.
+template <int M>
+struct EnormArgs {
+  double x[M];
+};
+
+template <int M>
+__device__ __noinline__ double hy_enorm_full(EnormArgs<M> a) {
+  return hy_enorm_ranges<M>(a.x);
+}
+
+// enorm for the usual vector, every component zero or of intermediate size
+// (rdwarf < |x| < rgiant / M): the three-range accumulation then adds only
+// to s2, in index order from zero, and returns
+// sqrt(s2 * (1 + (0 / s2) * (0 * s3))) = sqrt(s2), or x3max * sqrt(s3) = 0
+// when every component is zero, which sqrt(s2) also gives.  Any other vector
+// takes the full form, out of line: the many call sites of the hybrid
+// method then carry the short form only.
+template <int M>
+__device__ __forceinline__ double hy_enorm(const double* x) {
+  const double rdwarf = 1.82691291192569e-153;
+  const double agiant = 1.34078079299426e+153 / (double)M;
+  double s2 = 0.;
+  bool mid = true;
+#pragma unroll
+  for (int i = 0; i < M; ++i) {
+    const double xabs = fabs(x[i]);
+    mid = mid && xabs < agiant && (xabs > rdwarf || xabs == 0.);
+    s2 += xabs * xabs;
+  }
+  if (mid) return sqrt(s2);
+  EnormArgs<M> a;
+#pragma unroll
+  for (int i = 0; i < M; ++i) a.x[i] = x[i];
+  return hy_enorm_full<M>(a);
 }
 
 template <int N>
@@ -337,7 +375,31 @@ struct Hybrd {
     return enorm_len(buf, m);
   }
 
+  __device__ static __noinline__ double enorm_len_full(EnormArgs<N> a, int m) {
+    return enorm_len_ranges(a.x, m);
+  }
+
+  // enorm of x[0 .. m): the short form of hy_enorm for the usual vector.
   __device__ static __forceinline__ double enorm_len(const double* x, int m) {
+    const double rdwarf = 1.82691291192569e-153;
+    const double agiant = 1.34078079299426e+153 / (double)m;
+    double s2 = 0.;
+    bool mid = true;
+#pragma unroll (UNR)
+    for (int i = 0; i < N; ++i) {
+      if (i >= m) break;
+      const double xabs = fabs(x[i]);
+      mid = mid && xabs < agiant && (xabs > rdwarf || xabs == 0.);
+      s2 += xabs * xabs;
+    }
+    if (mid) return sqrt(s2);
+    EnormArgs<N> a;
+#pragma unroll (UNR)
+    for (int i = 0; i < N; ++i) a.x[i] = x[i];
+    return enorm_len_full(a, m);
+  }
+
+  __device__ static __forceinline__ double enorm_len_ranges(const double* x, int m) {
     const double rdwarf = 1.82691291192569e-153;
     const double rgiant = 1.34078079299426e+153;
     double s1 = 0., s2 = 0., s3 = 0., x1max = 0., x3max = 0.;

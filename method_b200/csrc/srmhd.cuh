@@ -7,6 +7,7 @@
 // Every expression below keeps the reference's association order so that the
 // FP64 build without FMA contraction reproduces the reference bit for bit.
 #pragma once
+#include "common.cuh"
 #include "minpack.cuh"
 
 namespace mth {
@@ -202,19 +203,19 @@ __device__ __forceinline__ void source(const double* c, double cp, double* s) {
 // Model trait used by the stencil kernels.
 struct SRMHD {
   static constexpr int NC = 9, NP = 8, NA = 13;
-  template <typename R>
+  template <typename R, bool LDG = true>
   __device__ __forceinline__ static void load_flux_inputs(const double* __restrict__ cons,
                                                           const double* __restrict__ prims,
                                                           const double* __restrict__ aux,
                                                           long long N, long long cell, R* c, R* p,
                                                           R* a) {
 #pragma unroll
-    for (int v = 0; v < NC; ++v) c[v] = R(__ldg(cons + v * N + cell));
+    for (int v = 0; v < NC; ++v) c[v] = R(ld_in<LDG>(cons + v * N + cell));
 #pragma unroll
-    for (int v = 1; v < 8; ++v) p[v] = R(__ldg(prims + v * N + cell));
-    a[1] = R(__ldg(aux + 1 * N + cell));
+    for (int v = 1; v < 8; ++v) p[v] = R(ld_in<LDG>(prims + v * N + cell));
+    a[1] = R(ld_in<LDG>(aux + 1 * N + cell));
 #pragma unroll
-    for (int v = 4; v < 9; ++v) a[v] = R(__ldg(aux + v * N + cell));
+    for (int v = 4; v < 9; ++v) a[v] = R(ld_in<LDG>(aux + v * N + cell));
   }
   template <typename R>
   __device__ __forceinline__ static void flux(const R* c, const R* p, const R* a, int dir, R* f) {

@@ -253,19 +253,19 @@ struct ImexResidual {
 
 struct SRRMHD {
   static constexpr int NC = 14, NP = 11, NA = 17;
-  template <typename R>
+  template <typename R, bool LDG = true>
   __device__ __forceinline__ static void load_flux_inputs(const double* __restrict__ cons,
                                                           const double* __restrict__ prims,
                                                           const double* __restrict__ aux,
                                                           long long N, long long cell, R* c, R* p,
                                                           R* a) {
 #pragma unroll
-    for (int v = 0; v < NC; ++v) c[v] = R(__ldg(cons + v * N + cell));
+    for (int v = 0; v < NC; ++v) c[v] = R(ld_in<LDG>(cons + v * N + cell));
 #pragma unroll
-    for (int v = 1; v < 5; ++v) p[v] = R(__ldg(prims + v * N + cell));
+    for (int v = 1; v < 5; ++v) p[v] = R(ld_in<LDG>(prims + v * N + cell));
 #pragma unroll
-    for (int v = 4; v < 9; ++v) a[v] = R(__ldg(aux + v * N + cell));
-    a[10] = R(__ldg(aux + 10 * N + cell));
+    for (int v = 4; v < 9; ++v) a[v] = R(ld_in<LDG>(aux + v * N + cell));
+    a[10] = R(ld_in<LDG>(aux + 10 * N + cell));
   }
   template <typename R>
   __device__ __forceinline__ static void flux(const R* c, const R* p, const R* a, int dir, R* f) {

@@ -34,12 +34,24 @@ def test_forward_matches_oracle():
     assert np.all(err <= 2e-2 * (1 + np.abs(y_ref)))
 
 
-def test_gradient_matches_oracle():
+@pytest.mark.parametrize("seed", [2, 3, 4, 5, 6])
+@pytest.mark.parametrize("n", [512, 4096])
+def test_gradient_matches_oracle(seed, n):
+    """Loss and gradient of the device's backward pass against the oracle run
+    with the same BF16 rounding points (operands and activations rounded to
+    BF16, accumulation exact in FP64).  What remains between them is the
+    accumulation: the device sums in FP32 on the tensor cores, so a
+    pre-activation that lies next to a BF16 rounding boundary can round to the
+    neighbouring BF16 value (one BF16 unit, 2^-8 relative) or, next to zero,
+    flip its ReLU mask, and that difference propagates to the layers below.
+    Measured over these seeds: at most 1.7e-3 relative (W1, seed 4, n = 512),
+    mostly below 2e-5; the bound asserted is 5e-3 per parameter block.  (The
+    BF16 rounding itself moves the gradient by 0.2-4% from the FP64 one, which
+    is why the oracle keeps the same rounding points.)"""
     from method_b200 import _lib
     L = _lib.load()
-    rng = np.random.default_rng(5)
-    P = M.init_params(2).astype(np.float32)
-    n = 512
+    rng = np.random.default_rng(seed + 3)
+    P = M.init_params(seed).astype(np.float32)
     x = rng.normal(size=(n, M.IN)).astype(np.float32)
     t = rng.normal(size=(n, M.OUT)).astype(np.float32)
     g = np.zeros(M.NPARAM, dtype=np.float32)
@@ -47,7 +59,7 @@ def test_gradient_matches_oracle():
     assert L.mth_mlp_grad(fptr(P), n, fptr(x), fptr(t), fptr(g), fptr(loss), 0) == 0
     l_ref, g_ref, _ = M.loss_and_grad(P.astype(np.float64), x.astype(np.float64),
                                       t.astype(np.float64), bf=True)
-    assert abs(loss[0] - l_ref) <= 1e-3 * l_ref
+    assert abs(loss[0] - l_ref) <= 1e-4 * l_ref
     d, dr = M.unpack(g), M.unpack(g_ref)
     for name, _ in M.SHAPES:
         a, b = d[name].ravel(), dr[name].ravel()
@@ -55,8 +67,7 @@ def test_gradient_matches_oracle():
             assert np.all(a == 0), name
             continue
         rel = np.linalg.norm(a - b) / np.linalg.norm(b)
-        cos = float(a @ b / (np.linalg.norm(a) * np.linalg.norm(b)))
-        assert rel < 2e-2 and cos > 0.9995, (name, rel, cos)
+        assert rel < 5e-3, (name, rel)
 
 
 @pytest.fixture(scope="module")
