@@ -222,6 +222,10 @@ mth_status mth_mlp_grad(const float* params, int n, const float* x, const float*
                         float* loss, int device);
 /* Standardised outputs y [n][2] of standardised features x [n][8]. */
 mth_status mth_mlp_forward(const float* params, int n, const float* x, float* y, int device);
+/* The same on the tcgen05 tensor-core path (M = 128 products, accumulators in
+ * tensor memory): the same weights and rounding points, FP32 sums in the
+ * tensor cores' order.  No reference counterpart (the learned guess). */
+mth_status mth_mlp_forward_tc(const float* params, int n, const float* x, float* y, int device);
 /* Solver-generated training pairs: features [n][8], targets [n][2] (raw,
  * not standardised), optionally the conserved [9][n] and generating
  * primitive [8][n] states.  Output pointers may be host or device memory

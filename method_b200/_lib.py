@@ -25,6 +25,7 @@ SYMBOLS = [
     "mth_get_stats", "mth_reset_stats", "mth_step_host", "mth_step_host_bytes", "mth_pin_host",
     "mth_unpin_host",
     "mth_set_stream", "mth_profile_step", "mth_mlp_train", "mth_mlp_grad", "mth_mlp_forward",
+    "mth_mlp_forward_tc",
     "mth_mlp_make_pairs", "mth_mlp_make_pairs_srrmhd", "mth_set_mlp", "mth_c2p_batch", "mth_c2p_ctx_create", "mth_c2p_ctx_destroy",
     "mth_c2p_ctx_set_mlp", "mth_c2p_ctx_run", "mth_c2p_ctx_stats", "mth_c2p_srmhd_noalloc",
     "mth_save_text", "mth_device_state", "mth_ensemble_create", "mth_ensemble_destroy",
@@ -135,6 +136,7 @@ def load():
     L.mth_mlp_train.argtypes = [C.POINTER(MlpTrainConfig), F, F, F, C.c_int]
     L.mth_mlp_grad.argtypes = [F, C.c_int, F, F, F, F, C.c_int]
     L.mth_mlp_forward.argtypes = [F, C.c_int, F, F, C.c_int]
+    L.mth_mlp_forward_tc.argtypes = [F, C.c_int, F, F, C.c_int]
     L.mth_mlp_make_pairs.argtypes = [C.c_longlong, C.c_ulonglong, C.c_double, F, F, D, D, C.c_int]
     L.mth_mlp_make_pairs_srrmhd.argtypes = [C.c_longlong, C.c_ulonglong, C.c_double, F, F, D, D,
                                             C.c_int]

@@ -35,6 +35,7 @@ UNITS = [
     ("kernels_fp64.cu", ["-fmad=false", "-prec-div=true", "-prec-sqrt=true"]),
     ("kernels_mixed.cu", []),
     ("mlp.cu", []),
+    ("mlp_tc.cu", []),
     ("api.cu", []),
     ("noalloc.cu", []),
     ("ensemble.cu", []),

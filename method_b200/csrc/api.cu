@@ -425,6 +425,8 @@ mth_status read_status(mth_handle* h) {
     return fail(h, MTH_ERR_IMPLICIT,
                 "IMEX time integrator could not converge to a solution (implicit stage)");
   if (flags & ERR_C2P) return fail(h, MTH_ERR_C2P, "C2P could not converge.");
+  if (flags & ERR_DEVICE)
+    return fail(h, MTH_ERR_CUDA, "a tensor-core wait of the guess network ran out");
   return MTH_OK;
 }
 

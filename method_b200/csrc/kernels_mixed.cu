@@ -945,7 +945,7 @@ cudaError_t launch_c2p_mixed(const Grid& g, int model, int guess, const double* 
   if (nt <= 0) return cudaSuccess;
   if (model == MODEL_SRMHD && guess == 1 && mw.has_mlp) {
     cudaError_t e = mlp::launch_zguess(g, nI, false, cons, mw.mlp_params, mw.feat_stats,
-                                       mw.zguess, st);
+                                       mw.zguess, st, MODEL_SRMHD, w.counters + 3);
     if (e != cudaSuccess) return e;
   }
   if (model == MODEL_SRMHD) {
@@ -960,7 +960,7 @@ cudaError_t launch_c2p_mixed(const Grid& g, int model, int guess, const double* 
     const double* zseed = nullptr;
     if (guess == 1 && mw.has_mlp) {
       cudaError_t e = mlp::launch_zguess(g, nI, false, cons, mw.mlp_params, mw.feat_stats,
-                                         mw.zguess, st, MODEL_SRRMHD);
+                                         mw.zguess, st, MODEL_SRRMHD, w.counters + 3);
       if (e != cudaSuccess) return e;
       zseed = mw.zguess;
     }
@@ -988,7 +988,8 @@ cudaError_t launch_imex_fast(const Grid& g, int stage, const double* cons,
     if (stage == 2)
       k_imex_explicit_part<2><<<blocks, 128, 0, st>>>(g, cons, flux1, source1, out, dt);
     cudaError_t e = mlp::launch_zguess(g, nI, false, stage == 1 ? cons : out, mw->mlp_params,
-                                       mw->feat_stats, mw->zguess, st, MODEL_SRRMHD);
+                                       mw->feat_stats, mw->zguess, st, MODEL_SRRMHD,
+                                       w.counters + 3);
     if (e != cudaSuccess) return e;
     zseed = mw->zguess;
   }

@@ -21,6 +21,7 @@ struct C2PWork {
 enum ErrFlag : long long {
   ERR_C2P = 1,       // primitive recovery did not converge
   ERR_IMPLICIT = 2,  // implicit source solve did not converge
+  ERR_DEVICE = 4,    // a bounded device-side wait ran out (tensor-core inference)
 };
 
 // Data::initData geometry (simData.cc:61-97) for a configuration; returns

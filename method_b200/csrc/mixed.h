@@ -24,9 +24,11 @@ namespace mlp {
 size_t smem_bytes();
 cudaError_t configure();
 // model 0: SRMHD features of cons (9 vars); 1: SRRMHD (14 vars).
+// Runs on the tcgen05 path (mlp_tc.cu); a bounded wait there that runs out
+// sets ERR_DEVICE in *err when err is given.
 cudaError_t launch_zguess(const Grid& g, long long n_cells, bool batch, const double* cons,
                           const float* P, const float* st, double* zguess, cudaStream_t s,
-                          int model = 0);
+                          int model = 0, long long* err = nullptr);
 }  // namespace mlp
 
 // SSP2 implicit stage of the mixed form (closed-form psi/phi, Newton on E).

@@ -595,9 +595,24 @@ cudaError_t launch_forward(const float* P, int n, const float* x, float* y, cuda
   return cudaGetLastError();
 }
 
+cudaError_t launch_zguess_tc(const Grid& g, long long n_cells, bool batch, const double* cons,
+                             const float* P, const float* stats, double* zguess, long long* err,
+                             cudaStream_t st, int model);
+
+// Inference path of grids, batches and ensembles: the warp-level kernels
+// below, or the tcgen05 kernels of mlp_tc.cu (same weights and rounding
+// points).  Measured on B200: the tcgen05 path takes 1.33 ms for 256^3
+// cells against 1.21 ms, and 0.12 ms against 0.09 ms per OT 1024^2
+// recovery: this network's layers are 16-64 wide, so each 128-cell tile's
+// four dependent products wait on commit -> TMEM load -> shared-memory
+// round trips, where the warp-level path keeps the activations in registers
+// from one layer to the next.  The faster path is the default.
+constexpr bool kTcInference = false;
+
 cudaError_t launch_zguess(const Grid& g, long long n_cells, bool batch, const double* cons,
                           const float* P, const float* st, double* zguess, cudaStream_t s,
-                          int model) {
+                          int model, long long* err) {
+  if (kTcInference) return launch_zguess_tc(g, n_cells, batch, cons, P, st, zguess, err, s, model);
   if (model == 0)
     k_mlp_zguess<0><<<infer_grid((const void*)k_mlp_zguess<0>, n_cells), 256, sizeof(InferSmem),
                       s>>>(g, n_cells, batch ? 1 : 0, cons, P, st, zguess);
@@ -609,10 +624,17 @@ cudaError_t launch_zguess(const Grid& g, long long n_cells, bool batch, const do
 
 }  // namespace mlp
 
+namespace mlp {
+cudaError_t ens_zguess_tc(const Member* mem, const Item* items, int n_items, int ic,
+                          const float* P, const float* stats, cudaStream_t st, int model);
+}
+
 cudaError_t ens_mlp_zguess(const Member* mem, const Item* items, int n_items, int ic,
                            const float* params, const float* stats, int grid, cudaStream_t st,
                            int model) {
   (void)grid;
+  if (mlp::kTcInference)
+    return mlp::ens_zguess_tc(mem, items, n_items, ic, params, stats, st, model);
   const int blocks = mlp::infer_grid((const void*)mlp::k_ens_mlp_zguess<0>,
                                      (long long)n_items * ENS_CHUNK);
   if (model == 0)

@@ -34,6 +34,30 @@ def test_forward_matches_oracle():
     assert np.all(err <= 2e-2 * (1 + np.abs(y_ref)))
 
 
+@pytest.mark.parametrize("n", [300, 70000])
+def test_forward_tcgen05_matches_oracle(n):
+    """The tcgen05 tensor-core inference (M = 128 products into tensor memory)
+    against the oracle with the same BF16 rounding points, and against the
+    warp-level path: same weights and activations, FP32 sums in another
+    order, so a pre-activation next to a BF16 rounding boundary may round
+    one BF16 unit the other way."""
+    from method_b200 import _lib
+    L = _lib.load()
+    rng = np.random.default_rng(1)
+    P = M.init_params(1).astype(np.float32)
+    x = rng.normal(size=(n, M.IN)).astype(np.float32)
+    y = np.zeros((n, M.OUT), dtype=np.float32)
+    y_mma = np.zeros((n, M.OUT), dtype=np.float32)
+    assert L.mth_mlp_forward_tc(fptr(P), n, fptr(x), fptr(y), 0) == 0
+    assert L.mth_mlp_forward(fptr(P), n, fptr(x), fptr(y_mma), 0) == 0
+    _, _, y_ref = M.loss_and_grad(P.astype(np.float64), x.astype(np.float64),
+                                  np.zeros((n, M.OUT)), bf=True)
+    err = np.abs(y - y_ref)
+    assert np.median(err) < 1e-4
+    assert np.all(err <= 2e-2 * (1 + np.abs(y_ref)))
+    assert np.median(np.abs(y - y_mma)) < 1e-4
+
+
 @pytest.mark.parametrize("seed", [2, 3, 4, 5, 6])
 @pytest.mark.parametrize("n", [512, 4096])
 def test_gradient_matches_oracle(seed, n):
