@@ -192,6 +192,25 @@ __device__ __forceinline__ void stage_update(const Grid& g, const double* __rest
   }
 }
 
+// The epilogue's inputs that no earlier phase of the stage reads (U^n of
+// the RK2 corrector; U^n, flux1 and source1 of SSP2's final combination),
+// requested into L2 when the tile starts so that their latency overlaps the
+// flux phases (OT 1024^2 corrector tile: 0.154 -> 0.151 ms average launch).
+template <class M>
+__device__ __forceinline__ void prefetch_tail(const Grid& g, const double* u0, int mode,
+                                              const StageTail& tail, long long cell) {
+  if (mode != STAGE_RK2_CORR && mode != STAGE_SSP2_FINAL) return;
+#pragma unroll
+  for (int v = 0; v < M::NC; ++v) {
+    const long long o = (long long)v * g.Ntot + cell;
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(u0 + o));
+    if (mode == STAGE_SSP2_FINAL) {
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(tail.flux1 + o));
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(tail.source1 + o));
+    }
+  }
+}
+
 // One TI x 32 tile (tile row ti, tile column tj) of the fused stage; the
 // whole CTA participates and `smem_raw` holds Fvs2dSmem::bytes.
 template <class M, typename R, int ORDER, int TI>
@@ -210,6 +229,7 @@ __device__ __forceinline__ void fvs2d_tile(const Grid& g, const double* __restri
   const int i0 = g.is + ti * TI, j0 = g.js + tj * TJ;
   const int ci = i0 + ty, cj = j0 + lane;
   R acc[NC];
+  if (ci < g.ie && cj < g.je) prefetch_tail<M>(g, u0, mode, tail, cell_id(g, ci, cj, 0));
 
   // ---------------- x direction ----------------
   for (int e = tid; e < S::RX; e += NT) {

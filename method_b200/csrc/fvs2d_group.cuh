@@ -124,9 +124,10 @@ __global__ void __launch_bounds__(32 * TI, MINB)
                   int mode, StageTail tail) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int i0 = g.is + blockIdx.y * TI, j0 = g.js + blockIdx.x * 32;
+  const int ci = i0 + threadIdx.y, cj = j0 + threadIdx.x;
+  if (ci < g.ie && cj < g.je) prefetch_tail<M>(g, u0, mode, tail, cell_id(g, ci, cj, 0));
   double acc[M::NC];
   group_pass<M, ORDER, TI, G, 0>(g, cons, prims, aux, i0, j0, acc, smem_raw);
-  const int ci = i0 + threadIdx.y, cj = j0 + threadIdx.x;
   if (ci < g.ie && cj < g.je)
     stage_update<M, double>(g, cons, aux, u0, out, dt, mode, tail, cell_id(g, ci, cj, 0), acc);
 }
