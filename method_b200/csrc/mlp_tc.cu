@@ -2,24 +2,28 @@
 //
 // The same network, weights and rounding points as the warp-level path of
 // mlp.cu (BF16 weights and activations, FP32 accumulation, ReLU between
-// layers), computed as four M = 128 matrix products per tile of 128 cells:
+// layers), computed as four M = 128 matrix products per tile of 128 cells.
+// Each warpgroup of a CTA (two per CTA, sharing the weights) owns a tile:
 //   * one thread per cell stages the cell's standardised features as BF16 in
-//     shared memory (row m of the A operand);
+//     shared memory (row m of the warpgroup's A operand);
 //   * one thread issues `tcgen05.mma.cta_group::1.kind::f16` with A and the
 //     layer's weights (B) read from shared memory through matrix
 //     descriptors, the FP32 product accumulating in tensor memory (TMEM,
-//     64 columns per CTA), and `tcgen05.commit` signals an mbarrier;
-//   * every thread then reads its own row back from TMEM (`tcgen05.ld`,
-//     warp w owns TMEM lanes 32w .. 32w+31), adds the bias, applies ReLU,
-//     rounds to BF16 and writes the next layer's A row.
+//     64 columns per warpgroup), and `tcgen05.commit` signals the
+//     warpgroup's mbarrier;
+//   * every thread then reads its own row back from TMEM (`tcgen05.ld`, warp
+//     w owns TMEM lanes 32 (w mod 4) .. 32 (w mod 4) + 31), adds the bias,
+//     applies ReLU, rounds to BF16 and writes the next layer's A row.
 // Operands use the K-major layout without swizzle: 8-row x 16-byte core
 // matrices, the two 8-element K halves of a 16-wide K slab 128 bytes apart
 // (leading byte offset), 8-row groups 256 bytes apart (stride byte offset),
 // K slabs one after another; the descriptor and instruction-descriptor
 // fields follow the PTX ISA's tcgen05 matrix and instruction descriptors.
 //
-// Every wait on the mbarrier is bounded; a wait that runs out stops the CTA's
-// remaining tiles, sets the error word and still frees the CTA's TMEM.
+// Every wait on an mbarrier is bounded; a wait that runs out stops the
+// warpgroup's remaining tiles, sets the error word and still frees the CTA's
+// TMEM.  The solver uses the warp-level path of mlp.cu by default (faster for
+// this small network on B200, mlp.cu: kTcInference).
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
