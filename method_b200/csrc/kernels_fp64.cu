@@ -781,13 +781,14 @@ __global__ void __launch_bounds__(128)
 
 // The plain tile runs in passes of kFp64Group variables (fvs2d_group.cuh)
 // with registers sized for kFp64Blocks CTAs per SM: WENO3/5 4 CTAs (64
-// registers, a few spilled; OT 1024^2 WENO5 0.550 ms per launch against
-// 0.600 at 3 CTAs and 0.66 for the one-pass tile), WENO7 3, WENO9/11 2.
+// registers, a few spilled), WENO7 3, WENO9/11 2.  OT 1024^2 WENO5: two
+// passes of 5 + 4 variables 0.515 ms per launch, three of 3 0.549 ms (0.600
+// at 3 CTAs per SM), the one-pass tile 0.66 ms.
 // Grids of fewer than two tiles per SM keep the one-pass tile: there the
 // passes only lengthen each CTA (KH 64 x 128: 0.145 against 0.131 ms per
 // step).  Both forms give the same bits.
 template <class M>
-constexpr int kFp64Group = M::NC == 9 ? 3 : 5;
+constexpr int kFp64Group = 5;
 template <int ORDER>
 constexpr int kFp64Blocks = ORDER <= 5 ? 4 : ORDER <= 7 ? 3 : 2;
 
