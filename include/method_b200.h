@@ -61,6 +61,11 @@ typedef struct {
   int x_slab;
   int x_global_nx;
   int x_offset;
+  /* 1: the REGIME resistive extension of SRMHD (REGIME.cc, Wright & Hawke
+   * 2019) as RKSplit's model extension, as `REGIME ext(&data, &fvs);
+   * RKSplit ti(&data, &model, &bcs, &fvs, &ext)`: SRMHD, RKSplit, one or two
+   * dimensions; sigma is its conductivity. */
+  int regime;
 } mth_config;
 
 typedef struct {

@@ -231,8 +231,33 @@ class Flow : public Bcs {
   int bcId() const override { return MTH_FLOW; }
 };
 
+// ---------------------------------------------------------- model extensions
+// A source an integrator adds to the model's (modelExtension.h:13-50).
+class ModelExtension {
+ public:
+  Data* data = nullptr;
+  bool sourceExists = false;
+  bool fluxExists = false;
+  ModelExtension() {}
+  explicit ModelExtension(Data* data) : data(data) {}
+  virtual ~ModelExtension() {}
+  // 0: none this library evaluates; 1: REGIME.
+  virtual int extensionId() const { return 0; }
+};
+// REGIME, the resistive extension of ideal SRMHD (REGIME.h:81-160).  Only
+// RKSplit applies a model extension (rkSplit.cc:15-16), and it does so on
+// the device; REGIME with another model is rejected.
+class REGIME : public ModelExtension {
+ public:
+  FluxMethod* fluxMethod = nullptr;
+  REGIME() {}
+  REGIME(Data* data, FluxMethod* fluxMethod) : ModelExtension(data), fluxMethod(fluxMethod) {
+    sourceExists = true;
+  }
+  int extensionId() const override { return 1; }
+};
+
 // --------------------------------------------------------- time integrators
-class ModelExtension;
 class TimeIntegrator {
  public:
   Data* data;

@@ -50,9 +50,10 @@ def _dptr(a):
 def _config(nx, ny, nz=0, xmin=0.0, xmax=1.0, ymin=0.0, ymax=1.0, zmin=0.0, zmax=1.0,
             endTime=1.0, cfl=0.5, Ng=4, gamma=5.0 / 3.0, sigma=1e3, cp=0.1, model="srmhd",
             weno=3, bcs="periodic", integrator="rk2", precision="fp64", guess="previous",
-            device=0, functionalSigma=False, gam=12.0, x_slab=None):
+            device=0, functionalSigma=False, gam=12.0, x_slab=None, regime=False):
     """mth_config from the reference Data constructor's arguments plus the
-    class choices of a reference main.cc."""
+    class choices of a reference main.cc (``regime=True``: the REGIME model
+    extension with RKSplit)."""
     c = _lib.Config()
     c.model = MODELS[model]
     c.nx, c.ny, c.nz = nx, ny, nz
@@ -67,6 +68,7 @@ def _config(nx, ny, nz=0, xmin=0.0, xmax=1.0, ymin=0.0, ymax=1.0, zmin=0.0, zmax
     c.device = device
     c.functional_sigma = 1 if functionalSigma else 0
     c.sigma_exp = gam
+    c.regime = 1 if regime else 0
     if x_slab is not None:  # (offset, global nx): columns [offset, offset + nx) of the domain
         c.x_slab = 1
         c.x_offset, c.x_global_nx = x_slab
@@ -78,7 +80,8 @@ class Simulation:
 
     Keyword arguments are the reference Data constructor's (nx, ny, nz, xmin ..
     zmax, endTime, cfl, Ng, gamma, sigma, cp) plus ``model``, ``weno``,
-    ``bcs``, ``integrator``, ``precision`` and ``guess``.
+    ``bcs``, ``integrator``, ``precision``, ``guess`` and ``regime`` (the
+    REGIME resistive extension of SRMHD under RKSplit, REGIME.cc).
     """
 
     def __init__(self, nx, ny, nz=0, **kw):

@@ -33,6 +33,7 @@ COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler",
 
 UNITS = [
     ("kernels_fp64.cu", ["-fmad=false", "-prec-div=true", "-prec-sqrt=true"]),
+    ("regime.cu", ["-fmad=false", "-prec-div=true", "-prec-sqrt=true"]),
     ("kernels_mixed.cu", []),
     ("mlp.cu", []),
     ("mlp_tc.cu", []),

@@ -41,6 +41,7 @@ struct mth_handle {
   int* fail_count = nullptr;
   long long* counters = nullptr;  // [0..3] C2P, [4..7] implicit, [8..9] Newton fallbacks
   MixedWork mixed{};
+  RegimeWork regime{};
   double t = 0, dt = 0;
   int iters = 0;
   long long steps = 0;
@@ -283,11 +284,23 @@ cudaError_t enqueue_part(mth_handle* h, double dt, int part) {
     if ((e = c2p(h, h->cons, h->prims, h->aux, h->prims, h->aux))) return e;
     if (integ == MTH_RKSPLIT) {
       // RKSplit::step (rkSplit.cc:31-53): U += dt S(U), finalise.
-      if ((e = timed(h, "source_add", 2.0 * h->NC, [&] {
-             return launch_source_add(h->g, h->cfg.model, h->cons, h->prims, h->aux, h->cons, dt,
-                                      h->st);
-           })))
+      if (h->cfg.regime) {
+        // with the REGIME extension, whose stencils read the ghosts that
+        // RK2's finalise leaves filled
+        if ((e = launch_apply_bcs(h->g, h->cons, h->NC, h->st)) ||
+            (e = launch_apply_bcs(h->g, h->prims, h->NP, h->st)))
+          return e;
+        if ((e = timed(h, "regime_source_add", 40.0, [&] {
+               return launch_regime_source_add(h->g, h->cfg.weno_order, h->cons, h->prims,
+                                               h->cons, dt, h->regime, h->st);
+             })))
+          return e;
+      } else if ((e = timed(h, "source_add", 2.0 * h->NC, [&] {
+                    return launch_source_add(h->g, h->cfg.model, h->cons, h->prims, h->aux,
+                                             h->cons, dt, h->st);
+                  }))) {
         return e;
+      }
       if ((e = c2p(h, h->cons, h->prims, h->aux, h->prims, h->aux))) return e;
     }
     return cudaSuccess;
@@ -516,7 +529,9 @@ mth_status mth_create(const mth_config* cfg, mth_handle** out) {
       (c.integrator >= MTH_SSP3 && c.guess != 0) ||
       c.precision < 0 || c.precision > 1 || c.guess < 0 || c.guess > 1 ||
       (c.x_slab && c.integrator != MTH_RK2 && c.integrator != MTH_RKSPLIT &&
-       c.integrator != MTH_SSP2)) {
+       c.integrator != MTH_SSP2) ||
+      (c.regime && (c.model != MTH_SRMHD || c.integrator != MTH_RKSPLIT || c.nz != 0 ||
+                    c.x_slab))) {
     delete h;
     return MTH_ERR_INVALID;
   }
@@ -573,6 +588,14 @@ mth_status mth_create(const mth_config* cfg, mth_handle** out) {
   if (c.precision == MTH_MIXED || c.guess == MTH_GUESS_MLP) {
     if ((e = mixed_init(&h->mixed, g, c.model, h->st))) return bail("mixed", e);
   }
+  if (c.regime) {
+    RegimeWork& w = h->regime;
+    for (auto pn : {std::make_pair(&w.E, 3), std::make_pair(&w.q, 1), std::make_pair(&w.fp, 3),
+                    std::make_pair(&w.fm, 3), std::make_pair(&w.frx, 3),
+                    std::make_pair(&w.fry, 3), std::make_pair(&w.K, 3), std::make_pair(&w.DX, 8),
+                    std::make_pair(&w.DY, 8)})
+      if ((e = alloc0(pn.first, bytes(h, pn.second), h->st))) return bail("regime", e);
+  }
   if ((e = cudaStreamSynchronize(h->st))) return bail("sync", e);
   *out = h;
   return MTH_OK;
@@ -585,7 +608,9 @@ mth_status mth_destroy(mth_handle* h) {
   for (auto& kv : h->graphs) cudaGraphExecDestroy(kv.second);
   for (double* p : {h->cons, h->prims, h->aux, h->p1cons, h->p1prims, h->p1aux, h->solution,
                     h->u1, h->u2, h->flux1, h->flux2, h->src1, h->src2, h->fnet, h->fplus,
-                    h->fminus, h->frecon, h->u3, h->flux3, h->src3, h->tprims, h->taux})
+                    h->fminus, h->frecon, h->u3, h->flux3, h->src3, h->tprims, h->taux,
+                    h->regime.E, h->regime.q, h->regime.fp, h->regime.fm, h->regime.frx,
+                    h->regime.fry, h->regime.K, h->regime.DX, h->regime.DY})
     if (p) cudaFree(p);
   if (h->fail_list) cudaFree(h->fail_list);
   if (h->fail_count) cudaFree(h->fail_count);

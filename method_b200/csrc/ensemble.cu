@@ -341,7 +341,7 @@ mth_status mth_ensemble_create(const mth_config* cfgs, int n, mth_ensemble** out
     d = Member{};
     if (!ok_model || c.ny <= 0 || c.nz != 0 || c.precision != e->precision ||
         c.weno_order != e->order || (c.weno_order != 3 && c.weno_order != 5) ||
-        c.device != e->device || c.sigma < 0 || c.x_slab ||
+        c.device != e->device || c.sigma < 0 || c.x_slab || c.regime ||
         c.guess != cfgs[0].guess ||
         (c.guess == MTH_GUESS_MLP && c.precision != MTH_MIXED) ||
         c.Ng < (c.weno_order + 1) / 2 + 1 || !grid_from_config(&c, &d.g)) {

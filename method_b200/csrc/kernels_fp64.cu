@@ -1030,6 +1030,12 @@ cudaError_t launch_fvs2d_fp64(const Grid& g, int model, int order, const double*
 #undef FVS64
 }
 
+cudaError_t launch_weno_dir(const Grid& g, int nc, int order, int dir, const double* fplus,
+                            const double* fminus, double* frecon, cudaStream_t st) {
+  k_weno_dir<<<blocks_for(g.Ntot), kThreads, 0, st>>>(g, nc, order, dir, fplus, fminus, frecon);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_fvs_generic(const Grid& g, int model, int order, double* cons, double* prims,
                                double* aux, double* fplus, double* fminus, double* frecon,
                                double* fnet, cudaStream_t st) {

@@ -37,6 +37,19 @@ cudaError_t format_body(const Grid& g, const double* arr, int nvars, std::string
 cudaError_t launch_prims_to_all(const Grid& g, int model, const double* prims, double* cons,
                                 double* aux, cudaStream_t st);
 cudaError_t launch_apply_bcs(const Grid& g, double* arr, int nvars, cudaStream_t st);
+// WenoBase::reconstructUpwind + reconstructDownwind of nc variables along dir
+// on materialised ghosts: frecon = upwind(f+) + downwind(f-) on
+// [shift, N - shift), zero elsewhere (fluxVectorSplitting.cc:36-49).
+cudaError_t launch_weno_dir(const Grid& g, int nc, int order, int dir, const double* fplus,
+                            const double* fminus, double* frecon, cudaStream_t st);
+
+// REGIME, the resistive source extension of SRMHD (regime.cu).
+struct RegimeWork {
+  double *E, *q, *fp, *fm, *frx, *fry, *K, *DX, *DY;
+};
+cudaError_t launch_regime_source_add(const Grid& g, int order, const double* cons,
+                                     const double* prims, double* target, double dt,
+                                     const RegimeWork& w, cudaStream_t st);
 // Bcs::apply for the ghost cells of x-rows [r0, r1) (ghost-inclusive indices).
 cudaError_t launch_apply_bcs_rows(const Grid& g, double* arr, int nvars, int r0, int r1,
                                   cudaStream_t st);

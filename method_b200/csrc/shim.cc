@@ -110,6 +110,12 @@ mth_handle* Data::gpu() {
   c.integrator = timeInt_ ? timeInt_->integratorId() : MTH_RK2;
   if (c.integrator >= MTH_SSP2 && c.model != MTH_SRRMHD)
     throw std::invalid_argument("the IMEX integrators are provided for the SRRMHD model");
+  if (timeInt_ && timeInt_->integratorId() == MTH_RKSPLIT && timeInt_->modelExtension &&
+      timeInt_->modelExtension->sourceExists && timeInt_->modelExtension->extensionId() == 1) {
+    if (c.model != MTH_SRMHD || dims == 3)
+      throw std::invalid_argument("REGIME extends the SRMHD model in one or two dimensions");
+    c.regime = 1;
+  }
   c.precision = precision;
   c.guess = guess;
   c.device = device;

@@ -33,7 +33,7 @@ class RefConfig(C.Structure):
         ("gamma", C.c_double), ("sigma", C.c_double), ("cp", C.c_double),
         ("weno", C.c_int), ("bcs", C.c_int), ("integrator", C.c_int),
         ("init", C.c_int), ("init_arg0", C.c_int), ("init_arg1", C.c_int),
-        ("functional_sigma", C.c_int), ("sigma_exp", C.c_double),
+        ("functional_sigma", C.c_int), ("sigma_exp", C.c_double), ("extension", C.c_int),
     ]
 
 
@@ -109,6 +109,7 @@ def make_config(**kw) -> RefConfig:
     c.init_arg1 = kw.get("init_arg1", 0)
     c.functional_sigma = 1 if kw.get("functionalSigma", False) else 0
     c.sigma_exp = kw.get("gam", 12.0)
+    c.extension = 1 if kw.get("regime", False) else 0
     return c
 
 

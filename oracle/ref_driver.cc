@@ -24,6 +24,7 @@
 #include "srmhd.h"
 #include "srrmhd.h"
 #include "weno.h"
+#include "REGIME.h"
 #include "wenoUpwinds.h"
 #include "fluxVectorSplitting.h"
 #include "boundaryConds.h"
@@ -56,6 +57,7 @@ typedef struct {
   int init_arg0, init_arg1;
   int functional_sigma;  // Data::functionalSigma
   double sigma_exp;      // Data::gam
+  int extension;         // 0 = none, 1 = REGIME (RKSplit's model extension)
 } mref_config;
 
 }  // extern "C"
@@ -84,8 +86,10 @@ struct RefSim {
   Simulation* sim = nullptr;
   InitialFunc* init = nullptr;
   TimeIntegrator* timeInt = nullptr;
+  ModelExtension* ext = nullptr;
   ~RefSim() {
     delete timeInt;
+    delete ext;
     delete init;
     delete sim;
     delete outflow;
@@ -133,7 +137,10 @@ void* mref_create(const mref_config* c, const double* prims) {
       default: r->init = new CurrentSheetSingleFluid(r->data, c->init_arg0); break;
     }
     if (c->integrator == 0) r->timeInt = new RK2(r->data, r->model, r->bcs, r->flux);
-    else if (c->integrator == 1) r->timeInt = new RKSplit(r->data, r->model, r->bcs, r->flux);
+    else if (c->integrator == 1) {
+      if (c->extension == 1) r->ext = new REGIME(r->data, r->flux);
+      r->timeInt = new RKSplit(r->data, r->model, r->bcs, r->flux, r->ext);
+    }
     else if (c->integrator == 3) r->timeInt = new SSP3(r->data, r->model, r->bcs, r->flux);
     else if (c->integrator == 4) r->timeInt = mref_new_ssp2322(r->data, r->model, r->bcs, r->flux);
     else r->timeInt = new SSP2(r->data, r->model, r->bcs, r->flux);

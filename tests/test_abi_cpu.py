@@ -74,3 +74,14 @@ def test_reference_style_driver_builds(tmp_path):
            "-Wl,-rpath," + os.path.join(ROOT, "method_b200")]
     r = subprocess.run(cmd, capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+def test_regime_configuration_rules():
+    """The REGIME extension runs with SRMHD and RKSplit in one or two
+    dimensions; other combinations are rejected on the host."""
+    import method_b200 as mb
+    base = dict(nx=16, ny=16, Ng=4, weno=3, bcs="periodic", regime=True)
+    for bad in (dict(model="srrmhd", integrator="rksplit"), dict(model="srmhd", integrator="rk2"),
+                dict(model="srmhd", integrator="rksplit", nz=16)):
+        with pytest.raises(ValueError):
+            mb.Simulation(**dict(base, **bad))

@@ -91,3 +91,35 @@ def test_single_cell_c2p_batch_matches_oracle():
     W = 1.0 / np.sqrt(1.0 - sol[ok, 0])
     assert np.array_equal(aux[1, ok], W)
     assert (rc == 1) == (not np.all(ok))
+
+
+@pytest.mark.skipif(shutil.which("g++") is None, reason="no host compiler")
+def test_regime_driver_matches_reference(tmp_path, ref):
+    """tests/cpp/regime_main.cc: REGIME(&data, &fvs) handed to RKSplit, as the
+    reference's REGIME examples wire it, against the reference CPU build."""
+    exe = tmp_path / "regime_main"
+    r = subprocess.run(["g++", "-std=c++11", "-O2", "-I",
+                        os.path.join(ROOT, "include", "method_b200"),
+                        os.path.join(ROOT, "tests", "cpp", "regime_main.cc"), "-o", str(exe),
+                        "-L", os.path.join(ROOT, "method_b200"), "-lmethod_b200",
+                        "-Wl,-rpath," + os.path.join(ROOT, "method_b200")],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    out, init = tmp_path / "state.bin", tmp_path / "prims0.bin"
+    r = subprocess.run([str(exe), str(out), str(init)], capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    Nx = Ny = 48
+    data = np.fromfile(out, dtype=np.float64)
+    cons = data[:9 * Nx * Ny].reshape(9, Nx, Ny, 1)
+    prims = data[9 * Nx * Ny:].reshape(8, Nx, Ny, 1)
+    prims0 = np.fromfile(init, dtype=np.float64).reshape(8, Nx, Ny, 1)
+    cfg = dict(model="srmhd", nx=40, ny=40, xmin=0.0, xmax=1.0, ymin=0.0, ymax=1.0, endTime=1.0,
+               cfl=0.4, Ng=4, gamma=2.0, sigma=1e3, weno=3, bcs="periodic",
+               integrator="rksplit", regime=True)
+    rs = ref.RefSim(prims=prims0, **cfg)
+    rs.update_time(5)
+    rc, rp, _ = rs.state()
+    rs.close()
+    assert np.array_equal(cons, rc)
+    assert np.array_equal(prims, rp)
