@@ -567,8 +567,76 @@ def cpu_kh(cfg, p0, steps=100):
                                     f"serial build (-O3), {el:.1f} s on the host"}
 
 
-def cpu_legs(initial, sheet, kh, ensemble):
+REGIME_WORKLOAD = ("SRMHD relativistic Orszag-Tang 2D 1024x1024 periodic, FVS+WENO5, RKSplit "
+                   "with the REGIME resistive extension, sigma 1e4, CFL 0.4, gamma 4/3")
+
+
+def regime_cfg():
+    return dict(CFG, integrator="rksplit", regime=True, sigma=1e4)
+
+
+def run_regime(mb, initial, torch, ranks, n, K, W, peak):
+    """REGIME (the resistive extension of SRMHD, REGIME.cc) as RKSplit's model
+    extension on the Orszag-Tang grid, plain and mixed forms; the extension's
+    launches are timed as one group (`regime_source_add`)."""
+    cfg = regime_cfg()
+    p0 = initial.orszag_tang(n, Ng=4)
+    dt = steady_dt(n)
+    cells = n * n
+    res = {"workload": REGIME_WORKLOAD, "unit": "zone-updates/s", "n": n}
+    for form, prec in (("plain", "fp64"), ("mixed", "mixed")):
+        sim = mb.Simulation(nx=n, ny=n, precision=prec, device=ranks.local, **cfg)
+        sim.set_prims(p0)
+        kk = max(2, K // 5) if form == "plain" else K
+        ms = timed_steps(sim, torch, ranks.local, dt, kk, W, ranks.barrier, ranks.max)
+        st = sim.stats()
+        ks = sim.profile_step(dt, reps=3)
+        step_ms = sum(k["total_ms"] for k in ks) / 3.0
+        reg = next(k for k in ks if k["name"] == "regime_source_add")
+        reg_ms = reg["total_ms"] / reg["launches"]
+        res[form] = {
+            "value": ranks.world * cells * kk / (ms * 1e-3), "ms_per_step": ms / kk,
+            "steps": kk, "c2p_unconverged": st["c2p_unconverged"],
+            "regime": {"ms_per_launch": round(reg_ms, 4),
+                       "share_of_profiled_step": round(reg_ms / step_ms, 4),
+                       "bytes_per_launch": reg["bytes_per_launch"],
+                       "achieved_gbs": round(reg["bytes_per_launch"] / (reg_ms * 1e-3) / 1e9, 1),
+                       "peak": peak},
+            "kernels": [{"name": k["name"], "launches_per_step": k["launches"] / 3.0,
+                         "ms_per_launch": round(k["total_ms"] / k["launches"], 4)} for k in ks],
+        }
+        sim.close()
+    return res
+
+
+def cpu_regime(n=512, steps=2):
+    """The reference build's serial RKSplit + REGIME step on an n^2 Orszag-Tang
+    grid (bounded sample of the REGIME workload)."""
+    from method_b200 import initial
+    cfg = regime_cfg()
+    p0 = initial.orszag_tang(n, Ng=4)
+    try:
+        from oracle import ref
+        if not ref.available():
+            raise FileNotFoundError
+        sim = ref.RefSim(prims=p0, nx=n, ny=n, **cfg)
+    except (FileNotFoundError, OSError):
+        return None  # the oracle port has no REGIME
+    dt = steady_dt(n)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        sim.step_dt(dt)
+    el = time.perf_counter() - t0
+    sim.close()
+    return {"value": n * n * steps / el, "unit": "zone-updates/s", "cores": 1,
+            "kind": "reference", "sample": f"{steps} RKSplit + REGIME steps of a {n}x{n} grid, "
+                                           f"serial build (-O3), {el:.1f} s on the host"}
+
+
+def cpu_legs(initial, sheet, kh, ensemble, regime=None):
     """The reference build's CPU baselines of the side workloads."""
+    if regime is not None:
+        regime["cpu_baseline"] = cpu_regime()
     if sheet is not None:
         sheet["cpu_baseline"] = cpu_sheet(sheet_cfg(sheet["sigma"]),
                                           initial.current_sheet(*SHEET_N, seed=SHEET_SEED),
@@ -726,6 +794,7 @@ def main():
     ap.add_argument("--no-sheet", action="store_true", help="skip the SSP2 current sheet")
     ap.add_argument("--no-kh", action="store_true", help="skip the whole KH 64x128 run")
     ap.add_argument("--no-long-l1", action="store_true", help="skip the 500-step L1 check")
+    ap.add_argument("--no-regime", action="store_true", help="skip the REGIME RKSplit workload")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
@@ -804,11 +873,14 @@ def main():
         kh = None
         if not args.no_kh:
             kh = run_kh_full(mb, initial, torch, ranks, peak, cpu=False)
+        regime = None
+        if not args.no_regime:
+            regime = run_regime(mb, initial, torch, ranks, n, max(K // 5, 5), max(W, 3), peak)
     clk = clocks.summary()
     long_l1 = None if args.no_long_l1 else long_run_l1(mb, initial, ranks, n)
     if want_cpu:  # reference-build baselines on the host, after the timed GPU work
         with quiet_stdout():
-            cpu_legs(initial, sheet, kh, ensemble)
+            cpu_legs(initial, sheet, kh, ensemble, regime)
 
     cells = n * n
     for form in forms:
@@ -907,6 +979,7 @@ def main():
             "l1_mixed_vs_fp64": l1,
             "l1_mixed_vs_fp64_500_steps": long_l1,
             "kh64x128_full_run": kh,
+            "regime_rksplit": regime,
             "sheet_ssp2": sheet,
             "ensemble": ensemble,
             "c2p_batch": c2p_batch,

@@ -290,9 +290,11 @@ cudaError_t enqueue_part(mth_handle* h, double dt, int part) {
         if ((e = launch_apply_bcs(h->g, h->cons, h->NC, h->st)) ||
             (e = launch_apply_bcs(h->g, h->prims, h->NP, h->st)))
           return e;
-        if ((e = timed(h, "regime_source_add", 40.0, [&] {
+        // algorithmic traffic: prims (8) and cons (9) read, cons (9) written
+        if ((e = timed(h, "regime_source_add", 26.0, [&] {
                return launch_regime_source_add(h->g, h->cfg.weno_order, h->cons, h->prims,
-                                               h->cons, dt, h->regime, h->st);
+                                               h->cons, dt, h->regime,
+                                               h->cfg.precision == MTH_MIXED, h->st);
              })))
           return e;
       } else if ((e = timed(h, "source_add", 2.0 * h->NC, [&] {

@@ -47,9 +47,22 @@ cudaError_t launch_weno_dir(const Grid& g, int nc, int order, int dir, const dou
 struct RegimeWork {
   double *E, *q, *fp, *fm, *frx, *fry, *K, *DX, *DY;
 };
+// target (interior) += dt (S(cons) + S_REGIME).  `mixed`: the 2D tile
+// reconstructs the stiff fluxes in FP32 (the diffusion vectors and the update
+// stay FP64); otherwise every value is the reference's.
 cudaError_t launch_regime_source_add(const Grid& g, int order, const double* cons,
                                      const double* prims, double* target, double dt,
-                                     const RegimeWork& w, cudaStream_t st);
+                                     const RegimeWork& w, bool mixed, cudaStream_t st);
+// The fused 2D tile with FP32 stiff-flux reconstruction (regime_mixed.cu).
+cudaError_t launch_regime_tile_mixed(const Grid& g, int order, const double* cons,
+                                     const double* prims, double* target, double dt,
+                                     cudaStream_t st);
+// Whether the fused tile serves the grid: two dimensions and a constant
+// conductivity (with functionalSigma a halo cell's sigma would read cons[0]
+// that a neighbouring CTA updates in place).
+inline bool regime_tile_applies(const Grid& g) {
+  return g.dims == 2 && g.Nz == 1 && !g.functional_sigma;
+}
 // Bcs::apply for the ghost cells of x-rows [r0, r1) (ghost-inclusive indices).
 cudaError_t launch_apply_bcs_rows(const Grid& g, double* arr, int nvars, int r0, int r1,
                                   cudaStream_t st);
