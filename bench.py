@@ -877,6 +877,15 @@ def main():
         if not args.no_regime:
             regime = run_regime(mb, initial, torch, ranks, n, max(K // 5, 5), max(W, 3), peak)
     clk = clocks.summary()
+    if regime is not None:  # what bounds the tile (ncu figures of a 768^2 capture)
+        for form, key in (("plain", "regime_tile_fp64"), ("mixed", "regime_tile_mixed")):
+            rec, rg = ncu_record(key), regime[form]["regime"]
+            rg["ncu"] = {k: rec[k] for k in ("fp64_pipe_active_pct", "fma_pipe_active_pct",
+                                             "issue_active_pct", "warps_active_pct")
+                         if k in rec} or None
+            if rec.get("fp64_thread_inst_per_cell"):
+                rg["fp64_pipe"] = fp64_pipe_roofline(rec["fp64_thread_inst_per_cell"],
+                                                     regime["n"] ** 2, rg["ms_per_launch"], clk)
     long_l1 = None if args.no_long_l1 else long_run_l1(mb, initial, ranks, n)
     if want_cpu:  # reference-build baselines on the host, after the timed GPU work
         with quiet_stdout():
