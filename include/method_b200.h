@@ -27,10 +27,10 @@ typedef enum {
   MTH_ERR_CUDA = 4        /* CUDA runtime error (no device, launch failure, ...) */
 } mth_status;
 
-enum { MTH_SRMHD = 0, MTH_SRRMHD = 1 };                       /* Model subclasses */
+enum { MTH_SRMHD = 0, MTH_SRRMHD = 1, MTH_HYBRID = 2 };       /* Model subclasses */
 enum { MTH_OUTFLOW = 0, MTH_PERIODIC = 1, MTH_FLOW = 2 };     /* Bcs subclasses */
 enum { MTH_RK2 = 0, MTH_RKSPLIT = 1, MTH_SSP2 = 2,             /* TimeIntegrator subclasses */
-       MTH_SSP3 = 3, MTH_SSP2322 = 4 };                         /* (IMEX: SRRMHD only) */
+       MTH_SSP3 = 3, MTH_SSP2322 = 4, MTH_RKSPLIT2 = 5 };       /* (IMEX: SRRMHD only) */
 enum { MTH_PLAIN_FP64 = 0, MTH_MIXED = 1 };                   /* precision of the flux path */
 enum { MTH_GUESS_PREVIOUS = 0, MTH_GUESS_MLP = 1, MTH_GUESS_COLD = 2 }; /* C2P initial guess */
 enum { MTH_C2P_HYBRD = 0, MTH_C2P_NEWTON = 1 };               /* C2P solver */
@@ -38,7 +38,7 @@ enum { MTH_C2P_HYBRD = 0, MTH_C2P_NEWTON = 1 };               /* C2P solver */
 /* The Data constructor arguments (Project/CPU/Include/simData.h:205-218) plus
  * the choice of Model, WENO order, Bcs and TimeIntegrator. */
 typedef struct {
-  int model;                 /* MTH_SRMHD / MTH_SRRMHD */
+  int model;                 /* MTH_SRMHD / MTH_SRRMHD / MTH_HYBRID */
   int nx, ny, nz;            /* interior cells; ny = 0 for 1D, nz = 0 for 2D */
   double xmin, xmax, ymin, ymax, zmin, zmax;
   double endTime, cfl;
@@ -46,7 +46,8 @@ typedef struct {
   double gamma, sigma, cp;
   int weno_order;            /* 3 or 5 (Weno3 / Weno5) */
   int bcs;                   /* MTH_OUTFLOW / MTH_PERIODIC / MTH_FLOW */
-  int integrator;            /* MTH_RK2 / MTH_RKSPLIT / MTH_SSP2 / MTH_SSP3 / MTH_SSP2322 */
+  int integrator;            /* MTH_RK2 / MTH_RKSPLIT / MTH_SSP2 / MTH_SSP3 / MTH_SSP2322 /
+                                MTH_RKSPLIT2 (rkSplit2ndOrder.cc) */
   int precision;             /* MTH_PLAIN_FP64 / MTH_MIXED */
   int guess;                 /* MTH_GUESS_PREVIOUS / MTH_GUESS_MLP */
   int device;                /* CUDA device ordinal */
@@ -64,8 +65,14 @@ typedef struct {
   /* 1: the REGIME resistive extension of SRMHD (REGIME.cc, Wright & Hawke
    * 2019) as RKSplit's model extension, as `REGIME ext(&data, &fvs);
    * RKSplit ti(&data, &model, &bcs, &fvs, &ext)`: SRMHD, RKSplit, one or two
-   * dimensions; sigma is its conductivity. */
+   * dimensions; sigma is its conductivity.  With model MTH_HYBRID it is the
+   * Hybrid model's useREGIME instead (hybrid.h:76). */
   int regime;
+  /* MTH_HYBRID (Hybrid(data, sigmaCrossOver, sigmaSpan, useREGIME),
+   * hybrid.cc:26-77): the conductivity at which the ideal and resistive
+   * models are blended half and half, and the half-width of the blend. */
+  double sigma_crossover;
+  double sigma_span;
 } mth_config;
 
 typedef struct {

@@ -19,9 +19,9 @@ import numpy as np
 
 from . import _lib
 
-MODELS = {"srmhd": 0, "srrmhd": 1}
+MODELS = {"srmhd": 0, "srrmhd": 1, "hybrid": 2}
 BCS = {"outflow": 0, "periodic": 1, "flow": 2}
-INTEGRATORS = {"rk2": 0, "rksplit": 1, "ssp2": 2, "ssp3": 3, "ssp2322": 4}
+INTEGRATORS = {"rk2": 0, "rksplit": 1, "ssp2": 2, "ssp3": 3, "ssp2322": 4, "rksplit2": 5}
 PRECISIONS = {"fp64": 0, "mixed": 1}
 GUESSES = {"previous": 0, "mlp": 1}
 
@@ -50,10 +50,12 @@ def _dptr(a):
 def _config(nx, ny, nz=0, xmin=0.0, xmax=1.0, ymin=0.0, ymax=1.0, zmin=0.0, zmax=1.0,
             endTime=1.0, cfl=0.5, Ng=4, gamma=5.0 / 3.0, sigma=1e3, cp=0.1, model="srmhd",
             weno=3, bcs="periodic", integrator="rk2", precision="fp64", guess="previous",
-            device=0, functionalSigma=False, gam=12.0, x_slab=None, regime=False):
+            device=0, functionalSigma=False, gam=12.0, x_slab=None, regime=False,
+            sigmaCrossOver=150.0, sigmaSpan=50.0, useREGIME=True):
     """mth_config from the reference Data constructor's arguments plus the
     class choices of a reference main.cc (``regime=True``: the REGIME model
-    extension with RKSplit)."""
+    extension with RKSplit; ``model="hybrid"``: Hybrid(data, sigmaCrossOver,
+    sigmaSpan, useREGIME))."""
     c = _lib.Config()
     c.model = MODELS[model]
     c.nx, c.ny, c.nz = nx, ny, nz
@@ -69,6 +71,9 @@ def _config(nx, ny, nz=0, xmin=0.0, xmax=1.0, ymin=0.0, ymax=1.0, zmin=0.0, zmax
     c.functional_sigma = 1 if functionalSigma else 0
     c.sigma_exp = gam
     c.regime = 1 if regime else 0
+    c.sigma_crossover, c.sigma_span = sigmaCrossOver, sigmaSpan
+    if model == "hybrid":
+        c.regime = 1 if useREGIME else 0
     if x_slab is not None:  # (offset, global nx): columns [offset, offset + nx) of the domain
         c.x_slab = 1
         c.x_offset, c.x_global_nx = x_slab

@@ -59,6 +59,7 @@ class Config(C.Structure):
         ("precision", C.c_int), ("guess", C.c_int), ("device", C.c_int),
         ("functional_sigma", C.c_int), ("sigma_exp", C.c_double),
         ("x_slab", C.c_int), ("x_global_nx", C.c_int), ("x_offset", C.c_int), ("regime", C.c_int),
+        ("sigma_crossover", C.c_double), ("sigma_span", C.c_double),
     ]
 
 

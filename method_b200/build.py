@@ -8,6 +8,7 @@ Translation units and their floating-point contracts:
                     expression like the reference's x86-64 build (no FMA).
   regime.cu         -fmad=false: the REGIME source extension, plain form.
   regime_mixed.cu   FMA allowed: its fused tile with FP32 stiff-flux WENO.
+  hybrid.cu         -fmad=false: the Hybrid model (blended SRMHD / SRRMHD).
   kernels_mixed.cu  FMA allowed: FP32 flux path, Newton primitive recovery.
   mlp.cu            FMA allowed: guess-network inference / training kernels.
   api.cu            C-ABI, host logic only.
@@ -36,6 +37,7 @@ COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler",
 UNITS = [
     ("kernels_fp64.cu", ["-fmad=false", "-prec-div=true", "-prec-sqrt=true"]),
     ("regime.cu", ["-fmad=false", "-prec-div=true", "-prec-sqrt=true"]),
+    ("hybrid.cu", ["-fmad=false", "-prec-div=true", "-prec-sqrt=true"]),
     ("regime_mixed.cu", []),
     ("kernels_mixed.cu", []),
     ("mlp.cu", []),

@@ -42,6 +42,8 @@ struct mth_handle {
   long long* counters = nullptr;  // [0..3] C2P, [4..7] implicit, [8..9] Newton fallbacks
   MixedWork mixed{};
   RegimeWork regime{};
+  // RKSplit2's source array; the Hybrid model's REGIME term
+  double *hsrc = nullptr, *hext = nullptr;
   double t = 0, dt = 0;
   int iters = 0;
   long long steps = 0;
@@ -135,6 +137,8 @@ cudaError_t c2p_raw(mth_handle* h, const double* cons, const double* pg, const d
                             h->solution, c2p_work(h), h->mixed, lean && h->fused, h->st);
   if (h->cfg.model == MTH_SRMHD)
     return launch_c2p_srmhd(h->g, cons, pg, ag, prims, aux, h->solution, c2p_work(h), h->st);
+  if (h->cfg.model == MTH_HYBRID)  // with Hybrid::finalise, which updates cons' E
+    return launch_c2p_hybrid(h->g, cons, pg, ag, prims, aux, c2p_work(h), h->st);
   return launch_c2p_srrmhd(h->g, cons, ag, prims, aux, c2p_work(h), h->st);
 }
 
@@ -163,8 +167,10 @@ cudaError_t c2p(mth_handle* h, const double* cons, const double* pg, const doubl
                 double* prims, double* aux, bool lean = false) {
   const bool srmhd = h->cfg.model == MTH_SRMHD;
   const bool mixed = h->cfg.precision == MTH_MIXED || h->cfg.guess == MTH_GUESS_MLP;
-  const char* name = srmhd ? (mixed ? "c2p_newton_srmhd" : "c2p_hybrd_srmhd")
-                           : (mixed ? "c2p_newton_srrmhd" : "c2p_secant_srrmhd");
+  const char* name = h->cfg.model == MTH_HYBRID
+                         ? "c2p_hybrid"
+                         : srmhd ? (mixed ? "c2p_newton_srmhd" : "c2p_hybrd_srmhd")
+                                 : (mixed ? "c2p_newton_srrmhd" : "c2p_secant_srrmhd");
   // doubles per cell: SRMHD 14 read, 23 written (13 lean); SRRMHD 15 read, 28 written (10 lean)
   const bool lean_run = lean && mixed && h->fused;
   return timed(h, name, srmhd ? (lean_run ? 27 : 37) : (lean_run ? 25 : 43),
@@ -245,7 +251,7 @@ int n_parts(const mth_handle* h) {
   const int integ = h->cfg.integrator;
   if (integ == MTH_RK2 || integ == MTH_RKSPLIT) return 2;
   if (integ == MTH_SSP2) return 3;
-  return 1;
+  return 1;  // SSP3, SSP2322, RKSplit2
 }
 
 // The state a part leaves for the next part's flux (cons, prims, aux).
@@ -266,6 +272,42 @@ void part_state(mth_handle* h, int part, double** c, double** p, double** a) {
 }
 
 cudaError_t enqueue_ssp2_part(mth_handle* h, double dt, int part);
+
+// RKSplit2::setSource and the half step after it (rkSplit2ndOrder.cc:8-51):
+// S(U) of the model (the Hybrid model's with its REGIME term) on the state
+// whose ghosts the boundary conditions filled, U += dt/2 S, finalise.
+cudaError_t rksplit2_half_source(mth_handle* h, double dt) {
+  cudaError_t e;
+  if ((e = launch_apply_bcs(h->g, h->cons, h->NC, h->st)) ||
+      (e = launch_apply_bcs(h->g, h->prims, h->NP, h->st)) ||
+      (e = launch_apply_bcs(h->g, h->aux, h->NA, h->st)))
+    return e;
+  if ((e = timed(h, "source", 2.0 * h->NC, [&] {
+         if (h->cfg.model == MTH_HYBRID)
+           return launch_hybrid_source(h->g, h->cfg.weno_order, h->cons, h->prims, h->aux,
+                                       h->hsrc, h->cfg.regime ? &h->regime : nullptr, h->hext,
+                                       h->st);
+         return launch_source(h->g, h->cfg.model, h->cons, h->aux, h->hsrc, h->st);
+       })))
+    return e;
+  if ((e = launch_add_scaled(h->g, h->NC, h->cons, h->hsrc, 0.5 * dt, h->st))) return e;
+  return c2p(h, h->cons, h->prims, h->aux, h->prims, h->aux);
+}
+
+// RKSplit2::step (rkSplit2ndOrder.cc:33-67): half source, RK2::step, half
+// source, each followed by finalise.
+cudaError_t enqueue_rksplit2(mth_handle* h, double dt) {
+  cudaError_t e;
+  if ((e = rksplit2_half_source(h, dt))) return e;
+  if ((e = flux_stage(h, h->cons, h->prims, h->aux, nullptr, h->p1cons, dt, STAGE_EULER)))
+    return e;
+  if ((e = c2p(h, h->p1cons, h->prims, h->aux, h->p1prims, h->p1aux, true))) return e;
+  if ((e = flux_stage(h, h->p1cons, h->p1prims, h->p1aux, h->cons, h->cons, dt,
+                      STAGE_RK2_CORR)))
+    return e;
+  if ((e = c2p(h, h->cons, h->prims, h->aux, h->prims, h->aux))) return e;
+  return rksplit2_half_source(h, dt);
+}
 
 // Part `part` of one TimeIntegrator::step, enqueued on the handle's stream.
 cudaError_t enqueue_part(mth_handle* h, double dt, int part) {
@@ -308,6 +350,7 @@ cudaError_t enqueue_part(mth_handle* h, double dt, int part) {
     return cudaSuccess;
   }
   if (integ == MTH_SSP3 || integ == MTH_SSP2322) return enqueue_ssp3(h, dt);
+  if (integ == MTH_RKSPLIT2) return enqueue_rksplit2(h, dt);
   return enqueue_ssp2_part(h, dt, part);
 }
 
@@ -502,6 +545,8 @@ bool grid_from_config(const void* cfg, Grid* out) {
   g.sigma = c.sigma;
   g.functional_sigma = c.functional_sigma ? 1 : 0;
   g.sigma_exp = c.sigma_exp;
+  g.sigma_cross = c.sigma_crossover;
+  g.sigma_span = c.sigma_span;
   g.cp = c.cp;
   g.Ntot = (long long)g.Nx * g.Ny * g.Nz;
   return true;
@@ -518,7 +563,7 @@ mth_status mth_create(const mth_config* cfg, mth_handle** out) {
   const mth_config& c = *cfg;
   // Validation of Data::initData (simData.cc:98-107) and the WENO ghost rule
   // (weno.cc:13-20).
-  if (c.model != MTH_SRMHD && c.model != MTH_SRRMHD) {
+  if (c.model != MTH_SRMHD && c.model != MTH_SRRMHD && c.model != MTH_HYBRID) {
     delete h;
     return MTH_ERR_INVALID;
   }
@@ -527,13 +572,18 @@ mth_status mth_create(const mth_config* cfg, mth_handle** out) {
        c.weno_order != 11) ||
       c.Ng < (c.weno_order + 1) / 2 + 1 || c.nx <= 0 || c.ny < 0 || c.nz < 0 ||
       (c.ny == 0 && c.nz != 0) || c.bcs < 0 || c.bcs > 2 || c.integrator < 0 ||
-      c.integrator > 4 || (c.integrator >= MTH_SSP2 && c.model != MTH_SRRMHD) ||
-      (c.integrator >= MTH_SSP3 && c.guess != 0) ||
+      c.integrator > 5 ||
+      (c.integrator >= MTH_SSP2 && c.integrator <= MTH_SSP2322 && c.model != MTH_SRRMHD) ||
+      ((c.integrator == MTH_SSP3 || c.integrator == MTH_SSP2322) && c.guess != 0) ||
       c.precision < 0 || c.precision > 1 || c.guess < 0 || c.guess > 1 ||
       (c.x_slab && c.integrator != MTH_RK2 && c.integrator != MTH_RKSPLIT &&
        c.integrator != MTH_SSP2) ||
-      (c.regime && (c.model != MTH_SRMHD || c.integrator != MTH_RKSPLIT || c.nz != 0 ||
-                    c.x_slab))) {
+      (c.regime && c.model != MTH_HYBRID &&
+       (c.model != MTH_SRMHD || c.integrator != MTH_RKSPLIT || c.nz != 0 || c.x_slab)) ||
+      // the Hybrid model: plain form, RK2 or RKSplit2, previous-state guesses
+      (c.model == MTH_HYBRID &&
+       (c.precision != MTH_PLAIN_FP64 || c.guess != 0 || c.x_slab || !(c.sigma_span > 0) ||
+        (c.integrator != MTH_RK2 && c.integrator != MTH_RKSPLIT2)))) {
     delete h;
     return MTH_ERR_INVALID;
   }
@@ -545,7 +595,7 @@ mth_status mth_create(const mth_config* cfg, mth_handle** out) {
   h->NC = c.model == MTH_SRMHD ? 9 : 14;
   h->NP = c.model == MTH_SRMHD ? 8 : 11;
   h->NA = c.model == MTH_SRMHD ? 13 : 17;
-  h->fused = (g.dims == 2);
+  h->fused = (g.dims == 2) && c.model != MTH_HYBRID;
   h->device = c.device;
 
   auto bail = [&](const char* what, cudaError_t e) {
@@ -561,7 +611,9 @@ mth_status mth_create(const mth_config* cfg, mth_handle** out) {
   if ((e = alloc0(&h->cons, bytes(h, h->NC), h->st))) return bail("cons", e);
   if ((e = alloc0(&h->prims, bytes(h, h->NP), h->st))) return bail("prims", e);
   if ((e = alloc0(&h->aux, bytes(h, h->NA), h->st))) return bail("aux", e);
-  if (c.integrator == MTH_RK2 || c.integrator == MTH_RKSPLIT) {
+  if (c.integrator == MTH_RK2 || c.integrator == MTH_RKSPLIT || c.integrator == MTH_RKSPLIT2) {
+    if (c.integrator == MTH_RKSPLIT2 && (e = alloc0(&h->hsrc, bytes(h, h->NC), h->st)))
+      return bail("source", e);
     if ((e = alloc0(&h->p1cons, bytes(h, h->NC), h->st))) return bail("p1cons", e);
     if ((e = alloc0(&h->p1prims, bytes(h, h->NP), h->st))) return bail("p1prims", e);
     if ((e = alloc0(&h->p1aux, bytes(h, h->NA), h->st))) return bail("p1aux", e);
@@ -597,6 +649,8 @@ mth_status mth_create(const mth_config* cfg, mth_handle** out) {
                     std::make_pair(&w.fry, 3), std::make_pair(&w.K, 3), std::make_pair(&w.DX, 8),
                     std::make_pair(&w.DY, 8)})
       if ((e = alloc0(pn.first, bytes(h, pn.second), h->st))) return bail("regime", e);
+    if (c.model == MTH_HYBRID && (e = alloc0(&h->hext, bytes(h, 9), h->st)))
+      return bail("regime", e);
   }
   if ((e = cudaStreamSynchronize(h->st))) return bail("sync", e);
   *out = h;
@@ -612,7 +666,8 @@ mth_status mth_destroy(mth_handle* h) {
                     h->u1, h->u2, h->flux1, h->flux2, h->src1, h->src2, h->fnet, h->fplus,
                     h->fminus, h->frecon, h->u3, h->flux3, h->src3, h->tprims, h->taux,
                     h->regime.E, h->regime.q, h->regime.fp, h->regime.fm, h->regime.frx,
-                    h->regime.fry, h->regime.K, h->regime.DX, h->regime.DY})
+                    h->regime.fry, h->regime.K, h->regime.DX, h->regime.DY, h->hsrc,
+                    h->hext})
     if (p) cudaFree(p);
   if (h->fail_list) cudaFree(h->fail_list);
   if (h->fail_count) cudaFree(h->fail_count);
@@ -640,11 +695,23 @@ mth_status mth_get_dims(const mth_handle* h, int* d) {
   return MTH_OK;
 }
 
+// Model::primsToAll of the handle's prims.  The Hybrid model's
+// (hybrid.cc:438-472): SRRMHD's, SRMHD's of the first eight prims into
+// scratch planes, then the blend.
+cudaError_t prims_to_all(mth_handle* h) {
+  cudaError_t e;
+  if (h->cfg.model != MTH_HYBRID)
+    return launch_prims_to_all(h->g, h->cfg.model, h->prims, h->cons, h->aux, h->st);
+  if ((e = launch_prims_to_all(h->g, MTH_SRRMHD, h->prims, h->cons, h->aux, h->st))) return e;
+  if ((e = launch_prims_to_all(h->g, MTH_SRMHD, h->prims, h->fplus, h->fminus, h->st))) return e;
+  return launch_hybrid_blend(h->g, h->cons, h->prims, h->aux, h->fplus, h->fminus, h->st);
+}
+
 mth_status mth_set_prims(mth_handle* h, const double* prims_host) {
   if (!h || !prims_host) return MTH_ERR_INVALID;
   CU(h, cudaSetDevice(h->device));
   CU(h, cudaMemcpyAsync(h->prims, prims_host, bytes(h, h->NP), cudaMemcpyHostToDevice, h->st));
-  CU(h, launch_prims_to_all(h->g, h->cfg.model, h->prims, h->cons, h->aux, h->st));
+  CU(h, prims_to_all(h));
   CU(h, launch_apply_bcs(h->g, h->cons, h->NC, h->st));
   CU(h, launch_apply_bcs(h->g, h->prims, h->NP, h->st));
   CU(h, launch_apply_bcs(h->g, h->aux, h->NA, h->st));
@@ -693,7 +760,7 @@ mth_status mth_download(mth_handle* h, double* cons, double* prims, double* aux)
 mth_status mth_prims_to_all(mth_handle* h) {
   if (!h) return MTH_ERR_INVALID;
   CU(h, cudaSetDevice(h->device));
-  CU(h, launch_prims_to_all(h->g, h->cfg.model, h->prims, h->cons, h->aux, h->st));
+  CU(h, prims_to_all(h));
   CU(h, cudaStreamSynchronize(h->st));
   return MTH_OK;
 }
@@ -727,6 +794,7 @@ mth_status mth_flux_F(mth_handle* h, double* fnet_host) {
 
 mth_status mth_source(mth_handle* h, double* source_host) {
   if (!h || !source_host) return MTH_ERR_INVALID;
+  if (h->cfg.model == MTH_HYBRID) return MTH_ERR_INVALID;  // the step covers it
   CU(h, cudaSetDevice(h->device));
   CU(h, cudaMemsetAsync(h->fnet, 0, bytes(h, h->NC), h->st));
   CU(h, launch_source(h->g, h->cfg.model, h->cons, h->aux, h->fnet, h->st, true));
@@ -737,6 +805,7 @@ mth_status mth_source(mth_handle* h, double* source_host) {
 
 mth_status mth_flux_vector(mth_handle* h, int dir, double* f_host) {
   if (!h || !f_host || dir < 0 || dir >= 3) return MTH_ERR_INVALID;
+  if (h->cfg.model == MTH_HYBRID) return MTH_ERR_INVALID;  // the step covers it
   CU(h, cudaSetDevice(h->device));
   CU(h, launch_flux_vector(h->g, h->cfg.model, h->cons, h->prims, h->aux, dir, h->fnet, h->st));
   const size_t plane = bytes(h, 1);

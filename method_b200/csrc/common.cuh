@@ -47,6 +47,8 @@ struct Grid {
   long long Ntot;        // Nx*Ny*Nz
   double sigma_exp;      // Data::gam, exponent of a functional conductivity
   int functional_sigma;  // Data::functionalSigma
+  double sigma_cross;    // Hybrid::sigmaCrossOver
+  double sigma_span;     // Hybrid::sigmaSpan
 };
 
 // Data::sigmaFunc (simData.cc:114-127): the conductivity of a cell whose

@@ -1057,12 +1057,16 @@ cudaError_t launch_fvs_generic_raw(const Grid& g, int model, int order, const do
   const int nc = model == MODEL_SRMHD ? 9 : 14;
   const long long nI = (long long)(g.ie - g.is) * (g.je - g.js) * (g.ke - g.ks);
   for (int dir = 0; dir < g.dims; ++dir) {
-    if (model == MODEL_SRMHD)
+    if (model == MODEL_SRMHD) {
       k_split_dir_full<SRMHD><<<blocks_for(g.Ntot), kThreads, 0, st>>>(g, cons, prims, aux, dir,
                                                                         fplus, fminus);
-    else
+    } else if (model == MODEL_HYBRID) {
+      cudaError_t e = launch_hybrid_split(g, cons, prims, aux, dir, fplus, fminus, st);
+      if (e != cudaSuccess) return e;
+    } else {
       k_split_dir_full<SRRMHD><<<blocks_for(g.Ntot), kThreads, 0, st>>>(g, cons, prims, aux,
                                                                          dir, fplus, fminus);
+    }
     k_weno_dir<<<blocks_for(g.Ntot), kThreads, 0, st>>>(g, nc, order, dir, fplus, fminus,
                                                         frecon);
     k_fnet_dir<<<blocks_for(nI), kThreads, 0, st>>>(g, nc, dir, dir == 0, frecon, fnet);

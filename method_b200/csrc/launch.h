@@ -9,7 +9,7 @@
 
 namespace mth {
 
-enum ModelId : int { MODEL_SRMHD = 0, MODEL_SRRMHD = 1 };
+enum ModelId : int { MODEL_SRMHD = 0, MODEL_SRRMHD = 1, MODEL_HYBRID = 2 };
 
 // Per-call C2P bookkeeping on the device.
 struct C2PWork {
@@ -53,6 +53,28 @@ struct RegimeWork {
 cudaError_t launch_regime_source_add(const Grid& g, int order, const double* cons,
                                      const double* prims, double* target, double dt,
                                      const RegimeWork& w, bool mixed, cudaStream_t st);
+// REGIME::sourceExtension alone into ext (9 planes, interior cells): the
+// Hybrid model's REGIME term (hybrid.cc:320-345).
+cudaError_t launch_regime_ext(const Grid& g, int order, const double* cons, const double* prims,
+                              const RegimeWork& w, double* ext, cudaStream_t st);
+// The Hybrid model (hybrid.cu): flux + split along dir of every cell; the
+// recovery of interior cells followed by Hybrid::finalise (which updates
+// cons' E); the source of interior cells (+ REGIME when `regime`, into ext
+// first); primsToAll's blend of resistive and ideal variables.
+cudaError_t launch_hybrid_split(const Grid& g, const double* cons, const double* prims,
+                                const double* aux, int dir, double* fplus, double* fminus,
+                                cudaStream_t st);
+cudaError_t launch_c2p_hybrid(const Grid& g, const double* cons, const double* prims_guess,
+                              const double* aux_guess, double* prims, double* aux, C2PWork w,
+                              cudaStream_t st);
+cudaError_t launch_hybrid_source(const Grid& g, int order, const double* cons,
+                                 const double* prims, const double* aux, double* src,
+                                 const RegimeWork* regime, double* ext, cudaStream_t st);
+cudaError_t launch_hybrid_blend(const Grid& g, double* cons, double* prims, double* aux,
+                                const double* icons, const double* iaux, cudaStream_t st);
+// cons += h src on interior cells.
+cudaError_t launch_add_scaled(const Grid& g, int nc, double* cons, const double* src, double h,
+                              cudaStream_t st);
 // The fused 2D tile with FP32 stiff-flux reconstruction (regime_mixed.cu).
 cudaError_t launch_regime_tile_mixed(const Grid& g, int order, const double* cons,
                                      const double* prims, double* target, double dt,

@@ -152,6 +152,44 @@ __global__ void k_regime_source_add(Grid g, const double* __restrict__ cons,
   }
 }
 
+// REGIME::sourceExtension's result alone (REGIME.cc:97-133) on interior
+// cells: the central differences of the diffusion vectors; phi's entry 0.
+__global__ void k_regime_ext(Grid g, const double* __restrict__ DX,
+                             const double* __restrict__ DY, double* __restrict__ ext) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= n_interior(g)) return;
+  int i, j, k;
+  interior_ijk(g, t, i, j, k);
+  const long long N = g.Ntot, cell = cell_id(g, i, j, k);
+  const long long sx = (long long)g.Ny * g.Nz, sy = g.Nz;
+#pragma unroll
+  for (int v = 0; v < 8; ++v) {
+    double e = (DX[v * N + cell + sx] - DX[v * N + cell - sx]) / (2 * g.dx);
+    if (g.dims > 1) e += (DY[v * N + cell + sy] - DY[v * N + cell - sy]) / (2 * g.dy);
+    ext[v * N + cell] = e;
+  }
+  ext[8 * N + cell] = 0.0;
+}
+
+// E, q, the split stiff fluxes and their faces, K and the diffusion vectors
+// of every cell into w (the per-array chain).
+cudaError_t regime_chain(const Grid& g, int order, const double* cons, const double* prims,
+                         const RegimeWork& w, cudaStream_t st) {
+  const int b = blocks_for(g.Ntot);
+  k_regime_e<<<b, kThreads, 0, st>>>(g, prims, w.E);
+  k_regime_q<<<b, kThreads, 0, st>>>(g, w.E, w.q);
+  cudaError_t e;
+  k_regime_split<<<b, kThreads, 0, st>>>(g, 0, prims, w.E, w.fp, w.fm);
+  if ((e = launch_weno_dir(g, 3, order, 0, w.fp, w.fm, w.frx, st)) != cudaSuccess) return e;
+  if (g.dims > 1) {
+    k_regime_split<<<b, kThreads, 0, st>>>(g, 1, prims, w.E, w.fp, w.fm);
+    if ((e = launch_weno_dir(g, 3, order, 1, w.fp, w.fm, w.fry, st)) != cudaSuccess) return e;
+  }
+  k_regime_k<<<b, kThreads, 0, st>>>(g, w.frx, w.fry, w.K);
+  k_regime_diffu<<<b, kThreads, 0, st>>>(g, cons, prims, w.E, w.q, w.K, w.DX, w.DY);
+  return cudaGetLastError();
+}
+
 }  // namespace
 
 // cons (interior) += dt (S(cons) + S_REGIME) with cons and prims' ghosts
@@ -165,20 +203,18 @@ cudaError_t launch_regime_source_add(const Grid& g, int order, const double* con
     if (mixed) return launch_regime_tile_mixed(g, order, cons, prims, target, dt, st);
     return launch_regime_tile_order<double>(g, order, cons, prims, target, dt, st);
   }
-  const int b = blocks_for(g.Ntot);
-  k_regime_e<<<b, kThreads, 0, st>>>(g, prims, w.E);
-  k_regime_q<<<b, kThreads, 0, st>>>(g, w.E, w.q);
-  cudaError_t e;
-  k_regime_split<<<b, kThreads, 0, st>>>(g, 0, prims, w.E, w.fp, w.fm);
-  if ((e = launch_weno_dir(g, 3, order, 0, w.fp, w.fm, w.frx, st)) != cudaSuccess) return e;
-  if (g.dims > 1) {
-    k_regime_split<<<b, kThreads, 0, st>>>(g, 1, prims, w.E, w.fp, w.fm);
-    if ((e = launch_weno_dir(g, 3, order, 1, w.fp, w.fm, w.fry, st)) != cudaSuccess) return e;
-  }
-  k_regime_k<<<b, kThreads, 0, st>>>(g, w.frx, w.fry, w.K);
-  k_regime_diffu<<<b, kThreads, 0, st>>>(g, cons, prims, w.E, w.q, w.K, w.DX, w.DY);
+  cudaError_t e = regime_chain(g, order, cons, prims, w, st);
+  if (e != cudaSuccess) return e;
   const long long nI = n_interior_host(g);
   k_regime_source_add<<<blocks_for(nI), kThreads, 0, st>>>(g, cons, w.DX, w.DY, target, dt);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_regime_ext(const Grid& g, int order, const double* cons, const double* prims,
+                              const RegimeWork& w, double* ext, cudaStream_t st) {
+  cudaError_t e = regime_chain(g, order, cons, prims, w, st);
+  if (e != cudaSuccess) return e;
+  k_regime_ext<<<blocks_for(n_interior_host(g)), kThreads, 0, st>>>(g, w.DX, w.DY, ext);
   return cudaGetLastError();
 }
 

@@ -18,9 +18,9 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
 
-MODELS = {"srmhd": 0, "srrmhd": 1}
+MODELS = {"srmhd": 0, "srrmhd": 1, "hybrid": 2}
 BCS = {"outflow": 0, "periodic": 1, "flow": 2}
-INTEGRATORS = {"rk2": 0, "rksplit": 1, "ssp2": 2, "ssp3": 3, "ssp2322": 4}
+INTEGRATORS = {"rk2": 0, "rksplit": 1, "ssp2": 2, "ssp3": 3, "ssp2322": 4, "rksplit2": 5}
 INITS = {"array": 0, "ot": 1, "kh": 2, "khrandom": 3, "briowu": 4, "currentsheet": 5}
 
 
@@ -34,6 +34,7 @@ class RefConfig(C.Structure):
         ("weno", C.c_int), ("bcs", C.c_int), ("integrator", C.c_int),
         ("init", C.c_int), ("init_arg0", C.c_int), ("init_arg1", C.c_int),
         ("functional_sigma", C.c_int), ("sigma_exp", C.c_double), ("extension", C.c_int),
+        ("sigma_crossover", C.c_double), ("sigma_span", C.c_double), ("use_regime", C.c_int),
     ]
 
 
@@ -110,6 +111,9 @@ def make_config(**kw) -> RefConfig:
     c.functional_sigma = 1 if kw.get("functionalSigma", False) else 0
     c.sigma_exp = kw.get("gam", 12.0)
     c.extension = 1 if kw.get("regime", False) else 0
+    c.sigma_crossover = kw.get("sigmaCrossOver", 150.0)
+    c.sigma_span = kw.get("sigmaSpan", 50.0)
+    c.use_regime = 1 if kw.get("useREGIME", True) else 0
     return c
 
 

@@ -30,6 +30,8 @@
 #include "boundaryConds.h"
 #include "RK2.h"
 #include "rkSplit.h"
+#include "rkSplit2ndOrder.h"
+#include "hybrid.h"
 #include "SSP2.h"
 #include "SSP3.h"
 #include "serialEnv.h"
@@ -42,7 +44,7 @@ TimeIntegrator* mref_new_ssp2322(Data* data, Model* model, Bcs* bcs, FluxMethod*
 extern "C" {
 
 typedef struct {
-  int model;       // 0 = SRMHD, 1 = SRRMHD
+  int model;       // 0 = SRMHD, 1 = SRRMHD, 2 = Hybrid
   int nx, ny, nz;
   double xmin, xmax, ymin, ymax, zmin, zmax;
   double endTime, cfl;
@@ -50,7 +52,7 @@ typedef struct {
   double gamma, sigma, cp;
   int weno;        // 3 or 5
   int bcs;         // 0 = Outflow, 1 = Periodic, 2 = Flow
-  int integrator;  // 0 = RK2, 1 = RKSplit, 2 = SSP2, 3 = SSP3, 4 = SSP2322
+  int integrator;  // 0 = RK2, 1 = RKSplit, 2 = SSP2, 3 = SSP3, 4 = SSP2322, 5 = RKSplit2
   int init;        // 0 = caller prims, 1 = OTVortexSingleFluid, 2 = KHInstabilitySingleFluid,
                    // 3 = KHRandomInstabilitySingleFluid, 4 = BrioWuSingleFluid,
                    // 5 = CurrentSheetSingleFluid
@@ -58,6 +60,9 @@ typedef struct {
   int functional_sigma;  // Data::functionalSigma
   double sigma_exp;      // Data::gam
   int extension;         // 0 = none, 1 = REGIME (RKSplit's model extension)
+  double sigma_crossover;  // Hybrid(data, sigmaCrossOver, sigmaSpan, useREGIME)
+  double sigma_span;
+  int use_regime;
 } mref_config;
 
 }  // extern "C"
@@ -116,14 +121,19 @@ void* mref_create(const mref_config* c, const double* prims) {
                        c->zmin, c->zmax, c->endTime, r->env, c->cfl, c->Ng,
                        c->gamma, c->sigma, c->cp, -1.0e4, 1.0e4, 10, 1 << 30,
                        c->functional_sigma != 0, c->sigma_exp);
+    Hybrid* hybrid = nullptr;
     if (c->model == 0) r->model = new SRMHD(r->data);
-    else r->model = new SRRMHD(r->data);
+    else if (c->model == 1) r->model = new SRRMHD(r->data);
+    else
+      r->model = hybrid = new Hybrid(r->data, c->sigma_crossover, c->sigma_span,
+                                     c->use_regime != 0);
     if (c->weno == 3) r->weno = new Weno3(r->data);
     else if (c->weno == 5) r->weno = new Weno5(r->data);
     else if (c->weno == 7) r->weno = new Weno7(r->data);
     else if (c->weno == 9) r->weno = new Weno9(r->data);
     else r->weno = new Weno11(r->data);
     r->flux = new FVS(r->data, r->weno, r->model);
+    if (hybrid) hybrid->setupREGIME(r->flux);  // as Examples/Hybrid/*/main.cc
     if (c->bcs == 0) r->bcs = r->outflow = new Outflow(r->data);
     else if (c->bcs == 1) r->bcs = r->periodic = new Periodic(r->data);
     else r->bcs = r->flow = new Flow(r->data);
@@ -141,6 +151,7 @@ void* mref_create(const mref_config* c, const double* prims) {
       if (c->extension == 1) r->ext = new REGIME(r->data, r->flux);
       r->timeInt = new RKSplit(r->data, r->model, r->bcs, r->flux, r->ext);
     }
+    else if (c->integrator == 5) r->timeInt = new RKSplit2(r->data, r->model, r->bcs, r->flux);
     else if (c->integrator == 3) r->timeInt = new SSP3(r->data, r->model, r->bcs, r->flux);
     else if (c->integrator == 4) r->timeInt = mref_new_ssp2322(r->data, r->model, r->bcs, r->flux);
     else r->timeInt = new SSP2(r->data, r->model, r->bcs, r->flux);
