@@ -156,6 +156,26 @@ class SRRMHD : public Model {
                                   int j = -1, int k = -1) override;
 };
 
+// The Hybrid model (hybrid.h:33-296): SRRMHD's variables, the ideal and
+// resistive models blended by the conductivity (weight 0 below
+// sigmaCrossOver - sigmaSpan, 1 above sigmaCrossOver + sigmaSpan), with the
+// REGIME term on the ideal part when useREGIME.  Runs inside the device step
+// (RK2 or RKSplit2); its single-cell methods are not provided on the host.
+class Hybrid : public Model {
+ public:
+  double sigmaCrossOver = 150, sigmaSpan = 50;
+  bool useREGIME = true;
+  Hybrid();
+  Hybrid(Data* data, double sigmaCrossOver = 150, double sigmaSpan = 50, bool useREGIME = true);
+  int modelId() const override { return MTH_HYBRID; }
+  // The device step builds the REGIME term from the flux method's WENO order.
+  void setupREGIME(FluxMethod* fluxMethod) { (void)fluxMethod; }
+  void sourceTermSingleCell(double* cons, double* prims, double* aux, double* source, int i = -1,
+                            int j = -1, int k = -1) override;
+  void getPrimitiveVarsSingleCell(double* cons, double* prims, double* aux, int i = -1,
+                                  int j = -1, int k = -1) override;
+};
+
 // -------------------------------------------------------------------- WENO
 class WenoBase {
  public:
@@ -288,6 +308,15 @@ class RKSplit : public RK2 {
           ModelExtension* modelExtension = NULL)
       : RK2(data, model, bcs, fluxMethod, modelExtension) {}
   int integratorId() const override { return MTH_RKSPLIT; }
+};
+// Second-order (Strang) split: half source, RK2, half source
+// (rkSplit2ndOrder.h:42-76).
+class RKSplit2 : public RK2 {
+ public:
+  RKSplit2(Data* data, Model* model, Bcs* bcs, FluxMethod* fluxMethod,
+           ModelExtension* modelExtension = NULL)
+      : RK2(data, model, bcs, fluxMethod, modelExtension) {}
+  int integratorId() const override { return MTH_RKSPLIT2; }
 };
 class SSP2 : public TimeIntegrator {
  public:

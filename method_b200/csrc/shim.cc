@@ -108,8 +108,19 @@ mth_handle* Data::gpu() {
   c.weno_order = weno_ ? weno_->order : 3;
   c.bcs = bcs_ ? bcs_->bcId() : MTH_OUTFLOW;
   c.integrator = timeInt_ ? timeInt_->integratorId() : MTH_RK2;
-  if (c.integrator >= MTH_SSP2 && c.model != MTH_SRRMHD)
+  if (c.integrator >= MTH_SSP2 && c.integrator <= MTH_SSP2322 && c.model != MTH_SRRMHD)
     throw std::invalid_argument("the IMEX integrators are provided for the SRRMHD model");
+  if (const Hybrid* hy = dynamic_cast<const Hybrid*>(model_)) {
+    c.sigma_crossover = hy->sigmaCrossOver;
+    c.sigma_span = hy->sigmaSpan;
+    c.regime = hy->useREGIME ? 1 : 0;
+    if (timeInt_ && timeInt_->integratorId() != MTH_RK2 &&
+        timeInt_->integratorId() != MTH_RKSPLIT2)
+      throw std::invalid_argument("the Hybrid model runs with RK2 or RKSplit2");
+  }
+  if (timeInt_ && timeInt_->integratorId() == MTH_RKSPLIT2 && timeInt_->modelExtension &&
+      timeInt_->modelExtension->sourceExists)
+    throw std::invalid_argument("RKSplit2 takes no model extension here");
   if (timeInt_ && timeInt_->integratorId() == MTH_RKSPLIT && timeInt_->modelExtension &&
       timeInt_->modelExtension->sourceExists && timeInt_->modelExtension->extensionId() == 1) {
     if (c.model != MTH_SRMHD || dims == 3)
@@ -154,6 +165,28 @@ SRRMHD::SRRMHD(Data* d) : Model(d) {
                   "Sbarx", "Sbary", "Sbarz", "Sbarsq", "tauBar"};
   d->model_ = this;
   d->invalidateGpu();
+}
+
+Hybrid::Hybrid() : Model() { Ncons = 14; Nprims = 11; Naux = 17; }
+Hybrid::Hybrid(Data* d, double crossOver, double span, bool regime)
+    : Model(d), sigmaCrossOver(crossOver), sigmaSpan(span), useREGIME(regime) {
+  // the same variables and labels as SRRMHD (hybrid.cc:26-77)
+  Ncons = d->Ncons = 14;
+  Nprims = d->Nprims = 11;
+  Naux = d->Naux = 17;
+  d->consLabels = {"D", "Sx", "Sy", "Sz", "tau", "Bx", "By", "Bz", "Ex", "Ey", "Ez", "psi",
+                   "phi", "qch"};
+  d->primsLabels = {"rho", "vx", "vy", "vz", "p", "Bx", "By", "Bz", "Ex", "Ey", "Ez"};
+  d->auxLabels = {"h", "W", "e", "c", "Jx", "Jy", "Jz", "Bsq", "Esq", "vsq", "rhohWsq", "vE",
+                  "Sbarx", "Sbary", "Sbarz", "Sbarsq", "tauBar"};
+  d->model_ = this;
+  d->invalidateGpu();
+}
+void Hybrid::sourceTermSingleCell(double*, double*, double*, double*, int, int, int) {
+  throw std::invalid_argument("Hybrid::sourceTermSingleCell is not provided on the host");
+}
+void Hybrid::getPrimitiveVarsSingleCell(double*, double*, double*, int, int, int) {
+  throw std::invalid_argument("Hybrid::getPrimitiveVarsSingleCell is not provided on the host");
 }
 
 namespace {

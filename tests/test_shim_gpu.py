@@ -123,3 +123,38 @@ def test_regime_driver_matches_reference(tmp_path, ref):
     rs.close()
     assert np.array_equal(cons, rc)
     assert np.array_equal(prims, rp)
+
+
+@pytest.mark.skipif(shutil.which("g++") is None, reason="no host compiler")
+def test_hybrid_driver_matches_reference(tmp_path, ref):
+    """tests/cpp/hybrid_main.cc: Hybrid(&data, 150, 50, true) with
+    setupREGIME and RKSplit2, as the reference's Hybrid examples wire it, on
+    the reference's OTVortexSingleFluid, against the reference CPU build."""
+    exe = tmp_path / "hybrid_main"
+    r = subprocess.run(["g++", "-std=c++11", "-O2", "-I",
+                        os.path.join(ROOT, "include", "method_b200"),
+                        os.path.join(ROOT, "tests", "cpp", "hybrid_main.cc"), "-o", str(exe),
+                        "-L", os.path.join(ROOT, "method_b200"), "-lmethod_b200",
+                        "-Wl,-rpath," + os.path.join(ROOT, "method_b200")],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    out, init = tmp_path / "state.bin", tmp_path / "prims0.bin"
+    r = subprocess.run([str(exe), str(out), str(init)], capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    Nx = Ny = 40
+    data = np.fromfile(out, dtype=np.float64)
+    cons = data[:14 * Nx * Ny].reshape(14, Nx, Ny, 1)
+    prims = data[14 * Nx * Ny:].reshape(11, Nx, Ny, 1)
+    prims0 = np.fromfile(init, dtype=np.float64).reshape(11, Nx, Ny, 1)
+    cfg = dict(model="hybrid", nx=32, ny=32, xmin=0.0, xmax=1.0, ymin=0.0, ymax=1.0,
+               endTime=1.0, cfl=0.3, Ng=4, gamma=2.0, sigma=170.0, cp=1.0, weno=3,
+               bcs="periodic", integrator="rksplit2", sigmaCrossOver=150.0, sigmaSpan=50.0,
+               useREGIME=True)
+    rs = ref.RefSim(init="ot", **cfg)
+    assert np.array_equal(prims0, rs.state()[1])
+    rs.update_time(8)
+    rc, rp, _ = rs.state()
+    rs.close()
+    assert np.array_equal(cons, rc)
+    assert np.array_equal(prims, rp)
