@@ -633,10 +633,69 @@ def cpu_regime(n=512, steps=2):
                                            f"serial build (-O3), {el:.1f} s on the host"}
 
 
-def cpu_legs(initial, sheet, kh, ensemble, regime=None):
+HYBRID_WORKLOAD = ("Hybrid SRMHD/SRRMHD model, Orszag-Tang 2D 1024x1024 periodic, FVS+WENO3, "
+                   "RKSplit2, sigma 170 (blend weight 0.92), sigmaCrossOver 150, sigmaSpan 50, "
+                   "REGIME on the ideal part, CFL 0.3, gamma 2")
+
+
+def hybrid_cfg():
+    return dict(model="hybrid", integrator="rksplit2", xmin=0.0, xmax=1.0, ymin=0.0, ymax=1.0,
+                endTime=1e9, cfl=0.3, Ng=4, gamma=2.0, sigma=170.0, cp=1.0, weno=3,
+                bcs="periodic", sigmaCrossOver=150.0, sigmaSpan=50.0, useREGIME=True)
+
+
+def hybrid_prims(initial, n):
+    p = np.zeros((11, n + 8, n + 8, 1))
+    p[:8] = initial.orszag_tang(n, Ng=4)
+    return p
+
+
+def run_hybrid(mb, initial, torch, ranks, n, K, W):
+    """The Hybrid model (hybrid.cc) under RKSplit2 (rkSplit2ndOrder.cc), plain
+    form (the generic per-direction flux path): device time per step and
+    the per-kernel split of one profiled step."""
+    cfg = hybrid_cfg()
+    dt = 0.3 / n / np.sqrt(2.0)
+    sim = mb.Simulation(nx=n, ny=n, device=ranks.local, **cfg)
+    sim.set_prims(hybrid_prims(initial, n))
+    ms = timed_steps(sim, torch, ranks.local, dt, K, W, ranks.barrier, ranks.max)
+    st = sim.stats()
+    ks = sim.profile_step(dt, reps=2)
+    sim.close()
+    return {"workload": HYBRID_WORKLOAD, "unit": "zone-updates/s", "n": n, "form": "plain FP64",
+            "value": ranks.world * n * n * K / (ms * 1e-3), "ms_per_step": ms / K, "steps": K,
+            "c2p_unconverged": st["c2p_unconverged"],
+            "kernels": [{"name": k["name"], "launches_per_step": k["launches"] / 2.0,
+                         "ms_per_launch": round(k["total_ms"] / k["launches"], 4)} for k in ks]}
+
+
+def cpu_hybrid(n=256, steps=2):
+    """The reference build's serial Hybrid + RKSplit2 step on an n^2 grid."""
+    from method_b200 import initial
+    try:
+        from oracle import ref
+        if not ref.available():
+            raise FileNotFoundError
+        sim = ref.RefSim(prims=hybrid_prims(initial, n), nx=n, ny=n, **hybrid_cfg())
+    except (FileNotFoundError, OSError):
+        return None  # the oracle port has no Hybrid model
+    dt = 0.3 / n / np.sqrt(2.0)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        sim.step_dt(dt)
+    el = time.perf_counter() - t0
+    sim.close()
+    return {"value": n * n * steps / el, "unit": "zone-updates/s", "cores": 1,
+            "kind": "reference", "sample": f"{steps} RKSplit2 steps of the Hybrid model on a "
+                                           f"{n}x{n} grid, serial build (-O3), {el:.1f} s"}
+
+
+def cpu_legs(initial, sheet, kh, ensemble, regime=None, hybrid=None):
     """The reference build's CPU baselines of the side workloads."""
     if regime is not None:
         regime["cpu_baseline"] = cpu_regime()
+    if hybrid is not None:
+        hybrid["cpu_baseline"] = cpu_hybrid()
     if sheet is not None:
         sheet["cpu_baseline"] = cpu_sheet(sheet_cfg(sheet["sigma"]),
                                           initial.current_sheet(*SHEET_N, seed=SHEET_SEED),
@@ -795,6 +854,7 @@ def main():
     ap.add_argument("--no-kh", action="store_true", help="skip the whole KH 64x128 run")
     ap.add_argument("--no-long-l1", action="store_true", help="skip the 500-step L1 check")
     ap.add_argument("--no-regime", action="store_true", help="skip the REGIME RKSplit workload")
+    ap.add_argument("--no-hybrid", action="store_true", help="skip the Hybrid RKSplit2 workload")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
@@ -876,6 +936,9 @@ def main():
         regime = None
         if not args.no_regime:
             regime = run_regime(mb, initial, torch, ranks, n, max(K // 5, 5), max(W, 3), peak)
+        hybrid = None
+        if not args.no_hybrid:
+            hybrid = run_hybrid(mb, initial, torch, ranks, n, max(K // 20, 3), 3)
     clk = clocks.summary()
     if regime is not None:  # what bounds the tile (ncu figures of a 768^2 capture)
         for form, key in (("plain", "regime_tile_fp64"), ("mixed", "regime_tile_mixed")):
@@ -889,7 +952,7 @@ def main():
     long_l1 = None if args.no_long_l1 else long_run_l1(mb, initial, ranks, n)
     if want_cpu:  # reference-build baselines on the host, after the timed GPU work
         with quiet_stdout():
-            cpu_legs(initial, sheet, kh, ensemble, regime)
+            cpu_legs(initial, sheet, kh, ensemble, regime, hybrid)
 
     cells = n * n
     for form in forms:
@@ -989,6 +1052,7 @@ def main():
             "l1_mixed_vs_fp64_500_steps": long_l1,
             "kh64x128_full_run": kh,
             "regime_rksplit": regime,
+            "hybrid_rksplit2": hybrid,
             "sheet_ssp2": sheet,
             "ensemble": ensemble,
             "c2p_batch": c2p_batch,
