@@ -86,7 +86,10 @@ class Simulation:
     Keyword arguments are the reference Data constructor's (nx, ny, nz, xmin ..
     zmax, endTime, cfl, Ng, gamma, sigma, cp) plus ``model``, ``weno``,
     ``bcs``, ``integrator``, ``precision``, ``guess`` and ``regime`` (the
-    REGIME resistive extension of SRMHD under RKSplit, REGIME.cc).
+    REGIME resistive extension of SRMHD under RKSplit, REGIME.cc).  The Hybrid
+    model (``model="hybrid"``, hybrid.cc) takes ``sigmaCrossOver``,
+    ``sigmaSpan`` and ``useREGIME`` and runs with ``integrator="rk2"`` or
+    ``"rksplit2"`` (rkSplit2ndOrder.cc) in the plain form.
     """
 
     def __init__(self, nx, ny, nz=0, **kw):
