@@ -133,7 +133,18 @@ void* mref_create(const mref_config* c, const double* prims) {
     else if (c->weno == 9) r->weno = new Weno9(r->data);
     else r->weno = new Weno11(r->data);
     r->flux = new FVS(r->data, r->weno, r->model);
-    if (hybrid) hybrid->setupREGIME(r->flux);  // as Examples/Hybrid/*/main.cc
+    if (hybrid) {
+      hybrid->setupREGIME(r->flux);  // as Examples/Hybrid/*/main.cc
+      // Hybrid::sourceTerm adds all nine planes of regimeSource (hybrid.cc:
+      // 330-343), but REGIME::sourceExtension never writes its last plane
+      // (REGIME.cc:97-133), so the reference reads memory it did not
+      // initialise.  A fresh process gets that buffer zeroed from the OS; in a
+      // process that has freed earlier simulations the heap may recycle a
+      // used chunk.  Zero it here, which is the fresh-process behaviour.
+      if (c->use_regime)
+        std::memset(hybrid->regimeSource, 0,
+                    sizeof(double) * 9 * r->data->Nx * r->data->Ny * r->data->Nz);
+    }
     if (c->bcs == 0) r->bcs = r->outflow = new Outflow(r->data);
     else if (c->bcs == 1) r->bcs = r->periodic = new Periodic(r->data);
     else r->bcs = r->flow = new Flow(r->data);
