@@ -94,9 +94,9 @@ __global__ void __launch_bounds__(kThreads)
 // taken from cons, then the resistive recovery where the conductivity is
 // below sigmaCrossOver, else SRMHD's single-cell recovery (hybrd1, tol 1.4e-8,
 // srmhd.cc:297-377) of the ideal variables and its conversion back.
-// Registers capped at 64 (8 CTAs of 128 threads per SM), as for the plain
-// SRMHD recovery: the Powell-hybrid solve is latency-bound.
-__global__ void __launch_bounds__(kThreads, 8)
+// (A 64-register cap, as the plain SRMHD recovery has, measured slower
+// here: 0.80 -> 0.85 ms per OT 1024^2 launch.)
+__global__ void __launch_bounds__(kThreads)
     k_hybrid_c2p(Grid g, const double* __restrict__ cons, const double* prims_guess,
                  const double* aux_guess, double* prims, double* aux, C2PWork w) {
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
