@@ -94,8 +94,6 @@ __global__ void __launch_bounds__(kThreads)
 // taken from cons, then the resistive recovery where the conductivity is
 // below sigmaCrossOver, else SRMHD's single-cell recovery (hybrd1, tol 1.4e-8,
 // srmhd.cc:297-377) of the ideal variables and its conversion back.
-// (A 64-register cap, as the plain SRMHD recovery has, measured slower
-// here: 0.80 -> 0.85 ms per OT 1024^2 launch.)
 __global__ void __launch_bounds__(kThreads)
     k_hybrid_c2p(Grid g, const double* __restrict__ cons, const double* prims_guess,
                  const double* aux_guess, double* prims, double* aux, C2PWork w) {
@@ -105,17 +103,25 @@ __global__ void __launch_bounds__(kThreads)
   interior_ijk(g, t, i, j, k);
   const long long N = g.Ntot, cell = cell_id(g, i, j, k);
   double c[14], p[11], a[17];
-  load_cell(g, cons, prims_guess, aux_guess, cell, c, p, a);
+  for (int v = 0; v < 14; ++v) c[v] = cons[v * N + cell];
   for (int v = 5; v < 11; ++v) p[v] = c[v];
   bool ok;
   long long evals = 0;
+  // Each branch reads only the guesses its recovery uses: the secant on Z
+  // its aux[10] (and it writes all of prims and aux), SRMHD's hybrd1 the
+  // velocity, density and enthalpy of the ideal variables, which
+  // Hybrid::setIdealCPAs copies from the resistive prims[0..3] and aux[0].
   if (sigma_of(g, c[0]) < g.sigma_cross) {
+    a[10] = aux_guess[10 * N + cell];
     int ev = 0;
     ok = srrmhd::c2p_cell(c, g.gamma, sigma_of(g, c[0]), p, a, ev);
     evals = ev;
   } else {
     double ic[9], ip[8], ia[13];
-    ideal_cpas(c, p, a, ic, ip, ia);
+    for (int v = 0; v < 8; ++v) ic[v] = c[v];
+    ic[8] = c[12];
+    for (int v = 0; v < 4; ++v) ip[v] = prims_guess[v * N + cell];
+    ia[0] = aux_guess[cell];
     srmhd::Residual R = srmhd::residual_args(ic, g.gamma);
     double x[2], fv[2];
     srmhd::guess_from_prims(ip, ia[0], x);

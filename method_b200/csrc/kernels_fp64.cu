@@ -78,7 +78,8 @@ __global__ void k_split_dir_full(Grid g, const double* __restrict__ cons,
   }
 }
 
-__global__ void k_weno_dir(Grid g, int nc, int order, int dir, const double* __restrict__ fplus,
+template <int ORDER>
+__global__ void k_weno_dir(Grid g, int nc, int dir, const double* __restrict__ fplus,
                            const double* __restrict__ fminus, double* __restrict__ frecon) {
   long long cell = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (cell >= g.Ntot) return;
@@ -86,44 +87,48 @@ __global__ void k_weno_dir(Grid g, int nc, int order, int dir, const double* __r
   long long t = cell / g.Nz;
   int j = (int)(t % g.Ny);
   int i = (int)(t / g.Ny);
-  const int shift = (order + 1) / 2;
+  constexpr int shift = (ORDER + 1) / 2;
   int idx = dir == 0 ? i : (dir == 1 ? j : k);
   int n = dir == 0 ? g.Nx : (dir == 1 ? g.Ny : g.Nz);
   long long stride = dir == 0 ? (long long)g.Ny * g.Nz : (dir == 1 ? g.Nz : 1);
+  const bool inside = idx >= shift && idx < n - shift;
   for (int v = 0; v < nc; ++v) {
     double r = 0.0;  // the reference zero-initialises its reconstruction arrays
-    if (idx >= shift && idx < n - shift) {
+    if (inside) {
       const double* P = fplus + v * g.Ntot + cell;
       const double* Mm = fminus + v * g.Ntot + cell;
       double up, dn;
-      if (order == 3) {
+      if constexpr (ORDER == 3) {
         up = weno3_exact(P[-2 * stride], P[-1 * stride], P[0]);
         dn = weno3_exact(Mm[1 * stride], Mm[0], Mm[-1 * stride]);
-      } else if (order == 5) {
+      } else if constexpr (ORDER == 5) {
         up = weno5_exact(P[-3 * stride], P[-2 * stride], P[-1 * stride], P[0], P[1 * stride]);
         dn = weno5_exact(Mm[2 * stride], Mm[1 * stride], Mm[0], Mm[-1 * stride],
                          Mm[-2 * stride]);
       } else {
         // upwind i-shift .. i-shift+order-1, downwind i+shift-1 .. i+shift-order
         const int s = (int)stride;
-        const double* U = P - shift * stride;
-        const double* Dn = Mm + (shift - 1) * stride;
-        if (order == 7) {
-          up = weno_point<7, double>(U, s);
-          dn = weno_point<7, double>(Dn, -s);
-        } else if (order == 9) {
-          up = weno_point<9, double>(U, s);
-          dn = weno_point<9, double>(Dn, -s);
-        } else {
-          up = weno_point<11, double>(U, s);
-          dn = weno_point<11, double>(Dn, -s);
-        }
+        up = weno_point<ORDER, double>(P - shift * stride, s);
+        dn = weno_point<ORDER, double>(Mm + (shift - 1) * stride, -s);
       }
       r = up + dn;
     } else {
       r = 0.0 + 0.0;
     }
     frecon[v * g.Ntot + cell] = r;
+  }
+}
+
+// k_weno_dir for a runtime order.
+void weno_dir_launch(const Grid& g, int nc, int order, int dir, const double* fplus,
+                     const double* fminus, double* frecon, cudaStream_t st) {
+  const int b = (int)((g.Ntot + kThreads - 1) / kThreads);
+  switch (order) {
+    case 3: k_weno_dir<3><<<b, kThreads, 0, st>>>(g, nc, dir, fplus, fminus, frecon); break;
+    case 5: k_weno_dir<5><<<b, kThreads, 0, st>>>(g, nc, dir, fplus, fminus, frecon); break;
+    case 7: k_weno_dir<7><<<b, kThreads, 0, st>>>(g, nc, dir, fplus, fminus, frecon); break;
+    case 9: k_weno_dir<9><<<b, kThreads, 0, st>>>(g, nc, dir, fplus, fminus, frecon); break;
+    default: k_weno_dir<11><<<b, kThreads, 0, st>>>(g, nc, dir, fplus, fminus, frecon); break;
   }
 }
 
@@ -1032,7 +1037,7 @@ cudaError_t launch_fvs2d_fp64(const Grid& g, int model, int order, const double*
 
 cudaError_t launch_weno_dir(const Grid& g, int nc, int order, int dir, const double* fplus,
                             const double* fminus, double* frecon, cudaStream_t st) {
-  k_weno_dir<<<blocks_for(g.Ntot), kThreads, 0, st>>>(g, nc, order, dir, fplus, fminus, frecon);
+  weno_dir_launch(g, nc, order, dir, fplus, fminus, frecon, st);
   return cudaGetLastError();
 }
 
@@ -1067,8 +1072,7 @@ cudaError_t launch_fvs_generic_raw(const Grid& g, int model, int order, const do
       k_split_dir_full<SRRMHD><<<blocks_for(g.Ntot), kThreads, 0, st>>>(g, cons, prims, aux,
                                                                          dir, fplus, fminus);
     }
-    k_weno_dir<<<blocks_for(g.Ntot), kThreads, 0, st>>>(g, nc, order, dir, fplus, fminus,
-                                                        frecon);
+    weno_dir_launch(g, nc, order, dir, fplus, fminus, frecon, st);
     k_fnet_dir<<<blocks_for(nI), kThreads, 0, st>>>(g, nc, dir, dir == 0, frecon, fnet);
   }
   return cudaGetLastError();
