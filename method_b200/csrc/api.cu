@@ -595,7 +595,7 @@ mth_status mth_create(const mth_config* cfg, mth_handle** out) {
   h->NC = c.model == MTH_SRMHD ? 9 : 14;
   h->NP = c.model == MTH_SRMHD ? 8 : 11;
   h->NA = c.model == MTH_SRMHD ? 13 : 17;
-  h->fused = (g.dims == 2) && c.model != MTH_HYBRID;
+  h->fused = (g.dims == 2) && (c.model != MTH_HYBRID || c.weno_order <= 5);
   h->device = c.device;
 
   auto bail = [&](const char* what, cudaError_t e) {
@@ -630,7 +630,9 @@ mth_status mth_create(const mth_config* cfg, mth_handle** out) {
   if (c.model == MTH_SRMHD && (e = alloc0(&h->solution, bytes(h, 2), h->st)))
     return bail("solution", e);
   if ((e = alloc0(&h->fnet, bytes(h, h->NC), h->st))) return bail("fnet", e);
-  if (!h->fused) {
+  // the generic flux path's arrays; the Hybrid model's primsToAll also uses
+  // fplus / fminus as scratch for the ideal cons and aux (prims_to_all)
+  if (!h->fused || c.model == MTH_HYBRID) {
     for (double** p : {&h->fplus, &h->fminus, &h->frecon})
       if ((e = alloc0(p, bytes(h, h->NC), h->st))) return bail("generic", e);
   }
@@ -702,6 +704,7 @@ cudaError_t prims_to_all(mth_handle* h) {
   cudaError_t e;
   if (h->cfg.model != MTH_HYBRID)
     return launch_prims_to_all(h->g, h->cfg.model, h->prims, h->cons, h->aux, h->st);
+  if (!h->fplus || !h->fminus) return cudaErrorInvalidValue;
   if ((e = launch_prims_to_all(h->g, MTH_SRRMHD, h->prims, h->cons, h->aux, h->st))) return e;
   if ((e = launch_prims_to_all(h->g, MTH_SRMHD, h->prims, h->fplus, h->fminus, h->st))) return e;
   return launch_hybrid_blend(h->g, h->cons, h->prims, h->aux, h->fplus, h->fminus, h->st);

@@ -127,7 +127,7 @@ __device__ __forceinline__ void split_cell(const Grid& g, const double* __restri
   R c[M::NC], p[M::NP], a[M::NA];
   M::template load_flux_inputs<R>(cons, prims, aux, g.Ntot, cell, c, p, a);
   R f[M::NC];
-  M::template flux<R>(c, p, a, dir, f);
+  M::template flux_g<R>(g, c, p, a, dir, f);
 #pragma unroll
   for (int v = 0; v < M::NC; ++v) {
     if constexpr (sizeof(R) == 4) {

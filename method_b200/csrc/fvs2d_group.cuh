@@ -34,7 +34,7 @@ __device__ __forceinline__ void split_group(const Grid& g, const double* __restr
   double c[M::NC], p[M::NP], a[M::NA];
   M::template load_flux_inputs<double, false>(cons, prims, aux, g.Ntot, cell, c, p, a);
   double f[M::NC];
-  M::template flux<double>(c, p, a, dir, f);
+  M::template flux_g<double>(g, c, p, a, dir, f);
 #pragma unroll
   for (int v = 0; v < NV; ++v) {
     sp[v * stride] = 0.5 * (f[V0 + v] + c[V0 + v]);

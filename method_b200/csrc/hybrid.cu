@@ -12,48 +12,13 @@
 #include "minpack.cuh"
 #include "srmhd.cuh"
 #include "srrmhd.cuh"
+#include "hybrid.cuh"
 
 namespace mth {
 namespace {
 
 constexpr int kThreads = 128;
 inline int blocks_for(long long n) { return (int)((n + kThreads - 1) / kThreads); }
-
-// Hybrid::idealWeight (hybrid.cc:115-131): 0 below sigmaCrossOver -
-// sigmaSpan, 1 above sigmaCrossOver + sigmaSpan, a tanh ramp between.
-__device__ __forceinline__ double ideal_weight(const Grid& g, double sig) {
-  return sig < g.sigma_cross - g.sigma_span
-             ? 0
-             : sig < g.sigma_cross + g.sigma_span
-                   ? (tanh((sig - g.sigma_cross) / (g.sigma_span / 3)) + 1) / 2
-                   : 1;
-}
-
-// Hybrid::setIdealCPAs (hybrid.cc:139-168): the SRMHD cons (9), prims (8) and
-// aux (13) of one cell from its resistive cons (14), prims (11) and aux (17).
-__device__ __forceinline__ void ideal_cpas(const double* rc, const double* rp, const double* ra,
-                                           double* c, double* p, double* a) {
-  for (int v = 0; v < 8; ++v) c[v] = rc[v];
-  c[8] = rc[12];
-  for (int v = 0; v < 8; ++v) p[v] = rp[v];
-  for (int v = 0; v < 4; ++v) a[v] = ra[v];
-  const double b0 = ra[1] * (rp[5] * rp[1] + rp[6] * rp[2] + rp[7] * rp[3]);
-  const double bx = rp[5] / ra[1] + b0 * rp[1];
-  const double by = rp[6] / ra[1] + b0 * rp[2];
-  const double bz = rp[7] / ra[1] + b0 * rp[3];
-  const double bsq = (rp[5] * rp[5] + rp[6] * rp[6] + rp[7] * rp[7] + b0 * b0) / (ra[1] * ra[1]);
-  const double BS = ra[1] * (rp[5] * rc[1] + rp[6] * rc[2] + rp[7] * rc[3]);
-  const double Ssq = rc[1] * rc[1] + rc[2] * rc[2] + rc[3] * rc[3];
-  a[4] = b0;
-  a[5] = bx;
-  a[6] = by;
-  a[7] = bz;
-  a[8] = bsq;
-  a[9] = ra[9];
-  a[10] = BS;
-  a[11] = ra[7];
-  a[12] = Ssq;
-}
 
 __device__ __forceinline__ void load_cell(const Grid& g, const double* cons, const double* prims,
                                           const double* aux, long long cell, double* c, double* p,
@@ -75,14 +40,8 @@ __global__ void __launch_bounds__(kThreads)
   if (cell >= g.Ntot) return;
   double c[14], p[11], a[17];
   load_cell(g, cons, prims, aux, cell, c, p, a);
-  const double iW = ideal_weight(g, sigma_of(g, c[0]));
-  double ic[9], ip[8], ia[13], fi[9], f[14];
-  ideal_cpas(c, p, a, ic, ip, ia);
-  srmhd::flux<double>(ic, ip, ia, dir, fi);
-  srrmhd::flux<double>(c, p, a, dir, f);
-  for (int v = 0; v < 14; ++v) f[v] = (1 - iW) * f[v];
-  for (int v = 0; v < 8; ++v) f[v] += iW * fi[v];
-  f[12] += iW * fi[8];
+  double f[14];
+  hybrid_flux(g, c, p, a, dir, f);
   const long long N = g.Ntot;
   for (int v = 0; v < 14; ++v) {
     fplus[v * N + cell] = 0.5 * (f[v] + 1.0 * c[v]);

@@ -10,6 +10,7 @@
 #include "ensemble.h"
 #include "fvs2d.cuh"
 #include "fvs2d_group.cuh"
+#include "hybrid.cuh"
 #include "launch.h"
 #include "minpack.cuh"
 #include "srmhd.cuh"
@@ -1024,6 +1025,11 @@ cudaError_t launch_fvs2d_fp64(const Grid& g, int model, int order, const double*
       case 9: FVS64(SRMHD, 9);
       default: FVS64(SRMHD, 11);
     }
+  }
+  if (model == MODEL_HYBRID) {  // WENO3 / WENO5; higher orders take the generic path
+    if (order == 3) FVS64(HYBRID, 3);
+    if (order == 5) FVS64(HYBRID, 5);
+    return cudaErrorInvalidValue;
   }
   switch (order) {
     case 3: FVS64(SRRMHD, 3);

@@ -221,6 +221,13 @@ struct SRMHD {
   __device__ __forceinline__ static void flux(const R* c, const R* p, const R* a, int dir, R* f) {
     srmhd::flux<R>(c, p, a, dir, f);
   }
+  // The fused tiles' form, which also passes the grid (the Hybrid model's
+  // flux depends on the conductivity parameters).
+  template <typename R>
+  __device__ __forceinline__ static void flux_g(const Grid&, const R* c, const R* p, const R* a,
+                                                int dir, R* f) {
+    srmhd::flux<R>(c, p, a, dir, f);
+  }
   // Model::sourceTerm of one cell in FP64 (srmhd.cc:215-250): S_phi = -phi/cp^2.
   __device__ __forceinline__ static void cell_source(const double* __restrict__ cons,
                                                      const double*, long long N, long long cell,

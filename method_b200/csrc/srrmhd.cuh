@@ -271,6 +271,13 @@ struct SRRMHD {
   __device__ __forceinline__ static void flux(const R* c, const R* p, const R* a, int dir, R* f) {
     srrmhd::flux<R>(c, p, a, dir, f);
   }
+  // The fused tiles' form, which also passes the grid (the Hybrid model's
+  // flux depends on the conductivity parameters).
+  template <typename R>
+  __device__ __forceinline__ static void flux_g(const Grid&, const R* c, const R* p, const R* a,
+                                                int dir, R* f) {
+    srrmhd::flux<R>(c, p, a, dir, f);
+  }
   // Model::sourceTerm of one cell in FP64 (srrmhd.cc:194-206): reads cons
   // 11-13 and aux 4-6 only.
   __device__ __forceinline__ static void cell_source(const double* __restrict__ cons,
