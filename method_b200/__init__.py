@@ -89,7 +89,7 @@ class Simulation:
     REGIME resistive extension of SRMHD under RKSplit, REGIME.cc).  The Hybrid
     model (``model="hybrid"``, hybrid.cc) takes ``sigmaCrossOver``,
     ``sigmaSpan`` and ``useREGIME`` and runs with ``integrator="rk2"`` or
-    ``"rksplit2"`` (rkSplit2ndOrder.cc) in the plain form.
+    ``"rksplit2"`` (rkSplit2ndOrder.cc), plain or mixed.
     """
 
     def __init__(self, nx, ny, nz=0, **kw):

@@ -132,6 +132,8 @@ cudaError_t alloc0(double** p, size_t n, cudaStream_t st) {
 // recovery writes their inputs alone.
 cudaError_t c2p_raw(mth_handle* h, const double* cons, const double* pg, const double* ag,
                 double* prims, double* aux, bool lean) {
+  if (h->cfg.model == MTH_HYBRID && h->cfg.precision == MTH_MIXED)
+    return launch_c2p_hybrid_mixed(h->g, cons, pg, ag, prims, aux, c2p_work(h), h->st);
   if (h->cfg.precision == MTH_MIXED || h->cfg.guess == MTH_GUESS_MLP)
     return launch_c2p_mixed(h->g, h->cfg.model, h->cfg.guess, cons, pg, ag, prims, aux,
                             h->solution, c2p_work(h), h->mixed, lean && h->fused, h->st);
@@ -580,9 +582,9 @@ mth_status mth_create(const mth_config* cfg, mth_handle** out) {
        c.integrator != MTH_SSP2) ||
       (c.regime && c.model != MTH_HYBRID &&
        (c.model != MTH_SRMHD || c.integrator != MTH_RKSPLIT || c.nz != 0 || c.x_slab)) ||
-      // the Hybrid model: plain form, RK2 or RKSplit2, previous-state guesses
+      // the Hybrid model: RK2 or RKSplit2, previous-state guesses
       (c.model == MTH_HYBRID &&
-       (c.precision != MTH_PLAIN_FP64 || c.guess != 0 || c.x_slab || !(c.sigma_span > 0) ||
+       (c.guess != 0 || c.x_slab || !(c.sigma_span > 0) ||
         (c.integrator != MTH_RK2 && c.integrator != MTH_RKSPLIT2)))) {
     delete h;
     return MTH_ERR_INVALID;

@@ -41,7 +41,7 @@ __global__ void __launch_bounds__(kThreads)
   double c[14], p[11], a[17];
   load_cell(g, cons, prims, aux, cell, c, p, a);
   double f[14];
-  hybrid_flux(g, c, p, a, dir, f);
+  hybrid_flux<double>(g, c, p, a, dir, f);
   const long long N = g.Ntot;
   for (int v = 0; v < 14; ++v) {
     fplus[v * N + cell] = 0.5 * (f[v] + 1.0 * c[v]);
@@ -149,7 +149,7 @@ __global__ void __launch_bounds__(kThreads)
   load_cell(g, cons, prims, aux, cell, c, p, a);
   const double iW = ideal_weight(g, sigma_of(g, c[0]));
   double ic[9], ip[8], ia[13], is[9], rs[14];
-  ideal_cpas(c, p, a, ic, ip, ia);
+  ideal_cpas<double>(c, p, a, ic, ip, ia);
   srrmhd::source(c, a, g.cp, rs);
   srmhd::source(ic, g.cp, is);
   for (int v = 0; v < 8; ++v) src[v * N + cell] = iW * is[v] + (1 - iW) * rs[v];
@@ -260,6 +260,11 @@ cudaError_t launch_c2p_hybrid(const Grid& g, const double* cons, const double* p
   if (e != cudaSuccess) return e;
   k_hybrid_finalise<<<blocks_for(n_interior_host(g)), kThreads, 0, st>>>(g, const_cast<double*>(cons),
                                                                          prims);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_hybrid_finalise(const Grid& g, double* cons, double* prims, cudaStream_t st) {
+  k_hybrid_finalise<<<blocks_for(n_interior_host(g)), kThreads, 0, st>>>(g, cons, prims);
   return cudaGetLastError();
 }
 

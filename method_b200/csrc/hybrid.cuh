@@ -20,19 +20,20 @@ __device__ __forceinline__ double ideal_weight(const Grid& g, double sig) {
 
 // Hybrid::setIdealCPAs (hybrid.cc:139-168): the SRMHD cons (9), prims (8) and
 // aux (13) of one cell from its resistive cons (14), prims (11) and aux (17).
-__device__ __forceinline__ void ideal_cpas(const double* rc, const double* rp, const double* ra,
-                                           double* c, double* p, double* a) {
+template <typename R>
+__device__ __forceinline__ void ideal_cpas(const R* rc, const R* rp, const R* ra, R* c, R* p,
+                                           R* a) {
   for (int v = 0; v < 8; ++v) c[v] = rc[v];
   c[8] = rc[12];
   for (int v = 0; v < 8; ++v) p[v] = rp[v];
   for (int v = 0; v < 4; ++v) a[v] = ra[v];
-  const double b0 = ra[1] * (rp[5] * rp[1] + rp[6] * rp[2] + rp[7] * rp[3]);
-  const double bx = rp[5] / ra[1] + b0 * rp[1];
-  const double by = rp[6] / ra[1] + b0 * rp[2];
-  const double bz = rp[7] / ra[1] + b0 * rp[3];
-  const double bsq = (rp[5] * rp[5] + rp[6] * rp[6] + rp[7] * rp[7] + b0 * b0) / (ra[1] * ra[1]);
-  const double BS = ra[1] * (rp[5] * rc[1] + rp[6] * rc[2] + rp[7] * rc[3]);
-  const double Ssq = rc[1] * rc[1] + rc[2] * rc[2] + rc[3] * rc[3];
+  const R b0 = ra[1] * (rp[5] * rp[1] + rp[6] * rp[2] + rp[7] * rp[3]);
+  const R bx = rp[5] / ra[1] + b0 * rp[1];
+  const R by = rp[6] / ra[1] + b0 * rp[2];
+  const R bz = rp[7] / ra[1] + b0 * rp[3];
+  const R bsq = (rp[5] * rp[5] + rp[6] * rp[6] + rp[7] * rp[7] + b0 * b0) / (ra[1] * ra[1]);
+  const R BS = ra[1] * (rp[5] * rc[1] + rp[6] * rc[2] + rp[7] * rc[3]);
+  const R Ssq = rc[1] * rc[1] + rc[2] * rc[2] + rc[3] * rc[3];
   a[4] = b0;
   a[5] = bx;
   a[6] = by;
@@ -46,20 +47,21 @@ __device__ __forceinline__ void ideal_cpas(const double* rc, const double* rp, c
 
 // Hybrid::fluxVector of one cell (hybrid.cc:210-259): f = (1 - w) f_resistive,
 // then + w f_ideal on D, S, tau, B and + w f_ideal(phi) on phi.
-__device__ __forceinline__ void hybrid_flux(const Grid& g, const double* c, const double* p,
-                                            const double* a, int dir, double* f) {
-  const double iW = ideal_weight(g, sigma_of(g, c[0]));
-  double ic[9], ip[8], ia[13], fi[9];
-  ideal_cpas(c, p, a, ic, ip, ia);
-  srmhd::flux<double>(ic, ip, ia, dir, fi);
-  srrmhd::flux<double>(c, p, a, dir, f);
+// R = float: the mixed form's flux (the weight from the FP64 conductivity).
+template <typename R>
+__device__ __forceinline__ void hybrid_flux(const Grid& g, const R* c, const R* p, const R* a,
+                                            int dir, R* f) {
+  const R iW = R(ideal_weight(g, sigma_of(g, double(c[0]))));
+  R ic[9], ip[8], ia[13], fi[9];
+  ideal_cpas<R>(c, p, a, ic, ip, ia);
+  srmhd::flux<R>(ic, ip, ia, dir, fi);
+  srrmhd::flux<R>(c, p, a, dir, f);
   for (int v = 0; v < 14; ++v) f[v] = (1 - iW) * f[v];
   for (int v = 0; v < 8; ++v) f[v] += iW * fi[v];
   f[12] += iW * fi[8];
 }
 
-// The model interface of the fused flux tiles (fvs2d.cuh, fvs2d_group.cuh),
-// plain form only.
+// The model interface of the fused flux tiles (fvs2d.cuh, fvs2d_group.cuh).
 struct HYBRID {
   static constexpr int NC = 14, NP = 11, NA = 17;
   template <typename R, bool LDG = true>
@@ -78,8 +80,7 @@ struct HYBRID {
   template <typename R>
   __device__ __forceinline__ static void flux_g(const Grid& g, const R* c, const R* p, const R* a,
                                                 int dir, R* f) {
-    static_assert(sizeof(R) == sizeof(double), "the Hybrid model has the plain form only");
-    hybrid_flux(g, c, p, a, dir, f);
+    hybrid_flux<R>(g, c, p, a, dir, f);
   }
   // The SSP2 closing stage does not run with this model (RK2 and RKSplit2
   // only); the tile's stage epilogue still names a cell source.

@@ -19,6 +19,7 @@
 #include "common.cuh"
 #include "ensemble.h"
 #include "fvs2d.cuh"
+#include "hybrid.cuh"
 #include "launch.h"
 #include "minpack.cuh"
 #include "mixed.h"
@@ -389,6 +390,83 @@ __device__ __forceinline__ void c2p_srrmhd_newton_cell(const Grid& g, long long 
 #pragma unroll
     for (int v = 0; v < 17; ++v) aux[v * N + cell] = a[v];
   }
+}
+
+// Mixed-form recovery of the Hybrid model (hybrid.cc:354-436): SRRMHD's
+// Newton recovery where the conductivity is below sigmaCrossOver, else
+// SRMHD's Newton recovery of the ideal variables (Powell-hybrid fallback)
+// started from the previous velocity and enthalpy, converted back to the
+// resistive prims and aux as Hybrid::getPrimitiveVarsSingleCell does.  A
+// cell neither solver recovers raises ERR_C2P (the reference throws).
+__global__ void __launch_bounds__(128)
+    k_c2p_newton_hybrid(Grid g, const double* __restrict__ cons, const double* prims_guess,
+                        const double* aux_guess, double* prims, double* aux, C2PWork w) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const bool active = t < n_interior(g);
+  NewtonTally tl;
+  if (active) {
+    int i, j, k;
+    interior_ijk(g, t, i, j, k);
+    const long long N = g.Ntot, cell = cell_id(g, i, j, k);
+    const double D = cons[cell];
+    if (sigma_of(g, D) < g.sigma_cross) {
+      c2p_srrmhd_newton_cell<false>(g, cell, cons, aux_guess, prims, aux, tl, w.counters);
+    } else {
+      double c[14];
+#pragma unroll
+      for (int v = 0; v < 14; ++v) c[v] = cons[v * N + cell];
+      double ic[9];
+#pragma unroll
+      for (int v = 0; v < 8; ++v) ic[v] = c[v];
+      ic[8] = c[12];
+      srmhd::Residual R = srmhd::residual_args(ic, g.gamma);
+      const double BS2 = R.BS * R.BS;
+      double pg[4];
+#pragma unroll
+      for (int v = 0; v < 4; ++v) pg[v] = prims_guess[v * N + cell];
+      double prev[2];
+      srmhd::guess_from_prims(pg, aux_guess[cell], prev);
+      double Z = prev[1], vsq = prev[0];
+      int it = 0;
+      bool ok = newton_srmhd(R.D, R.tau, BS2, R.Bsq, R.Ssq, g.gamma, Z, vsq, it);
+      double x[2] = {vsq, Z};
+      if (!ok) {
+        tl.fb_hybrd += 1;
+        const HybrdOut res = hybrd2_fallback(R, prev[0], prev[1]);
+        x[0] = res.x0;
+        x[1] = res.x1;
+        it += res.nfev;
+        ok = res.info == 1;
+      }
+      tl.its += it;
+      if (!ok) {
+        tl.bad += 1;
+        atomicOr((unsigned long long*)&w.counters[3], (unsigned long long)ERR_C2P);
+      } else {
+        double ip[8], ia[13], p[11], a[17];
+        from_solution_fast(ic, x, g.gamma, R.BS, R.Bsq, R.Ssq, ip, ia);
+#pragma unroll
+        for (int v = 0; v < 8; ++v) p[v] = ip[v];
+        p[8] = c[8]; p[9] = c[9]; p[10] = c[10];
+        a[0] = ia[0]; a[1] = ia[1]; a[2] = ia[2]; a[3] = ia[3];
+        a[4] = 0; a[5] = 0; a[6] = 0; a[7] = ia[11];
+        a[8] = c[8] * c[8] + c[9] * c[9] + c[10] * c[10];
+        a[9] = ia[9];
+        a[10] = p[0] * a[0] * a[1] * a[1];
+        a[11] = p[1] * c[8] + p[2] * c[9] + p[3] * c[10];
+        a[12] = a[10] * p[1];
+        a[13] = a[10] * p[2];
+        a[14] = a[10] * p[3];
+        a[15] = a[12] * a[12] + a[13] * a[13] + a[14] * a[14];
+        a[16] = a[10] - p[4] - c[0];
+#pragma unroll
+        for (int v = 0; v < 11; ++v) prims[v * N + cell] = p[v];
+#pragma unroll
+        for (int v = 0; v < 17; ++v) aux[v * N + cell] = a[v];
+      }
+    }
+  }
+  tally_flush(tl, active, w.counters);
 }
 
 template <bool LEAN>
@@ -916,6 +994,11 @@ cudaError_t launch_fvs2d_fp32(const Grid& g, int model, int order, const double*
       default: FVS32(SRMHD, 11);
     }
   }
+  if (model == MODEL_HYBRID) {  // WENO3 / WENO5; higher orders take the generic path
+    if (order == 3) FVS32(HYBRID, 3);
+    if (order == 5) FVS32(HYBRID, 5);
+    return cudaErrorInvalidValue;
+  }
   switch (order) {
     case 3: FVS32(SRRMHD, 3);
     case 5: FVS32(SRRMHD, 5);
@@ -972,6 +1055,17 @@ cudaError_t launch_c2p_mixed(const Grid& g, int model, int guess, const double* 
                                                          zseed, t0, t_end);
   }
   return cudaGetLastError();
+}
+
+cudaError_t launch_c2p_hybrid_mixed(const Grid& g, const double* cons, const double* prims_guess,
+                                    const double* aux_guess, double* prims, double* aux,
+                                    C2PWork w, cudaStream_t st) {
+  const long long nI = n_interior_host(g);
+  k_c2p_newton_hybrid<<<(int)((nI + 127) / 128), 128, 0, st>>>(g, cons, prims_guess, aux_guess,
+                                                               prims, aux, w);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  return launch_hybrid_finalise(g, const_cast<double*>(cons), prims, st);
 }
 
 cudaError_t launch_imex_fast(const Grid& g, int stage, const double* cons,

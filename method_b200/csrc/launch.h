@@ -67,6 +67,12 @@ cudaError_t launch_hybrid_split(const Grid& g, const double* cons, const double*
 cudaError_t launch_c2p_hybrid(const Grid& g, const double* cons, const double* prims_guess,
                               const double* aux_guess, double* prims, double* aux, C2PWork w,
                               cudaStream_t st);
+// Hybrid::finalise on interior cells; the mixed-form recovery (FP64 Newton
+// in both branches, kernels_mixed.cu) followed by it.
+cudaError_t launch_hybrid_finalise(const Grid& g, double* cons, double* prims, cudaStream_t st);
+cudaError_t launch_c2p_hybrid_mixed(const Grid& g, const double* cons, const double* prims_guess,
+                                    const double* aux_guess, double* prims, double* aux,
+                                    C2PWork w, cudaStream_t st);
 cudaError_t launch_hybrid_source(const Grid& g, int order, const double* cons,
                                  const double* prims, const double* aux, double* src,
                                  const RegimeWork* regime, double* ext, cudaStream_t st);

@@ -88,11 +88,11 @@ def test_regime_configuration_rules():
 
 
 def test_hybrid_configuration_rules():
-    """The Hybrid model runs in the plain form with RK2 or RKSplit2 and a
+    """The Hybrid model runs with RK2 or RKSplit2, previous-state guesses and a
     positive blend width; other combinations are rejected on the host."""
     import method_b200 as mb
     base = dict(nx=16, ny=16, Ng=4, weno=3, bcs="periodic", model="hybrid")
-    for bad in (dict(integrator="rksplit2", precision="mixed"), dict(integrator="ssp2"),
+    for bad in (dict(integrator="ssp2"),
                 dict(integrator="rksplit"), dict(integrator="rk2", sigmaSpan=0.0),
                 dict(integrator="rk2", guess="mlp")):
         with pytest.raises(ValueError):

@@ -127,3 +127,33 @@ def test_current_sheet_recovery_failure_matches(ref):
     else:
         g.update_time(1)
     g.close()
+
+
+@pytest.mark.parametrize("case", ["ot2d", "briowu1d"])
+def test_mixed_form_against_plain(case):
+    """The mixed form (FP32 flux tile in 2D; Newton recoveries in both
+    branches) stays within 1e-6 (L1, relative) of the plain form."""
+    import method_b200 as mb
+    if case == "ot2d":
+        cfg = dict(model="hybrid", integrator="rksplit2", nx=64, ny=64, xmin=0.0, xmax=1.0,
+                   ymin=0.0, ymax=1.0, endTime=1.0, cfl=0.3, Ng=4, gamma=2.0, sigma=170.0,
+                   cp=1.0, weno=5, bcs="periodic", sigmaCrossOver=150.0, sigmaSpan=50.0)
+        p0 = np.zeros((11, 72, 72, 1))
+        p0[:8] = initial.orszag_tang(64, Ng=4)
+    else:
+        cfg = dict(BRIOWU)
+        p0 = np.zeros((11, 408, 1, 1))
+        p0[0] = np.where(np.arange(408) < 204, 1.0, 0.125)[:, None, None]
+        p0[4] = np.where(np.arange(408) < 204, 1.0, 0.1)[:, None, None]
+        p0[5] = 0.75
+        p0[6] = np.where(np.arange(408) < 204, 1.0, -1.0)[:, None, None]
+    out = {}
+    for prec in ("fp64", "mixed"):
+        s = mb.Simulation(precision=prec, **cfg)
+        s.set_prims(p0)
+        s.update_time(20)
+        out[prec] = s.state()[0][:, 4:-4]
+        s.close()
+    l1 = np.abs(out["mixed"] - out["fp64"]).sum() / np.abs(out["fp64"]).sum()
+    assert np.all(np.isfinite(out["mixed"]))
+    assert l1 < 1e-6, l1
