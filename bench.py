@@ -652,21 +652,24 @@ def hybrid_prims(initial, n):
 
 def run_hybrid(mb, initial, torch, ranks, n, K, W):
     """The Hybrid model (hybrid.cc) under RKSplit2 (rkSplit2ndOrder.cc), plain
-    form (the generic per-direction flux path): device time per step and
-    the per-kernel split of one profiled step."""
+    and mixed forms: device time per step and the per-kernel split of one
+    profiled step."""
     cfg = hybrid_cfg()
     dt = 0.3 / n / np.sqrt(2.0)
-    sim = mb.Simulation(nx=n, ny=n, device=ranks.local, **cfg)
-    sim.set_prims(hybrid_prims(initial, n))
-    ms = timed_steps(sim, torch, ranks.local, dt, K, W, ranks.barrier, ranks.max)
-    st = sim.stats()
-    ks = sim.profile_step(dt, reps=2)
-    sim.close()
-    return {"workload": HYBRID_WORKLOAD, "unit": "zone-updates/s", "n": n, "form": "plain FP64",
+    res = {"workload": HYBRID_WORKLOAD, "unit": "zone-updates/s", "n": n}
+    for form, prec in (("plain", "fp64"), ("mixed", "mixed")):
+        sim = mb.Simulation(nx=n, ny=n, device=ranks.local, precision=prec, **cfg)
+        sim.set_prims(hybrid_prims(initial, n))
+        ms = timed_steps(sim, torch, ranks.local, dt, K, W, ranks.barrier, ranks.max)
+        st = sim.stats()
+        ks = sim.profile_step(dt, reps=2)
+        sim.close()
+        res[form] = {
             "value": ranks.world * n * n * K / (ms * 1e-3), "ms_per_step": ms / K, "steps": K,
             "c2p_unconverged": st["c2p_unconverged"],
             "kernels": [{"name": k["name"], "launches_per_step": k["launches"] / 2.0,
                          "ms_per_launch": round(k["total_ms"] / k["launches"], 4)} for k in ks]}
+    return res
 
 
 def cpu_hybrid(n=256, steps=2):
