@@ -288,7 +288,7 @@ cudaError_t rksplit2_half_source(mth_handle* h, double dt) {
          if (h->cfg.model == MTH_HYBRID)
            return launch_hybrid_source(h->g, h->cfg.weno_order, h->cons, h->prims, h->aux,
                                        h->hsrc, h->cfg.regime ? &h->regime : nullptr, h->hext,
-                                       h->st);
+                                       h->cfg.precision == MTH_MIXED, h->st);
          return launch_source(h->g, h->cfg.model, h->cons, h->aux, h->hsrc, h->st);
        })))
     return e;

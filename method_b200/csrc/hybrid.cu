@@ -270,12 +270,14 @@ cudaError_t launch_hybrid_finalise(const Grid& g, double* cons, double* prims, c
 
 cudaError_t launch_hybrid_source(const Grid& g, int order, const double* cons,
                                  const double* prims, const double* aux, double* src,
-                                 const RegimeWork* regime, double* ext, cudaStream_t st) {
+                                 const RegimeWork* regime, double* ext, bool mixed,
+                                 cudaStream_t st) {
   const long long nI = n_interior_host(g);
   k_hybrid_source<<<blocks_for(nI), kThreads, 0, st>>>(g, cons, prims, aux, src);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess || !regime) return e;
-  if ((e = launch_regime_ext(g, order, cons, prims, *regime, ext, st)) != cudaSuccess) return e;
+  if ((e = launch_regime_ext(g, order, cons, prims, *regime, ext, mixed, st)) != cudaSuccess)
+    return e;
   k_hybrid_regime_add<<<blocks_for(nI), kThreads, 0, st>>>(g, cons, ext, src);
   return cudaGetLastError();
 }

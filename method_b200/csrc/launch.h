@@ -54,9 +54,10 @@ cudaError_t launch_regime_source_add(const Grid& g, int order, const double* con
                                      const double* prims, double* target, double dt,
                                      const RegimeWork& w, bool mixed, cudaStream_t st);
 // REGIME::sourceExtension alone into ext (9 planes, interior cells): the
-// Hybrid model's REGIME term (hybrid.cc:320-345).
+// Hybrid model's REGIME term (hybrid.cc:320-345); the fused tile where it
+// applies (FP32 stiff-flux WENO when `mixed`), else the per-array chain.
 cudaError_t launch_regime_ext(const Grid& g, int order, const double* cons, const double* prims,
-                              const RegimeWork& w, double* ext, cudaStream_t st);
+                              const RegimeWork& w, double* ext, bool mixed, cudaStream_t st);
 // The Hybrid model (hybrid.cu): flux + split along dir of every cell; the
 // recovery of interior cells followed by Hybrid::finalise (which updates
 // cons' E); the source of interior cells (+ REGIME when `regime`, into ext
@@ -75,7 +76,8 @@ cudaError_t launch_c2p_hybrid_mixed(const Grid& g, const double* cons, const dou
                                     C2PWork w, cudaStream_t st);
 cudaError_t launch_hybrid_source(const Grid& g, int order, const double* cons,
                                  const double* prims, const double* aux, double* src,
-                                 const RegimeWork* regime, double* ext, cudaStream_t st);
+                                 const RegimeWork* regime, double* ext, bool mixed,
+                                 cudaStream_t st);
 cudaError_t launch_hybrid_blend(const Grid& g, double* cons, double* prims, double* aux,
                                 const double* icons, const double* iaux, cudaStream_t st);
 // cons += h src on interior cells.
@@ -84,7 +86,7 @@ cudaError_t launch_add_scaled(const Grid& g, int nc, double* cons, const double*
 // The fused 2D tile with FP32 stiff-flux reconstruction (regime_mixed.cu).
 cudaError_t launch_regime_tile_mixed(const Grid& g, int order, const double* cons,
                                      const double* prims, double* target, double dt,
-                                     cudaStream_t st);
+                                     cudaStream_t st, bool ext_only = false);
 // Whether the fused tile serves the grid: two dimensions and a constant
 // conductivity (with functionalSigma a halo cell's sigma would read cons[0]
 // that a neighbouring CTA updates in place).

@@ -211,7 +211,11 @@ cudaError_t launch_regime_source_add(const Grid& g, int order, const double* con
 }
 
 cudaError_t launch_regime_ext(const Grid& g, int order, const double* cons, const double* prims,
-                              const RegimeWork& w, double* ext, cudaStream_t st) {
+                              const RegimeWork& w, double* ext, bool mixed, cudaStream_t st) {
+  if (regime_tile_applies(g)) {
+    if (mixed) return launch_regime_tile_mixed(g, order, cons, prims, ext, 0.0, st, true);
+    return launch_regime_tile_order<double>(g, order, cons, prims, ext, 0.0, st, true);
+  }
   cudaError_t e = regime_chain(g, order, cons, prims, w, st);
   if (e != cudaSuccess) return e;
   k_regime_ext<<<blocks_for(n_interior_host(g)), kThreads, 0, st>>>(g, w.DX, w.DY, ext);

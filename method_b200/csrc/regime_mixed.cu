@@ -10,8 +10,8 @@ namespace mth {
 
 cudaError_t launch_regime_tile_mixed(const Grid& g, int order, const double* cons,
                                      const double* prims, double* target, double dt,
-                                     cudaStream_t st) {
-  return launch_regime_tile_order<float>(g, order, cons, prims, target, dt, st);
+                                     cudaStream_t st, bool ext_only) {
+  return launch_regime_tile_order<float>(g, order, cons, prims, target, dt, st, ext_only);
 }
 
 }  // namespace mth

@@ -210,7 +210,7 @@ __device__ __forceinline__ long long clamped_cell(const Grid& g, int i, int j) {
 template <int ORDER, typename R>
 __global__ void __launch_bounds__(RegimeTile<ORDER, R>::NT, RegimeTile<ORDER, R>::MINB)
     k_regime_tile(Grid g, const double* __restrict__ cons, const double* __restrict__ prims,
-                  double* target, double dt) {
+                  double* target, double dt, bool ext_only) {
   using T = RegimeTile<ORDER, R>;
   constexpr int S = T::S, TJ = T::TJ, NT = T::NT, R1J = T::R1J, EJ = T::EJ;
   extern __shared__ __align__(16) unsigned char sh_raw[];
@@ -352,10 +352,15 @@ __global__ void __launch_bounds__(RegimeTile<ORDER, R>::NT, RegimeTile<ORDER, R>
   if (i >= g.ie || j >= g.je) return;
   const long long cell = (long long)i * g.Ny + j;
   const int e = (ty + 1) * R1J + tx + 1;
-  double cv[9], s[9];
+  // ext_only: the extension's source alone into target (REGIME::sourceExtension,
+  // phi's entry 0), as the Hybrid model's source reads it
+  double s[9];
+  if (!ext_only) {
+    double cv[9];
 #pragma unroll
-  for (int v = 0; v < 9; ++v) cv[v] = cons[v * N + cell];
-  srmhd::source(cv, g.cp, s);
+    for (int v = 0; v < 9; ++v) cv[v] = cons[v * N + cell];
+    srmhd::source(cv, g.cp, s);
+  }
 #pragma unroll
   for (int v = 0; v < 9; ++v) {
     double ext = 0.0;
@@ -369,34 +374,38 @@ __global__ void __launch_bounds__(RegimeTile<ORDER, R>::NT, RegimeTile<ORDER, R>
         ext = ddx * i2dx + ddy * i2dy;
       }
     }
-    const double src = s[v] + ext;
-    target[v * N + cell] = target[v * N + cell] + dt * src;
+    if (ext_only) {
+      target[v * N + cell] = ext;
+    } else {
+      const double src = s[v] + ext;
+      target[v * N + cell] = target[v * N + cell] + dt * src;
+    }
   }
 }
 
 template <int ORDER, typename R>
 cudaError_t launch_regime_tile(const Grid& g, const double* cons, const double* prims,
-                               double* target, double dt, cudaStream_t st) {
+                               double* target, double dt, bool ext_only, cudaStream_t st) {
   using T = RegimeTile<ORDER, R>;
   auto kern = k_regime_tile<ORDER, R>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)T::bytes);
   if (e != cudaSuccess) return e;
   const dim3 grid((g.je - g.js + T::TJ - 1) / T::TJ, (g.ie - g.is + T::TI - 1) / T::TI);
-  kern<<<grid, T::NT, T::bytes, st>>>(g, cons, prims, target, dt);
+  kern<<<grid, T::NT, T::bytes, st>>>(g, cons, prims, target, dt, ext_only);
   return cudaGetLastError();
 }
 
 template <typename R>
 cudaError_t launch_regime_tile_order(const Grid& g, int order, const double* cons,
                                      const double* prims, double* target, double dt,
-                                     cudaStream_t st) {
+                                     cudaStream_t st, bool ext_only = false) {
   switch (order) {
-    case 3: return launch_regime_tile<3, R>(g, cons, prims, target, dt, st);
-    case 5: return launch_regime_tile<5, R>(g, cons, prims, target, dt, st);
-    case 7: return launch_regime_tile<7, R>(g, cons, prims, target, dt, st);
-    case 9: return launch_regime_tile<9, R>(g, cons, prims, target, dt, st);
-    case 11: return launch_regime_tile<11, R>(g, cons, prims, target, dt, st);
+    case 3: return launch_regime_tile<3, R>(g, cons, prims, target, dt, ext_only, st);
+    case 5: return launch_regime_tile<5, R>(g, cons, prims, target, dt, ext_only, st);
+    case 7: return launch_regime_tile<7, R>(g, cons, prims, target, dt, ext_only, st);
+    case 9: return launch_regime_tile<9, R>(g, cons, prims, target, dt, ext_only, st);
+    case 11: return launch_regime_tile<11, R>(g, cons, prims, target, dt, ext_only, st);
     default: return cudaErrorInvalidValue;
   }
 }
